@@ -1,0 +1,309 @@
+/*
+ * medyan_b200.h — C ABI of the B200 mechanical-equilibration library.
+ *
+ * The library evaluates MEDYAN's mechanical energy and forces, rebuilds the
+ * cylinder neighbor list and runs the Polak–Ribière conjugate-gradient
+ * minimizer on one GPU. Every entry point takes plain host pointers and sizes;
+ * the library owns all device memory. A handle is not thread-safe and uses
+ * one CUDA stream.
+ *
+ * Array layouts are the ones the reference's ForceField::vectorize produces:
+ *   - coordinates and forces: AoS double[3*n_beads] (x0 y0 z0 x1 ...),
+ *     src/Structure/DofSerializer.hpp:64-190;
+ *   - bead sets: int32 coordinate offsets 3*beadIndex, n beads per
+ *     interaction, e.g. src/Mechanics/ForceField/Filament/FilamentStretching.cpp:35-36.
+ *
+ * Energy slots follow the reference's ForceFieldManager::forceFields order
+ * (src/Controller/MController.cpp:65-188): filament → linker → motor →
+ * branching → cylinder excluded volume → boundary.
+ */
+#ifndef MEDYAN_B200_H
+#define MEDYAN_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Status codes                                                              */
+/* ------------------------------------------------------------------------ */
+typedef enum medyan_status {
+    MEDYAN_OK = 0,
+    MEDYAN_ERR_INVALID_ARG = 1,   /* null pointer, negative size, bad enum      */
+    MEDYAN_ERR_INDEX_RANGE = 2,   /* bead-set entry outside [0, 3*n_beads) or not a multiple of 3 */
+    MEDYAN_ERR_NONFINITE = 3,     /* NaN/Inf energy: ForceFieldManager::computeEnergy returns +inf
+                                     (src/Mechanics/ForceField/ForceFieldManager.cpp:150-161) */
+    MEDYAN_ERR_ITER_CAP = 4,      /* a device loop hit its iteration cap      */
+    MEDYAN_ERR_CUDA = 5,          /* CUDA runtime error                        */
+    MEDYAN_ERR_OUT_OF_GRID = 6,   /* NL: midpoint outside the bin grid
+                                     (src/Structure/HybridNeighborListImpl.cpp:243-262 throws) */
+    MEDYAN_ERR_LINE_SEARCH = 7,   /* CG: line search failed, recovery disabled
+                                     (MinimizationResult::errorLineSearch) */
+    MEDYAN_ERR_NO_DEVICE = 8,     /* no CUDA device visible                    */
+    MEDYAN_ERR_CAPACITY = 9,      /* caller's output buffer too small          */
+    MEDYAN_ERR_UNSUPPORTED = 10   /* option the library does not implement     */
+} medyan_status;
+
+/* Energy slots (reference force-field order). */
+enum {
+    MEDYAN_FF_FILAMENT_STRETCHING = 0, /* FilamentStretching<FilamentStretchingHarmonic> */
+    MEDYAN_FF_FILAMENT_BENDING = 1,    /* FilamentBending<FilamentBendingCosine>         */
+    MEDYAN_FF_LINKER_STRETCHING = 2,   /* LinkerStretching<LinkerStretchingHarmonic>     */
+    MEDYAN_FF_MOTOR_STRETCHING = 3,    /* MotorGhostStretching<MotorGhostStretchingHarmonic> */
+    MEDYAN_FF_BRANCHING_STRETCHING = 4,/* BranchingStretching<BranchingStretchingHarmonic> */
+    MEDYAN_FF_BRANCHING_BENDING = 5,   /* BranchingBending<BranchingBendingCosine>       */
+    MEDYAN_FF_BRANCHING_DIHEDRAL = 6,  /* BranchingDihedral<BranchingDihedralCosine>     */
+    MEDYAN_FF_BRANCHING_POSITION = 7,  /* BranchingPosition<BranchingPositionCosine>     */
+    MEDYAN_FF_EXCLUDED_VOLUME = 8,     /* CylinderExclVolume<CylinderExclVolRepulsion>   */
+    MEDYAN_FF_BOUNDARY = 9,            /* BoundaryCylinderRepulsion<BoundaryCylinderRepulsionExp> */
+    MEDYAN_FF_COUNT = 10
+};
+
+typedef enum medyan_precision {
+    MEDYAN_PREC_FP64 = 0,   /* all arithmetic in double                                  */
+    MEDYAN_PREC_MIXED = 1   /* per-interaction math in float after FP64 coordinate
+                               differences; energy sums, dots, beta and the Armijo test in double */
+} medyan_precision;
+
+/* ------------------------------------------------------------------------ */
+/* Vectorized force-field description                                        */
+/* ------------------------------------------------------------------------ */
+/*
+ * One struct holds every force field's vectorized arrays. A count of 0 turns
+ * a force field off (its pointers may then be NULL). Each group cites the
+ * reference vectorize() that produces it.
+ */
+typedef struct medyan_system {
+    int32_t n_beads;                 /* DOF = 3*n_beads */
+
+    /* FilamentStretching::vectorize, Filament/FilamentStretching.cpp:24-44:
+       beads[2i..2i+1], k = kstr, l0 = eql (per cylinder). */
+    int32_t n_stretch;
+    const int32_t* stretch_beads;
+    const double* stretch_k;
+    const double* stretch_l0;
+
+    /* FilamentBending::vectorize, Filament/FilamentBending.cpp:28-66:
+       beads[3i..3i+2], k = kbend, theta0 = eqt. */
+    int32_t n_bend;
+    const int32_t* bend_beads;
+    const double* bend_k;
+    const double* bend_theta0;
+
+    /* LinkerStretching::vectorize, Linker/LinkerStretching.cpp:29-59:
+       beads[4i..4i+3], k, l0, pos1, pos2. */
+    int32_t n_linker;
+    const int32_t* linker_beads;
+    const double* linker_k;
+    const double* linker_l0;
+    const double* linker_pos1;
+    const double* linker_pos2;
+
+    /* MotorGhostStretching::vectorize, MotorGhost/MotorGhostStretching.cpp:29-59. */
+    int32_t n_motor;
+    const int32_t* motor_beads;
+    const double* motor_k;
+    const double* motor_l0;
+    const double* motor_pos1;
+    const double* motor_pos2;
+
+    /* Branching point b: beads are parent cylinder (first, second bead) and
+       child cylinder (first, second bead). BranchingStretching uses the
+       first 3 (Branching/BranchingStretching.cpp:29-52), BranchingBending and
+       BranchingDihedral all 4, BranchingPosition the first 3. One position
+       per branch point is shared by stretching, dihedral and position. */
+    int32_t n_branch;
+    const int32_t* branch_beads;     /* 4 per branch point */
+    const double* branch_pos;        /* adjusted relative position on the parent */
+    const double* branch_stretch_k;
+    const double* branch_stretch_l0;
+    const double* branch_bend_k;
+    const double* branch_bend_theta0;
+    const double* branch_dihedral_k;
+    const double* branch_position_k; /* NULL or all-zero disables BranchingPosition */
+    int32_t branch_ff_mask;          /* bit 0 stretch, 1 bend, 2 dihedral, 3 position */
+
+    /* CylinderExclVolume::vectorize, Volume/CylinderExclVolume.cpp:33-179:
+       beads[4i..4i+3] = (c1, c2) of the key cylinder and (c3, c4) of its
+       neighbor, krep, eqlen[2i], eqlen[2i+1]. */
+    int32_t n_excl;
+    const int32_t* excl_beads;
+    const double* excl_k;
+    const double* excl_eqlen;
+
+    /* BoundaryCylinderRepulsion::vectorize,
+       Boundary/BoundaryCylinderRepulsion.cpp:33-88: terms are grouped by
+       boundary element; element e owns nneighbors[e] consecutive terms.
+       Elements are planes a*x + b*y + c*z + d = 0
+       (src/Structure/BoundaryElementImpl.h:30-106). */
+    int32_t n_boundary;
+    const int32_t* boundary_beads;   /* 1 per term */
+    const double* boundary_k;
+    const double* boundary_slen;
+    int32_t n_planes;
+    const double* plane_eq;          /* 4 per plane: a, b, c, d */
+    const int32_t* plane_nneighbors; /* terms per plane */
+} medyan_system;
+
+/* ------------------------------------------------------------------------ */
+/* Force-field handle                                                        */
+/* ------------------------------------------------------------------------ */
+typedef struct medyan_mech medyan_mech;
+
+/* Create a handle on the current CUDA device and upload the vectorized
+   force fields (the device copy of ForceFieldManager::vectorizeAllForceFields,
+   src/Mechanics/ForceField/ForceFieldManager.cpp:35-93). Bead-set entries are
+   range-checked on the host before upload. */
+medyan_status medyan_mech_create(const medyan_system* sys, int32_t precision, medyan_mech** out);
+
+/* Replace every force field's arrays after a new vectorization (same handle,
+   same bead count). Device buffers grow when needed; none are freed. */
+medyan_status medyan_mech_update(medyan_mech* h, const medyan_system* sys);
+
+medyan_status medyan_mech_destroy(medyan_mech* h);
+
+/* Upload coordinates (double[3*n_beads], reference AoS order). */
+medyan_status medyan_mech_set_coords(medyan_mech* h, const double* coord);
+medyan_status medyan_mech_get_coords(medyan_mech* h, double* coord);
+
+/* ForceFieldManager::computeEnergy / computeIndividualEnergies
+   (ForceFieldManager.cpp:96-240): total and per-force-field energies at the
+   uploaded coordinates. e_per_ff may be NULL, else double[MEDYAN_FF_COUNT].
+   A non-finite force-field energy sets *e_total = +inf and returns
+   MEDYAN_ERR_NONFINITE. */
+medyan_status medyan_mech_energy(medyan_mech* h, double* e_total, double* e_per_ff);
+
+/* ForceFieldManager::computeForces (ForceFieldManager.cpp:242-290):
+   force_out = -dE/dx at the uploaded coordinates (zero-filled, then every
+   force field accumulates). */
+medyan_status medyan_mech_forces(medyan_mech* h, double* force_out);
+
+/* One call of both: upload coord, compute energy and forces, download forces.
+   This is MController::updateMechanics without the (de)serialization
+   (src/Controller/MController.h:214-230). */
+medyan_status medyan_mech_evaluate(medyan_mech* h, const double* coord, double* e_total,
+                                   double* e_per_ff, double* force_out);
+
+/* ------------------------------------------------------------------------ */
+/* Conjugate-gradient minimizer                                              */
+/* ------------------------------------------------------------------------ */
+typedef enum medyan_cg_method {
+    MEDYAN_CG_STEEPEST = 0,
+    MEDYAN_CG_FLETCHER_RIEVES = 1,
+    MEDYAN_CG_POLAK_RIBIERE = 2
+} medyan_cg_method;
+
+/* ConjugateGradientParams, src/Mechanics/Minimizer/CGMethod.hpp:44-63. */
+typedef struct medyan_cg_params {
+    int32_t method;                 /* medyan_cg_method                        */
+    double max_dist;                /* maxDist                                  */
+    double lambda_max;              /* lambdaMax                                */
+    double grad_tol;                /* gradTol (component infinity norm)        */
+    double energy_rel_tol;          /* energyRelTol                             */
+    int32_t energy_call_limit;      /* 0 = no limit                             */
+    int32_t force_call_limit;       /* raised to max(limit, 3*n_beads)          */
+    int32_t try_to_recover;         /* tryToRecoverInLineSearchError            */
+} medyan_cg_params;
+
+/* MinimizationResult, src/Mechanics/Minimizer/MinimizationTypes.hpp:10-64. */
+typedef struct medyan_min_result {
+    double energy_before[MEDYAN_FF_COUNT];
+    double energy_before_total;
+    double energy_after[MEDYAN_FF_COUNT];
+    double energy_after_total;
+    uint32_t error_flags;           /* bit 0: errorLineSearch                   */
+    int32_t num_energy_call;
+    int32_t energy_call_limit;
+    int32_t num_force_call;
+    int32_t force_call_limit;
+    int32_t num_iter;
+    double grad_inf_norm;
+    double grad_tol;
+    double energy_rel_change;
+    double energy_rel_tol;
+} medyan_min_result;
+
+/* CGMethod::minimize (CGMethod.hpp:826-1743) with backtracking line search
+   (:238-373) and MController's recovery step (src/Controller/MController.h:273-339).
+   The whole loop runs on the device. coord_inout is double[3*n_beads];
+   force_out may be NULL. */
+medyan_status medyan_cg_minimize(medyan_mech* h, const medyan_cg_params* p, double* coord_inout,
+                                 double* force_out, medyan_min_result* out);
+
+/* ------------------------------------------------------------------------ */
+/* Cylinder neighbor list                                                    */
+/* ------------------------------------------------------------------------ */
+/* Per-cylinder data the hybrid neighbor list reads (Cylinder::DbData,
+   src/Structure/Cylinder.cpp:31-42) plus the per-cylinder parameters that
+   CylinderExclVolume::vectorize and BoundaryCylinderRepulsion::vectorize
+   read. Cylinder order is Cylinder::getCylinders() order. */
+typedef struct medyan_cylinders {
+    int32_t n_cyl;
+    const int32_t* bead1;           /* bead index (not coordinate offset)      */
+    const int32_t* bead2;
+    const int32_t* id;              /* Cylinder::getId(), unique               */
+    const int32_t* filament_id;
+    const int32_t* position_on_filament;
+    const int32_t* type;            /* filament type                            */
+    const int32_t* branching_cylinder; /* index of the cylinder branching off this one, or -1
+                                          (Cylinder::getBranchingCylinder)   */
+    const int32_t* is_minus_end;    /* Cylinder::isMinusEnd()                  */
+    const double* eq_length;        /* MCylinder::getEqLength()                 */
+    const double* excl_k;           /* MCylinder::getExVolConst()               */
+} medyan_cylinders;
+
+/* Neighbor-list parameters: HybridCylinderCylinderNL with one
+   (rmin, rmax) bound, bins of 1.125*rmax over a grid of size grid_size
+   (NX*compartmentSizeX, ...), HybridNeighborListImpl.cpp:176-240. */
+typedef struct medyan_nl_params {
+    float rmax;                     /* stored as float, as in the reference    */
+    float rmin;
+    double grid_size[3];
+} medyan_nl_params;
+
+/* Cubic boundary (src/Structure/BoundaryImpl.cpp:24-52) and the boundary
+   cylinder NL (src/Structure/NeighborListImpl.cpp:738-809). */
+typedef struct medyan_boundary_params {
+    int32_t n_planes;
+    const double* plane_eq;         /* 4 per plane */
+    double k;                       /* BOUNDARYINTERACTIONK */
+    double screen_length;           /* BOUNDARYSCREENLENGTH */
+    float cutoff;                   /* BOUNDARYCUTOFF (NeighborList::_rMax is float) */
+} medyan_boundary_params;
+
+/* Standalone neighbor-list build from host arrays (parity entry point).
+   coord is double[3*n_beads]. Writes canonical pairs (key, neighbor) as
+   cylinder indices into pairs_out[2*k], ordered by key index then neighbor
+   index; key is the cylinder with the larger id. */
+medyan_status medyan_nl_build(const medyan_cylinders* cyl, const double* coord, int32_t n_beads,
+                              const medyan_nl_params* p, int32_t* pairs_out, int64_t capacity,
+                              int64_t* n_pairs);
+
+/* Attach cylinder topology and NL/boundary parameters to a handle. After this,
+   medyan_mech_rebuild_neighbors rebuilds the cylinder NL and the boundary NL
+   from the device coordinates and re-vectorizes the excluded-volume and
+   boundary force fields on the device. */
+medyan_status medyan_mech_set_cylinders(medyan_mech* h, const medyan_cylinders* cyl,
+                                        const medyan_nl_params* nl,
+                                        const medyan_boundary_params* boundary);
+medyan_status medyan_mech_rebuild_neighbors(medyan_mech* h, int64_t* n_excl_out,
+                                            int64_t* n_boundary_out);
+
+/* Copy the excluded-volume interactions currently on the device to the host
+   (beads: 4 per interaction). */
+medyan_status medyan_mech_get_excl_volume(medyan_mech* h, int32_t* beads_out, double* k_out,
+                                          double* eqlen_out, int64_t capacity, int64_t* n_out);
+
+/* ------------------------------------------------------------------------ */
+/* Library info                                                              */
+/* ------------------------------------------------------------------------ */
+const char* medyan_status_string(int32_t status);
+int32_t medyan_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MEDYAN_B200_H */
