@@ -186,6 +186,20 @@ medyan_status medyan_mech_forces(medyan_mech* h, double* force_out);
 medyan_status medyan_mech_evaluate(medyan_mech* h, const double* coord, double* e_total,
                                    double* e_per_ff, double* force_out);
 
+/* Device-resident variants for callers that keep data on the GPU: each
+   enqueues its work on the handle's stream and returns without synchronizing
+   or copying to the host. Results stay in the handle's device buffers
+   (medyan_mech_device_buffers); medyan_mech_synchronize waits and reports the
+   status of the enqueued passes. */
+medyan_status medyan_mech_enqueue_energy(medyan_mech* h);
+medyan_status medyan_mech_enqueue_forces(medyan_mech* h);
+medyan_status medyan_mech_synchronize(medyan_mech* h);
+/* The handle's cudaStream_t, for event timing or stream ordering. */
+void* medyan_mech_stream(medyan_mech* h);
+/* Device pointers of the coordinate and force arrays (double[3*n_beads]) and
+   of the energy output (double[MEDYAN_FF_COUNT + 1]: per force field, then total). */
+medyan_status medyan_mech_device_buffers(medyan_mech* h, double** coord, double** force, double** energy);
+
 /* ------------------------------------------------------------------------ */
 /* Conjugate-gradient minimizer                                              */
 /* ------------------------------------------------------------------------ */

@@ -1,0 +1,206 @@
+// excl.cuh — cylinder-cylinder excluded volume, CylinderExclVolRepulsion
+// (Volume/CylinderExclVolRepulsion.cpp:330-882): the analytic integral of
+// 1/r^4 over two segments and its gradient. The energy and force functions
+// reproduce the reference's expression order for R = double. Pairs whose
+// analytic result is non-finite are flagged for the quadrature fallback
+// (excl_fallback.cu), as energyN/forceN are in the reference.
+#pragma once
+
+#include "device_math.cuh"
+
+namespace mb {
+
+template <class R>
+struct ExclS {
+    R a, b, c, d, e, F, AA, BB, CC, DD, EE, FF, GG, HH, JJ, ATG1, ATG2, ATG3, ATG4;
+};
+
+template <class R>
+__device__ __forceinline__ R atan_r(R x);
+template <>
+__device__ __forceinline__ double atan_r<double>(double x) { return atan(x); }
+template <>
+__device__ __forceinline__ float atan_r<float>(float x) { return atanf(x); }
+
+// Scalars of the analytic integral, :360-410 / :643-690. Inputs are the four
+// bead positions; all differences are formed in FP64.
+template <class R>
+__device__ __forceinline__ void excl_scalars(const V3& c1, const V3& c2, const V3& c3, const V3& c4, ExclS<R>& s) {
+    T3<R> r12 = diff<R>(c1, c2);  // c2 - c1
+    T3<R> r34 = diff<R>(c3, c4);  // c4 - c3
+    T3<R> r31 = diff<R>(c3, c1);  // c1 - c3
+    T3<R> r14 = diff<R>(c1, c4);  // c4 - c1
+    T3<R> r32 = diff<R>(c3, c2);  // c2 - c3
+    s.a = dot(r12, r12);
+    s.b = dot(r34, r34);
+    s.c = dot(r31, r31);
+    s.d = dot(r12, r34);
+    s.e = dot(r12, r31);
+    s.F = dot(r34, r31);
+    R g = dot(r12, r14);  // scalarProduct(c1, c2, c1, c4)
+    R h = dot(r34, r32);  // scalarProduct(c3, c4, c3, c2)
+    R I = dot(r34, r14);  // scalarProduct(c3, c4, c1, c4)
+    // sqmagnitude(c1, c4) = |c1 - c4|^2 and sqmagnitude(c3, c2) = |c3 - c2|^2.
+    R dx = R(c1.x - c4.x), dy = R(c1.y - c4.y), dz = R(c1.z - c4.z);
+    R sqD = (dx * dx + dy * dy + dz * dz);
+    dx = R(c3.x - c2.x);
+    dy = R(c3.y - c2.y);
+    dz = R(c3.z - c2.z);
+    R sqE = (dx * dx + dy * dy + dz * dz);
+    // vec_A = c1 - c2, vec_B = c3 - c4, vec_C = c3 - c1.
+    T3<R> vA{R(c1.x - c2.x), R(c1.y - c2.y), R(c1.z - c2.z)};
+    T3<R> vB{R(c3.x - c4.x), R(c3.y - c4.y), R(c3.z - c4.z)};
+    T3<R> vC{R(c3.x - c1.x), R(c3.y - c1.y), R(c3.z - c1.z)};
+    const R a = s.a, b = s.b, c = s.c, d = s.d, e = s.e, F = s.F;
+    R ac = sqrt(a * c);
+    R bc = sqrt(b * c);
+    R aD = sqrt(a * sqD);
+    R bE = sqrt(b * sqE);
+    s.AA = sqrt(stdmax<R>(R(0), (ac + e) * (ac - e)));
+    s.BB = sqrt(stdmax<R>(R(0), (bc + F) * (bc - F)));
+    s.CC = d * e - a * F;
+    s.DD = b * e - d * F;
+    s.EE = sqrt(stdmax<R>(R(0), (aD + g) * (aD - g)));
+    s.FF = sqrt(stdmax<R>(R(0), (bE + h) * (bE - h)));
+    s.GG = d * g - a * I;
+    s.HH = s.CC + s.GG - s.DD;
+    R cpx = vA.y * vB.z - vA.z * vB.y;
+    R cpy = vA.z * vB.x - vA.x * vB.z;
+    R cpz = vA.x * vB.y - vA.y * vB.x;
+    R JJ = cpx * vC.x + cpy * vC.y + cpz * vC.z;
+    s.JJ = -JJ * JJ;
+    s.ATG1 = atan_r<R>((a + e) / s.AA) - atan_r<R>(e / s.AA);
+    s.ATG2 = atan_r<R>((a + e - d) / s.EE) - atan_r<R>((e - d) / s.EE);
+    s.ATG3 = atan_r<R>((F) / s.BB) - atan_r<R>((F - b) / s.BB);
+    s.ATG4 = atan_r<R>((d + F) / s.FF) - atan_r<R>((d + F - b) / s.FF);
+}
+
+// Analytic pair energy (:355 and :393-435). kRS = krep*L1*L2.
+template <class R>
+__device__ __forceinline__ double excl_energy(const V3& c1, const V3& c2, const V3& c3, const V3& c4, double kRS) {
+    ExclS<R> s;
+    excl_scalars<R>(c1, c2, c3, c4, s);
+    R U = R(0.5) * R(kRS) / s.JJ *
+          (s.CC / s.AA * s.ATG1 + s.GG / s.EE * s.ATG2 + s.DD / s.BB * s.ATG3 + s.HH / s.FF * s.ATG4);
+    return double(U);
+}
+
+// The reference accepts an energy unless it is +-inf, NaN or below -1 (:447-449).
+__device__ __forceinline__ bool excl_energy_bad(double U) { return isinf(U) || U != U || U < -1.0; }
+
+// areInPlane (MathFunctions.h:1101-1133) and movePointOutOfPlane for bead 2 by
+// d (:1221-1270), used by the force path (:610-626). FP64.
+__device__ __forceinline__ bool in_plane(const V3& p1, const V3& p2, const V3& p3, const V3& p4) {
+    double v1[3] = {p2.x - p1.x, p2.y - p1.y, p2.z - p1.z};
+    double v2[3] = {p3.x - p1.x, p3.y - p1.y, p3.z - p1.z};
+    double v3[3] = {p4.x - p1.x, p4.y - p1.y, p4.z - p1.z};
+    double cp[3] = {v1[1] * v2[2] - v1[2] * v2[1], v1[2] * v2[0] - v1[0] * v2[2], v1[0] * v2[1] - v1[1] * v2[0]};
+    double n1 = sqrt(cp[0] * cp[0] + cp[1] * cp[1] + cp[2] * cp[2]);
+    cp[0] = cp[0] / n1;
+    cp[1] = cp[1] / n1;
+    cp[2] = cp[2] / n1;
+    double n3 = sqrt(v3[0] * v3[0] + v3[1] * v3[1] + v3[2] * v3[2]);
+    v3[0] = v3[0] / n3;
+    v3[1] = v3[1] / n3;
+    v3[2] = v3[2] / n3;
+    return fabs(v3[0] * cp[0] + v3[1] * cp[1] + v3[2] * cp[2]) < 1e-1;
+}
+__device__ __forceinline__ V3 move_bead2_out_of_plane(const V3& p1, const V3& p2, const V3& p3, double d) {
+    double v1[3] = {p2.x - p1.x, p2.y - p1.y, p2.z - p1.z};
+    double v2[3] = {p3.x - p1.x, p3.y - p1.y, p3.z - p1.z};
+    double n[3] = {v1[1] * v2[2] - v1[2] * v2[1], v1[2] * v2[0] - v1[0] * v2[2], v1[0] * v2[1] - v1[1] * v2[0]};
+    double m = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+    n[0] = n[0] / m;
+    n[1] = n[1] / m;
+    n[2] = n[2] / m;
+    return V3{p2.x + n[0] * d, p2.y + n[1] * d, p2.z + n[2] * d};
+}
+
+// checkNaN_INF (MathFunctions.h:1377-1384).
+template <class R>
+__device__ __forceinline__ bool bad_force(R x) {
+    return isinf(x) || isnan(x) || fabs(double(x)) > 1e15;
+}
+
+// Analytic pair forces (:578-882). Returns false when any component is
+// non-finite or above 1e15 (the caller then uses the quadrature fallback).
+template <class R>
+__device__ __forceinline__ bool excl_force(const V3& c1, V3 c2, const V3& c3, const V3& c4, double kRS,
+                                           T3<R> (&fo)[4]) {
+    if (in_plane(c1, c2, c3, c4)) c2 = move_bead2_out_of_plane(c1, c2, c3, 0.01);
+    ExclS<R> S;
+    excl_scalars<R>(c1, c2, c3, c4, S);
+    const R a = S.a, b = S.b, c = S.c, d = S.d, e = S.e, F = S.F;
+    const R AA = S.AA, BB = S.BB, CC = S.CC, DD = S.DD, EE = S.EE, FF = S.FF, GG = S.GG, HH = S.HH;
+    const R JJ = S.JJ, ATG1 = S.ATG1, ATG2 = S.ATG2, ATG3 = S.ATG3, ATG4 = S.ATG4;
+    const R invJJ = R(1) / JJ;
+    const R sumBlock = CC / AA * ATG1 + GG / EE * ATG2 + DD / BB * ATG3 + HH / FF * ATG4;
+    const R enFactor = R(kRS) * invJJ / R(2);
+    const R A1 = AA * AA / (AA * AA + (a + e) * (a + e));
+    const R A2 = AA * AA / (AA * AA + e * e);
+    const R E1 = EE * EE / (EE * EE + (a + e - d) * (a + e - d));
+    const R E2 = EE * EE / (EE * EE + (e - d) * (e - d));
+    const R B1 = BB * BB / (BB * BB + F * F);
+    const R B2 = BB * BB / (BB * BB + (F - b) * (F - b));
+    const R F1 = FF * FF / (FF * FF + (d + F) * (d + F));
+    const R F2 = FF * FF / (FF * FF + (d + F - b) * (d + F - b));
+    const R bA_C = ATG1 / AA;
+    const R bA_A = -(ATG1 * CC) / (AA * AA) + (-A1 * (a + e) + A2 * e) * CC / (AA * AA * AA);
+    const R bA_e = ((A1 - A2) * CC) / (AA * AA);
+    const R bA_a = (A1 * CC) / (AA * AA);
+    const R bE_G = ATG2 / EE;
+    const R bE_E = -(ATG2 * GG) / (EE * EE) + (-E1 * (a + e - d) + E2 * (e - d)) * GG / (EE * EE * EE);
+    const R bE_emd = ((E1 - E2) * GG) / (EE * EE);
+    const R bE_a = (E1 * GG) / (EE * EE);
+    const R bB_D = ATG3 / BB;
+    const R bB_B = -(ATG3 * DD) / (BB * BB) + (-B1 * F + B2 * (F - b)) * DD / (BB * BB * BB);
+    const R bB_fmb = ((B1 - B2) * DD) / (BB * BB);
+    const R bB_b = (B1 * DD) / (BB * BB);
+    const R bF_H = ATG4 / FF;
+    const R bF_F = -(ATG4 * HH) / (FF * FF) + (-F1 * (d + F) + F2 * (d + F - b)) * HH / (FF * FF * FF);
+    const R bF_dpfmb = ((F1 - F2) * HH) / (FF * FF);
+    const R bF_b = (F1 * HH) / (FF * FF);
+    const R b11 = bA_C * (-2 * F) + bA_A * (c / AA) + bA_a * 2 + bE_G * (2 * (F - b)) + bE_E * ((b + c - 2 * F) / EE) +
+                  bE_a * 2 + bF_H * (-2 * b) + bF_F * (b / FF);
+    const R b12 = bA_C * e + bE_G * (2 * d - e) + bE_E * ((e - d) / EE) + bE_emd * (-1) + bB_D * (-F) +
+                  bF_H * (2 * d + F) + bF_F * (-(d + F) / FF) + bF_dpfmb;
+    const R b13 = bA_C * d + bA_A * (-e / AA) + bA_e + bE_G * (-d) + bE_E * (-(e - d) / EE) + bE_emd + bB_D * b +
+                  bF_H * (-b) + bF_F * (b / FF);
+    const R b21 = b12;
+    const R b22 = bE_G * (-2 * a) + bE_E * (a / EE) + bB_D * (2 * e) + bB_B * (c / BB) + bB_fmb * (-2) + bB_b * 2 +
+                  bF_H * (-2 * (a + e)) + bF_F * ((a + c + 2 * e) / FF) + bF_dpfmb * (-2) + bF_b * 2;
+    const R b23 = bA_C * (-a) + bE_G * a + bE_E * (-a / EE) + bB_D * (-d) + bB_B * (-F / BB) + bB_fmb + bF_H * d +
+                  bF_F * (-(d + F) / FF) + bF_dpfmb;
+    const R b31 = b13;
+    const R b32 = b23;
+    const R b33 = bA_A * (a / AA) + bE_E * (a / EE) + bB_B * (b / BB) + bF_F * (b / FF);
+    const R J11 = 2 * (-b * c + F * F), J12 = 2 * (c * d - e * F), J13 = 2 * (b * e - d * F);
+    const R J21 = 2 * (c * d - e * F), J22 = 2 * (-a * c + e * e), J23 = 2 * (-d * e + a * F);
+    const R J31 = 2 * (b * e - d * F), J32 = 2 * (-d * e + a * F), J33 = 2 * (d * d - a * b);
+    const R q = -invJJ * sumBlock;
+    R dv[4][3];
+    dv[0][0] = enFactor * (q * (J31 - J11) + (b31 - b11));
+    dv[0][1] = enFactor * (q * (J32 - J12) + (b32 - b12));
+    dv[0][2] = enFactor * (q * (J33 - J13) + (b33 - b13));
+    dv[1][0] = enFactor * (q * (J11) + (b11));
+    dv[1][1] = enFactor * (q * (J12) + (b12));
+    dv[1][2] = enFactor * (q * (J13) + (b13));
+    dv[2][0] = enFactor * (q * (-J31 - J21) + (-b31 - b21));
+    dv[2][1] = enFactor * (q * (-J32 - J22) + (-b32 - b22));
+    dv[2][2] = enFactor * (q * (-J33 - J23) + (-b33 - b23));
+    dv[3][0] = enFactor * (q * (J21) + (b21));
+    dv[3][1] = enFactor * (q * (J22) + (b22));
+    dv[3][2] = enFactor * (q * (J23) + (b23));
+    const T3<R> u = diff<R>(c1, c2), v = diff<R>(c3, c4), w = diff<R>(c3, c1);
+    bool bad = false;
+#pragma unroll
+    for (int bi = 0; bi < 4; ++bi) {
+        fo[bi].x = -(dv[bi][0] * u.x + dv[bi][1] * v.x + dv[bi][2] * w.x);
+        fo[bi].y = -(dv[bi][0] * u.y + dv[bi][1] * v.y + dv[bi][2] * w.y);
+        fo[bi].z = -(dv[bi][0] * u.z + dv[bi][1] * v.z + dv[bi][2] * w.z);
+        bad |= bad_force(fo[bi].x) | bad_force(fo[bi].y) | bad_force(fo[bi].z);
+    }
+    return !bad;
+}
+
+}  // namespace mb

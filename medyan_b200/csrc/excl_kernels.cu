@@ -1,0 +1,368 @@
+// excl_kernels.cu — cylinder excluded-volume energy/force kernels, the
+// quadrature fallbacks, and the energy-pass finish kernel.
+//
+// Built with --fmad=false: the analytic excluded-volume formula cancels
+// heavily for close or near-parallel cylinders, and rounding each operation
+// as written keeps the FP64 path within a few ulps of the CPU reference.
+//
+// Pairs whose analytic energy is +-inf, NaN or < -1 (or whose forces are
+// non-finite or > 1e15) go to a queue; a one-block kernel then evaluates the
+// reference's composite Simpson quadrature for them
+// (CylinderExclVolRepulsion::energyN/forceN, CylinderExclVolRepulsion.cpp:884-1256)
+// with all threads of the block splitting the grid.
+#include "internal.h"
+#include "excl.cuh"
+
+namespace mb {
+
+namespace {
+
+__device__ __forceinline__ V3 at(const V3& x, const V3& d, double lam, bool move) { return move ? move3(x, lam, d) : x; }
+
+template <class R>
+__global__ void __launch_bounds__(kBlock) k_excl_energy(const DeviceFF ff, const double* __restrict__ x,
+                                                        const double* __restrict__ d,
+                                                        const LambdaSet* __restrict__ lset,
+                                                        double* __restrict__ partial, int nblk_total, int blk_off,
+                                                        int* __restrict__ fb_count, int2* __restrict__ fb_list,
+                                                        int* __restrict__ bad) {
+    __shared__ double smem[4 * 32];
+    const int i = blockIdx.x * kBlock + threadIdx.x;
+    const bool move = d != nullptr;
+    const bool valid = i < ff.n_excl;
+    V3 X[4] = {}, D[4] = {};
+    double krs = 0;
+    if (valid) {
+        int4 q = ff.excl_bs[i];
+        krs = ff.excl_krs[i];
+        X[0] = load3(x + q.x); X[1] = load3(x + q.y); X[2] = load3(x + q.z); X[3] = load3(x + q.w);
+        if (move) { D[0] = load3(d + q.x); D[1] = load3(d + q.y); D[2] = load3(d + q.z); D[3] = load3(d + q.w); }
+    }
+    const int K = lset ? lset->K : 1;
+    for (int k = 0; k < K; ++k) {
+        const double lam = lset ? lset->lam[k] : 0.0;
+        double e[1] = {0.0};
+        if (valid) {
+            double U = excl_energy<R>(at(X[0], D[0], lam, move), at(X[1], D[1], lam, move),
+                                      at(X[2], D[2], lam, move), at(X[3], D[3], lam, move), krs);
+            if (excl_energy_bad(U)) {
+                int slot = atomicAdd(fb_count, 1);
+                if (slot < kFallbackCap) fb_list[slot] = make_int2(i, k);
+                else atomicOr(bad + k, 2);
+                U = 0.0;
+            }
+            e[0] = U;
+        }
+        block_sum<1>(e, smem);
+        if (threadIdx.x == 0) {
+            double* o = partial + ((size_t)k * nblk_total + blk_off + blockIdx.x) * 4;
+            o[0] = e[0];
+            o[1] = 0.0;
+            o[2] = 0.0;
+            o[3] = 0.0;
+        }
+    }
+}
+
+template <class R>
+__global__ void __launch_bounds__(kBlock) k_excl_forces(const DeviceFF ff, const double* __restrict__ x,
+                                                        double* __restrict__ f, int* __restrict__ fb_count,
+                                                        int* __restrict__ fb_list, int* __restrict__ status) {
+    const int i = blockIdx.x * kBlock + threadIdx.x;
+    if (i >= ff.n_excl) return;
+    int4 q = ff.excl_bs[i];
+    T3<R> fo[4];
+    if (excl_force<R>(load3(x + q.x), load3(x + q.y), load3(x + q.z), load3(x + q.w), ff.excl_krs[i], fo)) {
+        add_force(f, q.x, fo[0].x, fo[0].y, fo[0].z);
+        add_force(f, q.y, fo[1].x, fo[1].y, fo[1].z);
+        add_force(f, q.z, fo[2].x, fo[2].y, fo[2].z);
+        add_force(f, q.w, fo[3].x, fo[3].y, fo[3].z);
+    } else {
+        int slot = atomicAdd(fb_count, 1);
+        if (slot < kFallbackCap) fb_list[slot] = i;
+        else atomicOr(status, 2);
+    }
+}
+
+// ------------------------------------------------------------ quadrature
+// r^2(s, t) of CylinderExclVolRepulsion.h:50-71.
+__device__ __forceinline__ double r2_of(double a, double b, double c, double d, double e, double F, double s,
+                                        double t) {
+    return c + 2 * s * e + s * s * a - 2 * t * F - 2 * s * t * d + t * t * b;
+}
+
+struct Six {
+    double a, b, c, d, e, F;
+};
+__device__ __forceinline__ Six six_of(const V3& c1, const V3& c2, const V3& c3, const V3& c4) {
+    T3<double> r12 = diff<double>(c1, c2), r34 = diff<double>(c3, c4), r31 = diff<double>(c3, c1);
+    return Six{dot(r12, r12), dot(r34, r34), dot(r31, r31), dot(r12, r34), dot(r12, r31), dot(r34, r31)};
+}
+
+// Grid abscissae advance by repeated addition, as the reference's loops do
+// (s += deltas): grid[i] = value of s in iteration i.
+__device__ void fill_grid(double* grid, int n, double delta) {
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int i = 0; i <= n; ++i) {
+            s += delta;
+            grid[i] = s;
+        }
+    }
+    __syncthreads();
+}
+
+// energyN: 400 x 400 composite Simpson sum (:884-999). Block-parallel over
+// the interior grid; T1..T4 are reduced separately and combined as written.
+__device__ double energyN_block(const Six& q, double kRS, double* grid, double* red) {
+    const int N = 400;
+    const double ds = 1.0 / double(N), dt = 1.0 / double(N);
+    fill_grid(grid, N, ds);
+    auto g = [&](double s, double t) {
+        double r_2 = r2_of(q.a, q.b, q.c, q.d, q.e, q.F, s, t);
+        return (1.0 / (r_2 * r_2));
+    };
+    double T[4] = {0, 0, 0, 0};
+    if (threadIdx.x == 0) T[0] = g(0.0, 0.0) + g(0.0, 1.0) + g(1.0, 0.0) + g(1.0, 1.0);
+    for (int i = 1 + threadIdx.x; i < N; i += blockDim.x) {
+        const double s = grid[i], fs = (i % 2 == 0) ? 2.0 : 4.0;
+        T[1] += fs * (g(s, 0.0) + g(s, 1.0));
+        const double t = grid[i], ft = fs;  // the t grid equals the s grid (N1 == N2)
+        T[2] += ft * (g(0.0, t) + g(1.0, t));
+    }
+    for (int idx = threadIdx.x; idx < (N - 1) * (N - 1); idx += blockDim.x) {
+        const int i = 1 + idx / (N - 1), j = 1 + idx % (N - 1);
+        const double fs = (i % 2 == 0) ? 2.0 : 4.0, ft = (j % 2 == 0) ? 2.0 : 4.0;
+        T[3] += fs * ft * g(grid[i], grid[j]);
+    }
+    block_sum<4>(T, red);
+    __shared__ double result;
+    if (threadIdx.x == 0) result = kRS * (ds * dt / 9.0) * (T[0] + T[1] + T[2] + T[3]);
+    __syncthreads();
+    return result;
+}
+
+// forceN: 10^4 x 10^4 composite Simpson sums of the six force integrands,
+// then the bead forces of :1133-1148. Returns true when finite.
+__device__ bool forceN_block(V3 c1, V3 c2, const V3& c3, const V3& c4, double kRS, bool movebeads, double* grid,
+                             double* red, double (&out)[4][3]) {
+    if (movebeads && in_plane(c1, c2, c3, c4)) {
+        // movePointOutOfPlane for beads 2 and 1, both along the normal of the
+        // original (c1, c2, c3) plane.
+        double v1[3] = {c2.x - c1.x, c2.y - c1.y, c2.z - c1.z};
+        double v2[3] = {c3.x - c1.x, c3.y - c1.y, c3.z - c1.z};
+        double n[3] = {v1[1] * v2[2] - v1[2] * v2[1], v1[2] * v2[0] - v1[0] * v2[2], v1[0] * v2[1] - v1[1] * v2[0]};
+        double m = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+        n[0] = n[0] / m;
+        n[1] = n[1] / m;
+        n[2] = n[2] / m;
+        c2 = V3{c2.x + n[0] * 0.01, c2.y + n[1] * 0.01, c2.z + n[2] * 0.01};
+        c1 = V3{c1.x + n[0] * 0.01, c1.y + n[1] * 0.01, c1.z + n[2] * 0.01};
+    }
+    const Six q = six_of(c1, c2, c3, c4);
+    const int N = 10000;
+    const double ds = 1.0 / double(N), dt = 1.0 / double(N);
+    fill_grid(grid, N, ds);
+    double T[6] = {0, 0, 0, 0, 0, 0};
+    auto acc = [&](double s, double t, double w) {
+        double r_2 = r2_of(q.a, q.b, q.c, q.d, q.e, q.F, s, t);
+        double xi = (1.0 / (r_2 * r_2 * r_2));
+        T[0] += w * xi;
+        T[1] += w * (s * xi);
+        T[2] += w * (s * s * xi);
+        T[3] += w * (s * t * xi);
+        T[4] += w * (t * xi);
+        T[5] += w * (t * t * xi);
+    };
+    if (threadIdx.x == 0) {
+        acc(0.0, 0.0, 1.0); acc(0.0, 1.0, 1.0); acc(1.0, 0.0, 1.0); acc(1.0, 1.0, 1.0);
+    }
+    for (int i = 1 + threadIdx.x; i < N; i += blockDim.x) {
+        const double s = grid[i], w = (i % 2 == 0) ? 2.0 : 4.0;
+        acc(s, 0.0, w);
+        acc(s, 1.0, w);
+        acc(0.0, s, w);
+        acc(1.0, s, w);
+    }
+    for (long long idx = threadIdx.x; idx < (long long)(N - 1) * (N - 1); idx += blockDim.x) {
+        const int i = 1 + int(idx / (N - 1)), j = 1 + int(idx % (N - 1));
+        const double w = ((i % 2 == 0) ? 2.0 : 4.0) * ((j % 2 == 0) ? 2.0 : 4.0);
+        acc(grid[i], grid[j], w);
+    }
+    block_sum<6>(T, red);
+    __shared__ double I[6];
+    if (threadIdx.x == 0)
+        for (int k = 0; k < 6; ++k) I[k] = (ds * dt / 9.0) * T[k];
+    __syncthreads();
+    double vA[3] = {c1.x - c2.x, c1.y - c2.y, c1.z - c2.z};
+    double vB[3] = {c3.x - c4.x, c3.y - c4.y, c3.z - c4.z};
+    double vC[3] = {c3.x - c1.x, c3.y - c1.y, c3.z - c1.z};
+    bool ok = true;
+    for (int k = 0; k < 3; ++k) {
+        out[0][k] = 4.0 * kRS * (-I[0] * vC[k] + I[1] * (vC[k] - vA[k]) + I[2] * vA[k] + I[4] * vB[k] - I[3] * vB[k]);
+        out[1][k] = 4.0 * kRS * (-I[1] * vC[k] - I[2] * vA[k] + I[3] * vB[k]);
+        out[2][k] = 4.0 * kRS * (I[0] * vC[k] + I[1] * vA[k] - I[4] * (vB[k] + vC[k]) - I[3] * vA[k] + I[5] * vB[k]);
+        out[3][k] = 4.0 * kRS * (I[4] * vC[k] + I[3] * vA[k] - I[5] * vB[k]);
+        for (int b = 0; b < 4; ++b) ok &= !bad_force(out[b][k]);
+    }
+    return ok;
+}
+
+__global__ void __launch_bounds__(kBlock) k_excl_force_fallback(const DeviceFF ff, const double* __restrict__ x,
+                                                                double* __restrict__ f, int* __restrict__ fb_count,
+                                                                const int* __restrict__ fb_list,
+                                                                int* __restrict__ status) {
+    extern __shared__ double grid[];  // 10001 abscissae
+    __shared__ double red[6 * 32];
+    const int n = min(*fb_count, kFallbackCap);
+    for (int e = 0; e < n; ++e) {
+        const int i = fb_list[e];
+        const int4 q = ff.excl_bs[i];
+        const V3 c1 = load3(x + q.x), c2 = load3(x + q.y), c3 = load3(x + q.z), c4 = load3(x + q.w);
+        double out[4][3];
+        bool ok = forceN_block(c1, c2, c3, c4, ff.excl_krs[i], false, grid, red, out);
+        if (!ok) ok = forceN_block(c1, c2, c3, c4, ff.excl_krs[i], true, grid, red, out);
+        if (threadIdx.x == 0) {
+            if (ok) {
+                add_force(f, q.x, out[0][0], out[0][1], out[0][2]);
+                add_force(f, q.y, out[1][0], out[1][1], out[1][2]);
+                add_force(f, q.z, out[2][0], out[2][1], out[2][2]);
+                add_force(f, q.w, out[3][0], out[3][1], out[3][2]);
+            } else {
+                atomicOr(status, 1);
+            }
+        }
+        __syncthreads();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) *fb_count = 0;
+}
+
+// Sums the per-block energy partials of each force field (one warp per
+// (lambda, slot), fixed order), evaluates the energyN fallback for queued
+// pairs in (slot, pair) order, and applies ForceFieldManager::computeEnergy's
+// rule (ForceFieldManager.cpp:137-176): a force field at or below -1 makes the
+// total +inf.
+__global__ void __launch_bounds__(kBlock) k_energy_finish(const DeviceFF ff, const double* __restrict__ x,
+                                                          const double* __restrict__ d,
+                                                          const LambdaSet* __restrict__ lset,
+                                                          const double* __restrict__ partial, int nbb, int nbe,
+                                                          int* __restrict__ fb_count, int2* __restrict__ fb_list,
+                                                          int* __restrict__ bad, double* __restrict__ out) {
+    __shared__ double grid[401];
+    __shared__ double red[4 * 32];
+    __shared__ double sums[kMaxLambda][MEDYAN_FF_COUNT];
+    __shared__ double fbE[kMaxLambda];
+    __shared__ int nfb;
+    const int K = lset ? lset->K : 1;
+    const int total_blocks = nbb + nbe;
+    if (threadIdx.x == 0) {
+        int n = min(*fb_count, kFallbackCap);
+        // deterministic order: sort queued (pair, slot) by slot, then pair
+        for (int a = 1; a < n; ++a) {
+            int2 v = fb_list[a];
+            int b = a - 1;
+            while (b >= 0 && (fb_list[b].y > v.y || (fb_list[b].y == v.y && fb_list[b].x > v.x))) {
+                fb_list[b + 1] = fb_list[b];
+                --b;
+            }
+            fb_list[b + 1] = v;
+        }
+        nfb = n;
+        for (int k = 0; k < kMaxLambda; ++k) fbE[k] = 0.0;
+    }
+    __syncthreads();
+    for (int e = 0; e < nfb; ++e) {
+        const int2 q = fb_list[e];
+        const int4 bs = ff.excl_bs[q.x];
+        const double lam = lset ? lset->lam[q.y] : 0.0;
+        V3 P[4];
+        const int offs[4] = {bs.x, bs.y, bs.z, bs.w};
+        for (int j = 0; j < 4; ++j) {
+            V3 X = load3(x + offs[j]);
+            P[j] = d ? move3(X, lam, load3(d + offs[j])) : X;
+        }
+        double U = energyN_block(six_of(P[0], P[1], P[2], P[3]), ff.excl_krs[q.x], grid, red);
+        if (threadIdx.x == 0) {
+            if (excl_energy_bad(U)) atomicOr(bad + q.y, 1);
+            else fbE[q.y] += U;
+        }
+        __syncthreads();
+    }
+    // per-slot sums: warp w handles combos w, w + nwarps, ...
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    for (int combo = warp; combo < K * MEDYAN_FF_COUNT; combo += nwarp) {
+        const int k = combo / MEDYAN_FF_COUNT, slot = combo % MEDYAN_FF_COUNT;
+        int b0 = 0, b1 = 0, j = 0;
+        switch (slot) {
+            case 0: b0 = ff.seg[0]; b1 = ff.seg[1]; break;
+            case 1: b0 = ff.seg[1]; b1 = ff.seg[2]; break;
+            case 2: b0 = ff.seg[2]; b1 = ff.seg[3]; break;
+            case 3: b0 = ff.seg[3]; b1 = ff.seg[4]; break;
+            case 4: case 5: case 6: case 7: b0 = ff.seg[4]; b1 = ff.seg[5]; j = slot - 4; break;
+            case 8: b0 = nbb; b1 = nbb + nbe; break;
+            default: b0 = ff.seg[5]; b1 = ff.seg[6]; break;
+        }
+        double s = 0.0;
+        for (int b = b0 + lane; b < b1; b += 32) s += partial[((size_t)k * total_blocks + b) * 4 + j];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if (lane == 0) sums[k][slot] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < K; ++k) {
+            double* o = out + k * (MEDYAN_FF_COUNT + 1);
+            double tot = 0.0;
+            bool inf = false;
+            for (int slot = 0; slot < MEDYAN_FF_COUNT; ++slot) {
+                double v = sums[k][slot];
+                if (slot == MEDYAN_FF_EXCLUDED_VOLUME) {
+                    v += fbE[k];
+                    if (bad[k]) v = -1.0;
+                }
+                o[slot] = v;
+                if (v <= -1) inf = true;
+                else tot += v;
+            }
+            o[MEDYAN_FF_COUNT] = inf ? __longlong_as_double(0x7ff0000000000000ULL) : tot;
+            bad[k] = 0;
+        }
+        *fb_count = 0;
+    }
+}
+
+}  // namespace
+
+void launch_excl_energy(const DeviceFF& ff, int prec, const double* x, const double* d, const LambdaSet* lam,
+                        const EnergyScratch& es, cudaStream_t s) {
+    const int nbe = es.n_blocks_excl;
+    if (nbe <= 0) return;
+    const int total = es.n_blocks_bonded + nbe;
+    // FP64 in both precision modes: the analytic integral (differences of
+    // arctangents, JJ = -(triple product)^2) loses ~1e-6 relative in float.
+    (void)prec;
+    k_excl_energy<double><<<nbe, kBlock, 0, s>>>(ff, x, d, lam, es.partial, total, es.n_blocks_bonded, es.fb_count,
+                                                 es.fb_list, es.bad);
+}
+
+void launch_excl_energy_fallback_and_finish(const DeviceFF& ff, const double* x, const double* d,
+                                            const LambdaSet* lam, const EnergyScratch& es, cudaStream_t s) {
+    k_energy_finish<<<1, kBlock, 0, s>>>(ff, x, d, lam, es.partial, es.n_blocks_bonded, es.n_blocks_excl,
+                                         es.fb_count, es.fb_list, es.bad, es.out);
+}
+
+void launch_excl_forces(const DeviceFF& ff, int prec, const double* x, double* f, const ForceScratch& fs,
+                        cudaStream_t s) {
+    const int nbe = excl_blocks(ff);
+    if (nbe <= 0) return;
+    (void)prec;  // FP64 in both modes, as for the energy
+    k_excl_forces<double><<<nbe, kBlock, 0, s>>>(ff, x, f, fs.fb_count, fs.fb_list, fs.status);
+    k_excl_force_fallback<<<1, kBlock, kForceNGridBytes, s>>>(ff, x, f, fs.fb_count, fs.fb_list, fs.status);
+}
+
+cudaError_t init_excl_kernels() {
+    return cudaFuncSetAttribute(k_excl_force_fallback, cudaFuncAttributeMaxDynamicSharedMemorySize, kForceNGridBytes);
+}
+
+}  // namespace mb

@@ -1,0 +1,80 @@
+// internal.h — device-side data layout and launch entry points shared by the
+// library's translation units. Not part of the public ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "medyan_b200.h"
+
+namespace mb {
+
+constexpr int kMaxLambda = 8;   // step sizes evaluated per line-search energy pass
+constexpr int kBlock = 256;     // threads per block for interaction kernels
+constexpr int kFallbackCap = 256;
+
+// Vectorized force fields in device memory. Interaction records are packed so
+// each thread issues 16- or 32-byte loads: bead sets as int2/int4 coordinate
+// offsets (3*bead), parameters as double2/double4.
+struct DeviceFF {
+    int n_beads;
+    int n_stretch, n_bend, n_linker, n_motor, n_branch, n_excl, n_boundary, n_planes;
+    int branch_mask;
+    const int2* stretch_bs;    const double2* stretch_p;   // (k, l0)
+    const int4* bend_bs;       const double2* bend_p;      // beads x,y,z (w unused); (k, theta0)
+    const int4* linker_bs;     const double4* linker_p;    // (k, l0, pos1, pos2)
+    const int4* motor_bs;      const double4* motor_p;
+    const int4* branch_bs;     const double4* branch_pa;   // (pos, stretch k, stretch l0, bend k)
+    const double4* branch_pb;                              // (bend theta0, dihedral k, position k, 0)
+    const int4* excl_bs;       const double* excl_krs;     // krep*L1*L2 per pair
+    const int* boundary_bs;    const double2* boundary_p;  // (k, screening length)
+    const int* boundary_plane; const double4* planes;      // plane index per term; a, b, c, d
+    // Block ranges of the bonded kernel: [seg[s], seg[s+1]) for
+    // stretch, bend, linker, motor, branch, boundary.
+    int seg[7];
+};
+
+// Step sizes for one energy pass: positions are x + lam[k]*d.
+struct LambdaSet {
+    int K;
+    int pad;
+    double lam[kMaxLambda];
+};
+
+// Energy pass scratch: per-block partial sums and the quadrature fallback queue.
+struct EnergyScratch {
+    double* partial;      // [kMaxLambda][n_blocks_total][4]
+    int* fb_count;        // excluded-volume pairs needing energyN
+    int2* fb_list;        // (pair, lambda slot)
+    int* bad;             // per lambda slot: fallback failed / queue overflow
+    double* out;          // [kMaxLambda][MEDYAN_FF_COUNT + 1]: per FF, then total
+    int n_blocks_bonded;
+    int n_blocks_excl;
+};
+
+struct ForceScratch {
+    int* fb_count;        // excluded-volume pairs needing forceN
+    int* fb_list;
+    int* status;          // bit 0: fallback failed, bit 1: queue overflow
+};
+
+// Launchers (ff_kernels.cu / excl_kernels.cu). prec: MEDYAN_PREC_*.
+void launch_energy(const DeviceFF& ff, int prec, const double* x, const double* d, const LambdaSet* lam,
+                   const EnergyScratch& es, cudaStream_t s);
+void launch_forces(const DeviceFF& ff, int prec, const double* x, double* f, const ForceScratch& fs, cudaStream_t s);
+
+void launch_excl_energy(const DeviceFF& ff, int prec, const double* x, const double* d, const LambdaSet* lam,
+                        const EnergyScratch& es, cudaStream_t s);
+void launch_excl_forces(const DeviceFF& ff, int prec, const double* x, double* f, const ForceScratch& fs,
+                        cudaStream_t s);
+void launch_excl_energy_fallback_and_finish(const DeviceFF& ff, const double* x, const double* d,
+                                            const LambdaSet* lam, const EnergyScratch& es, cudaStream_t s);
+
+// One-time per-device kernel attributes (forceN's 80 KB abscissa table).
+constexpr int kForceNGridBytes = (10000 + 1) * (int)sizeof(double);
+cudaError_t init_excl_kernels();
+
+int bonded_blocks(const DeviceFF& ff);
+inline int excl_blocks(const DeviceFF& ff) { return (ff.n_excl + kBlock - 1) / kBlock; }
+
+}  // namespace mb

@@ -1,0 +1,191 @@
+"""Host-side mirror of the reference's ForceFieldManager and CGMethod
+interfaces over the CUDA library.
+
+``ForceFieldManager`` follows src/Mechanics/ForceField/ForceFieldManager.h:48-216:
+``vectorize_all_force_fields`` hands the per-force-field arrays to the device,
+``compute_energy`` returns the total (``inf`` when a force field fails, as
+ForceFieldManager.cpp:150-161 does), ``compute_individual_energies`` returns
+the per-force-field report, ``compute_forces`` returns -dE/dx.
+``minimize`` is CGMethod::minimize (src/Mechanics/Minimizer/CGMethod.hpp:826)
+run entirely on the device.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import lib as L
+from ._abi import (FF_COUNT, FF_NAMES, PREC_FP64, PREC_MIXED, CGParams, MinResult, SystemView, f64)
+
+_pd = C.POINTER(C.c_double)
+_pi = C.POINTER(C.c_int32)
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(_pd)
+
+
+@dataclass
+class EnergyReport:
+    """EnergyReport (src/Mechanics/ForceField/Types.hpp:24-33)."""
+    total: float
+    individual: list  # [(name, energy)]
+
+    def as_array(self) -> np.ndarray:
+        return np.array([e for _, e in self.individual])
+
+
+def conjugate_gradient_params(method: int = 2, max_dist: float = 1.0, lambda_max: float = 0.01,
+                              grad_tol: float = 1.0, energy_rel_tol: float = 1e-9, energy_call_limit: int = 0,
+                              force_call_limit: int = 10000, try_to_recover: bool = True) -> CGParams:
+    """ConjugateGradientParams (CGMethod.hpp:44-63); defaults are the
+    reference example's MAXDISTANCE/LAMBDAMAX and MechParams' tolerances."""
+    p = CGParams()
+    p.method = method
+    p.max_dist = max_dist
+    p.lambda_max = lambda_max
+    p.grad_tol = grad_tol
+    p.energy_rel_tol = energy_rel_tol
+    p.energy_call_limit = energy_call_limit
+    p.force_call_limit = force_call_limit
+    p.try_to_recover = 1 if try_to_recover else 0
+    return p
+
+
+class ForceFieldManager:
+    def __init__(self, precision: str = "fp64"):
+        self.lib = L.load()
+        self.precision = {"fp64": PREC_FP64, "mixed": PREC_MIXED}[precision]
+        self.handle = C.c_void_p()
+        self.n_beads = 0
+        self._system = None
+        self._cyl = None
+
+    # -- vectorization -----------------------------------------------------
+    def vectorize_all_force_fields(self, system: SystemView) -> None:
+        self._system = system
+        if not self.handle:
+            h = C.c_void_p()
+            L.check(self.lib.medyan_mech_create(system.ref(), self.precision, C.byref(h)), "medyan_mech_create")
+            self.handle = h
+            self.n_beads = system.n_beads
+        else:
+            L.check(self.lib.medyan_mech_update(self.handle, system.ref()), "medyan_mech_update")
+
+    # -- energy / forces ---------------------------------------------------
+    def set_coords(self, coord) -> None:
+        x = f64(coord)
+        assert x.size == 3 * self.n_beads
+        L.check(self.lib.medyan_mech_set_coords(self.handle, _dp(x)), "medyan_mech_set_coords")
+
+    def get_coords(self) -> np.ndarray:
+        x = np.zeros(3 * self.n_beads)
+        L.check(self.lib.medyan_mech_get_coords(self.handle, _dp(x)), "medyan_mech_get_coords")
+        return x
+
+    def _energy(self):
+        tot = C.c_double(0.0)
+        per = np.zeros(FF_COUNT)
+        st = self.lib.medyan_mech_energy(self.handle, C.byref(tot), _dp(per))
+        if st not in (0, 3):
+            L.check(st, "medyan_mech_energy")
+        return tot.value, per
+
+    def compute_energy(self, coord=None) -> float:
+        if coord is not None:
+            self.set_coords(coord)
+        return self._energy()[0]
+
+    def compute_individual_energies(self, coord=None) -> EnergyReport:
+        if coord is not None:
+            self.set_coords(coord)
+        _, per = self._energy()
+        return EnergyReport(total=float(np.sum(per)), individual=list(zip(FF_NAMES, per.tolist())))
+
+    def compute_forces(self, coord=None) -> np.ndarray:
+        if coord is not None:
+            self.set_coords(coord)
+        f = np.zeros(3 * self.n_beads)
+        L.check(self.lib.medyan_mech_forces(self.handle, _dp(f)), "medyan_mech_forces")
+        return f
+
+    def evaluate(self, coord):
+        """Energy, per-force-field energies and forces at coord in one call."""
+        x = f64(coord)
+        f = np.zeros_like(x)
+        tot = C.c_double(0.0)
+        per = np.zeros(FF_COUNT)
+        st = self.lib.medyan_mech_evaluate(self.handle, _dp(x), C.byref(tot), _dp(per), _dp(f))
+        if st not in (0, 3):
+            L.check(st, "medyan_mech_evaluate")
+        return tot.value, per, f
+
+    # -- minimizer ---------------------------------------------------------
+    def minimize(self, coord, params: CGParams):
+        """CGMethod::minimize on the device. Returns (status, coord, force, MinResult)."""
+        x = f64(coord).copy()
+        f = np.zeros_like(x)
+        r = MinResult()
+        st = self.lib.medyan_cg_minimize(self.handle, C.byref(params), _dp(x), _dp(f), C.byref(r))
+        if st not in (0, 7):
+            L.check(st, "medyan_cg_minimize")
+        return st, x, f, r
+
+    # -- neighbor lists ----------------------------------------------------
+    def set_cylinders(self, cylinders, nl_params, boundary_params) -> None:
+        self._cyl = (cylinders, nl_params, boundary_params)
+        L.check(self.lib.medyan_mech_set_cylinders(self.handle, cylinders.ref(), C.byref(nl_params),
+                                                   C.byref(boundary_params) if boundary_params is not None else None),
+                "medyan_mech_set_cylinders")
+
+    def rebuild_neighbor_lists(self) -> tuple[int, int]:
+        ne = C.c_int64(0)
+        nb = C.c_int64(0)
+        L.check(self.lib.medyan_mech_rebuild_neighbors(self.handle, C.byref(ne), C.byref(nb)),
+                "medyan_mech_rebuild_neighbors")
+        return ne.value, nb.value
+
+    def excluded_volume_interactions(self):
+        n = C.c_int64(0)
+        L.check(self.lib.medyan_mech_get_excl_volume(self.handle, None, None, None, 0, C.byref(n)),
+                "medyan_mech_get_excl_volume")
+        m = n.value
+        beads = np.zeros(4 * max(m, 1), np.int32)
+        k = np.zeros(max(m, 1))
+        eq = np.zeros(2 * max(m, 1))
+        L.check(self.lib.medyan_mech_get_excl_volume(self.handle, beads.ctypes.data_as(_pi), _dp(k), _dp(eq), m,
+                                                     C.byref(n)), "medyan_mech_get_excl_volume")
+        return beads[: 4 * m].reshape(-1, 4), k[:m], eq[: 2 * m].reshape(-1, 2)
+
+    # -- lifetime ----------------------------------------------------------
+    def close(self) -> None:
+        if self.handle:
+            self.lib.medyan_mech_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def neighbor_pairs(cylinders, coord, n_beads: int, nl_params) -> np.ndarray:
+    """medyan_nl_build: canonical (key, neighbor) cylinder-index pairs."""
+    lib = L.load()
+    x = f64(coord)
+    n = C.c_int64(0)
+    L.check(lib.medyan_nl_build(cylinders.ref(), _dp(x), n_beads, C.byref(nl_params), None, 0, C.byref(n)),
+            "medyan_nl_build")
+    pairs = np.zeros(2 * max(n.value, 1), np.int32)
+    L.check(lib.medyan_nl_build(cylinders.ref(), _dp(x), n_beads, C.byref(nl_params), pairs.ctypes.data_as(_pi),
+                                n.value, C.byref(n)), "medyan_nl_build")
+    return pairs[: 2 * n.value].reshape(-1, 2)

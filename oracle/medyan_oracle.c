@@ -946,7 +946,9 @@ void oracle_forces(const medyan_system* s, const double* x, double* f) {
 
 /* -------------------------------------------------------------------- CG */
 typedef struct CGState {
-    const medyan_system* s;
+    oracle_energy_fn efn;
+    oracle_force_fn ffn;
+    void* ctx;
     int ndof;
     double *force, *forcePrev, *searchDir, *coordLS, *coordMinE;
     int haveMinE;
@@ -980,7 +982,7 @@ static double cg_backtrack(CGState* st, const double* x, double maxDist, double 
     *newEnergy = 0;
     if (maxForce == 0.0) return 0.0;
     double lambda = lambdaMax < maxDist / maxForce ? lambdaMax : maxDist / maxForce;
-    const double currentEnergy = oracle_energy(st->s, x, NULL);
+    const double currentEnergy = st->efn(st->ctx, x);
     ++*nEnergy;
     const double expectedSlope = cg_dot(st->searchDir, st->force, st->ndof);
     const double reducedSlope = armijo * expectedSlope;
@@ -988,7 +990,7 @@ static double cg_backtrack(CGState* st, const double* x, double maxDist, double 
     double energyLambda = 0.0;
     while (!done) {
         for (int i = 0; i < st->ndof; ++i) st->coordLS[i] = x[i] + lambda * st->searchDir[i];
-        energyLambda = oracle_energy(st->s, st->coordLS, NULL);
+        energyLambda = st->efn(st->ctx, st->coordLS);
         ++*nEnergy;
         const double ideal = -reducedSlope * lambda;
         if (lambda < 0 || ideal > 0) {
@@ -1009,9 +1011,15 @@ static double cg_backtrack(CGState* st, const double* x, double maxDist, double 
     return lambda;
 }
 
-static void fill_energies(const medyan_system* s, const double* x, double* per, double* total) {
+static double sys_energy(void* ctx, const double* x) { return oracle_energy((const medyan_system*)ctx, x, NULL); }
+static void sys_forces(void* ctx, const double* x, double* f) { oracle_forces((const medyan_system*)ctx, x, f); }
+static void sys_individual(void* ctx, const double* x, double* per) { oracle_energy((const medyan_system*)ctx, x, per); }
+
+/* computeIndividualEnergies + total (ForceFieldManager.cpp:209-240). */
+static void fill_energies(oracle_individual_fn ifn, void* ctx, const double* x, double* per, double* total) {
     double e[MEDYAN_FF_COUNT];
-    oracle_energy(s, x, e);
+    for (int i = 0; i < MEDYAN_FF_COUNT; ++i) e[i] = 0.0;
+    ifn(ctx, x, e);
     double t = 0.0;
     for (int i = 0; i < MEDYAN_FF_COUNT; ++i) {
         per[i] = e[i];
@@ -1020,14 +1028,23 @@ static void fill_energies(const medyan_system* s, const double* x, double* per, 
     *total = t;
 }
 
-/* CGMethod::minimize, CGMethod.hpp:826-1743, with MController's recovery step
-   (src/Controller/MController.h:273-339). */
 int32_t oracle_cg_minimize(const medyan_system* s, const medyan_cg_params* p, double* x, double* f_out,
                            medyan_min_result* out) {
+    return oracle_cg_minimize_cb(3 * s->n_beads, s->n_beads, p, x, f_out, out, sys_energy, sys_forces,
+                                 sys_individual, (void*)s);
+}
+
+/* CGMethod::minimize, CGMethod.hpp:826-1743, with MController's recovery step
+   (src/Controller/MController.h:273-339). */
+int32_t oracle_cg_minimize_cb(int32_t ndof, int32_t n_beads, const medyan_cg_params* p, double* x, double* f_out,
+                              medyan_min_result* out, oracle_energy_fn efn, oracle_force_fn ffn,
+                              oracle_individual_fn ifn, void* ctx) {
     CGState st;
     memset(&st, 0, sizeof st);
-    st.s = s;
-    st.ndof = 3 * s->n_beads;
+    st.efn = efn;
+    st.ffn = ffn;
+    st.ctx = ctx;
+    st.ndof = ndof;
     const int n = st.ndof;
     st.force = calloc((size_t)n + 1, sizeof(double));
     st.forcePrev = calloc((size_t)n + 1, sizeof(double));
@@ -1040,16 +1057,16 @@ int32_t oracle_cg_minimize(const medyan_system* s, const medyan_cg_params* p, do
     r.energy_call_limit = p->energy_call_limit;
     r.grad_tol = p->grad_tol;
     r.energy_rel_tol = p->energy_rel_tol;
-    r.force_call_limit = p->force_call_limit > 3 * s->n_beads ? p->force_call_limit : 3 * s->n_beads;
+    r.force_call_limit = p->force_call_limit > 3 * n_beads ? p->force_call_limit : 3 * n_beads;
     r.grad_inf_norm = INFINITY;
     r.energy_rel_change = INFINITY;
     int32_t status = MEDYAN_OK;
     int err = 0;
     const int method = p->method;
 
-    fill_energies(s, x, r.energy_before, &r.energy_before_total);
+    fill_energies(ifn, ctx, x, r.energy_before, &r.energy_before_total);
     ++r.num_energy_call;
-    oracle_forces(s, x, st.force);
+    ffn(ctx, x, st.force);
     ++r.num_force_call;
     r.grad_inf_norm = cg_maxf(&st, &err);
     if (err) { status = MEDYAN_ERR_NONFINITE; goto done; }
@@ -1078,7 +1095,7 @@ int32_t oracle_cg_minimize(const medyan_system* s, const medyan_cg_params* p, do
                     }
                     if (step == INFINITY) { status = MEDYAN_ERR_NONFINITE; goto done; }
                     for (int i = 0; i < n; ++i) x[i] += step * st.searchDir[i];
-                    oracle_forces(s, x, st.force);
+                    ffn(ctx, x, st.force);
                     ++r.num_force_call;
                     r.grad_inf_norm = cg_maxf(&st, &err);
                     if (err) { status = MEDYAN_ERR_NONFINITE; goto done; }
@@ -1098,7 +1115,7 @@ int32_t oracle_cg_minimize(const medyan_system* s, const medyan_cg_params* p, do
             }
         } else {
             for (int i = 0; i < n; ++i) x[i] += lambda * st.searchDir[i];
-            oracle_forces(s, x, st.force);
+            ffn(ctx, x, st.force);
             ++r.num_force_call;
             r.grad_inf_norm = cg_maxf(&st, &err);
             if (err) { status = MEDYAN_ERR_NONFINITE; goto done; }
@@ -1127,7 +1144,7 @@ int32_t oracle_cg_minimize(const medyan_system* s, const medyan_cg_params* p, do
     if (CALL_LIMIT() && st.haveMinE) memcpy(x, st.coordMinE, sizeof(double) * n);
 #undef CALL_LIMIT
 #undef CONVERGED
-    fill_energies(s, x, r.energy_after, &r.energy_after_total);
+    fill_energies(ifn, ctx, x, r.energy_after, &r.energy_after_total);
     ++r.num_energy_call;
     r.num_iter = numIter;
 done:

@@ -52,8 +52,18 @@ void oracle_boundary_forces(const double* x, double* f, const medyan_system* s);
 double oracle_energy(const medyan_system* s, const double* x, double* e_per_ff);
 void oracle_forces(const medyan_system* s, const double* x, double* f);
 
-/* CGMethod::minimize. Returns MEDYAN_OK, MEDYAN_ERR_LINE_SEARCH or
-   MEDYAN_ERR_NONFINITE. */
+/* CGMethod::minimize driven by callbacks: energy(x), forces(x, f) and the
+   per-force-field energies (x, per[MEDYAN_FF_COUNT]). n_beads only sets the
+   force-call limit max(limit, 3*n_beads). */
+typedef double (*oracle_energy_fn)(void* ctx, const double* x);
+typedef void (*oracle_force_fn)(void* ctx, const double* x, double* f);
+typedef void (*oracle_individual_fn)(void* ctx, const double* x, double* per);
+int32_t oracle_cg_minimize_cb(int32_t ndof, int32_t n_beads, const medyan_cg_params* p, double* x, double* f_out,
+                              medyan_min_result* out, oracle_energy_fn efn, oracle_force_fn ffn,
+                              oracle_individual_fn ifn, void* ctx);
+
+/* CGMethod::minimize over the force fields of s. Returns MEDYAN_OK,
+   MEDYAN_ERR_LINE_SEARCH or MEDYAN_ERR_NONFINITE. */
 int32_t oracle_cg_minimize(const medyan_system* s, const medyan_cg_params* p, double* x, double* f_out,
                            medyan_min_result* out);
 

@@ -252,4 +252,74 @@ int medyan_ref_cg_minimize(const medyan_system* sys, const medyan_cg_params* p, 
     return res.errorFlags ? MEDYAN_ERR_LINE_SEARCH : MEDYAN_OK;
 }
 
+// CGMethod::minimize from the reference sources driven by C callbacks
+// (energy, forces, per-force-field energies), as the reference's own
+// TestCGMethod drives it with plain lambdas.
+typedef double (*ref_energy_fn)(void* ctx, const double* x);
+typedef void (*ref_force_fn)(void* ctx, const double* x, double* f);
+typedef void (*ref_individual_fn)(void* ctx, const double* x, double* per);
+
+int medyan_ref_cg_minimize_cb(int ndof, int n_beads, const medyan_cg_params* p, double* coord_io, double* force_out,
+                              medyan_min_result* out, ref_energy_fn efn, ref_force_fn ffn, ref_individual_fn ifn,
+                              void* ctx) {
+    Bead::count = n_beads;
+    std::vector<floatingpoint> coord(coord_io, coord_io + ndof);
+    std::vector<floatingpoint> force;
+    ConjugateGradientParams cg;
+    cg.descentSearchMethod = p->method == 0 ? ConjugateGradientDescentSearch::steepest
+                             : p->method == 1 ? ConjugateGradientDescentSearch::fletcherRieves
+                                              : ConjugateGradientDescentSearch::polakRibiere;
+    cg.maxDist = p->max_dist;
+    cg.lambdaMax = p->lambda_max;
+    cg.gradTol = p->grad_tol;
+    cg.energyRelTol = p->energy_rel_tol;
+    cg.energyCallLimit = p->energy_call_limit;
+    cg.forceCallLimit = p->force_call_limit;
+    cg.tryToRecoverInLineSearchError = p->try_to_recover != 0;
+    const auto energyFunc = [&](floatingpoint* c) { return efn(ctx, c); };
+    const auto forceFunc = [&](floatingpoint* c, floatingpoint* f, int) { ffn(ctx, c, f); };
+    const auto energyFuncIndividual = [&](floatingpoint* c) {
+        double e[MEDYAN_FF_COUNT] = {0};
+        ifn(ctx, c, e);
+        EnergyReport rep;
+        rep.total = 0.0;
+        for (int i = 0; i < MEDYAN_FF_COUNT; ++i) {
+            rep.individual.push_back({"", e[i]});
+            rep.total += e[i];
+        }
+        return rep;
+    };
+    const double maxDist = p->max_dist;
+    const auto recovery = [&](std::vector<floatingpoint>& c, const std::vector<floatingpoint>& dir) {
+        double step = std::numeric_limits<double>::infinity();
+        for (int i = 0; i < ndof; ++i) step = std::min(step, maxDist / std::abs(dir[i]));
+        if (step == std::numeric_limits<double>::infinity()) throw std::runtime_error("Invalid step size.");
+        for (int i = 0; i < ndof; ++i) c[i] += step * dir[i];
+    };
+    CGMethod method;
+    MinimizationResult res;
+    try {
+        res = method.minimize(cg, coord, ndof, energyFunc, forceFunc, energyFuncIndividual, recovery, &force);
+    } catch (const std::exception&) {
+        return MEDYAN_ERR_NONFINITE;
+    }
+    std::copy(coord.begin(), coord.begin() + ndof, coord_io);
+    if (force_out) std::copy(force.begin(), force.begin() + ndof, force_out);
+    if (out) {
+        fill_report(res.energiesBefore, out->energy_before, &out->energy_before_total);
+        fill_report(res.energiesAfter, out->energy_after, &out->energy_after_total);
+        out->error_flags = (uint32_t)res.errorFlags;
+        out->num_energy_call = res.numEnergyCall;
+        out->energy_call_limit = res.energyCallLimit;
+        out->num_force_call = res.numForceCall;
+        out->force_call_limit = res.forceCallLimit;
+        out->num_iter = -1;
+        out->grad_inf_norm = res.gradInfNorm;
+        out->grad_tol = res.gradTol;
+        out->energy_rel_change = res.energyRelChange;
+        out->energy_rel_tol = res.energyRelTol;
+    }
+    return res.errorFlags ? MEDYAN_ERR_LINE_SEARCH : MEDYAN_OK;
+}
+
 }  // extern "C"

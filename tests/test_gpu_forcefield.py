@@ -1,0 +1,126 @@
+"""GPU energy and force evaluation vs the oracle and the reference's outputs.
+
+Tolerances:
+- FP64 path: total energy relative error <= 1e-12; per-force-field energy
+  error <= 1e-12 * max(|E_ff|, |E_total|) (near-zero force-field energies are
+  rounding noise of cancelling terms); forces max|df| <= 1e-12 * max|f_ref|.
+- Mixed path (float interaction math, FP64 sums): forces max|df| <= 1e-6 *
+  max|f_ref|, energies relative <= 1e-6.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from medyan_b200._abi import SystemView
+from medyan_b200.forcefield import ForceFieldManager
+from medyan_b200.network import make_workload
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+FP64_TOL = 1e-12
+MIXED_TOL = 1e-6
+
+
+def check(ff_e, ff_per, ff_f, ref_e, ref_per, ref_f, tol, name=""):
+    assert np.isfinite(ff_e), name
+    assert abs(ff_e - ref_e) <= tol * abs(ref_e), (name, ff_e, ref_e)
+    scale = max(abs(ref_e), 1e-300)
+    for i in range(10):
+        assert abs(ff_per[i] - ref_per[i]) <= tol * max(abs(ref_per[i]), scale), (name, i, ff_per[i], ref_per[i])
+    fs = np.abs(ref_f).max()
+    if fs > 0:
+        err = np.abs(ff_f - ref_f).max() / fs
+        assert err <= tol, (name, err)
+
+
+def gpu_eval(sv, x, precision="fp64"):
+    with ForceFieldManager(precision) as ff:
+        ff.vectorize_all_force_fields(sv)
+        e, per, f = ff.evaluate(x)
+        # the separate entry points agree with the fused one
+        ff.set_coords(x)
+        assert ff.compute_energy() == e
+        f2 = ff.compute_forces()
+        assert np.allclose(f2, f, rtol=0, atol=1e-12 * max(np.abs(f).max(), 1.0))
+        rep = ff.compute_individual_energies()
+        assert np.array_equal(rep.as_array(), per)
+    return e, per, f
+
+
+@pytest.fixture(scope="module")
+def nets():
+    return dict(np.load(os.path.join(GOLDEN, "synthetic_networks.npz")))
+
+
+def network_system(nets, tag):
+    keys = [k.split("/", 1)[1] for k in nets if k.startswith(tag + "/") and k.count("/") == 1]
+    arrays = {k: nets[f"{tag}/{k}"] for k in keys if k not in ("n_beads", "coord", "branch_ff_mask")}
+    arrays["branch_ff_mask"] = int(nets[f"{tag}/branch_ff_mask"][0])
+    return SystemView(int(nets[f"{tag}/n_beads"][0]), **arrays), nets[f"{tag}/coord"]
+
+
+@pytest.mark.parametrize("tag", ["cfg0", "branched"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_golden_networks(gpu_lib, oracle, nets, tag, precision):
+    sv, x = network_system(nets, tag)
+    e, per, f = gpu_eval(sv, x, precision)
+    tol = FP64_TOL if precision == "fp64" else MIXED_TOL
+    for rtag in ("reference", "strict"):
+        check(e, per, f, nets[f"{tag}/{rtag}/energy"][0], nets[f"{tag}/{rtag}/per_ff"], nets[f"{tag}/{rtag}/force"],
+              tol, f"{tag}/{rtag}/{precision}")
+    eo, pero = oracle.energy(sv, x)
+    check(e, per, f, eo, pero, oracle.forces(sv, x), tol, f"{tag}/oracle/{precision}")
+
+
+@pytest.mark.parametrize("cfg", [3, 1])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_workload_networks(gpu_lib, oracle, cfg, precision):
+    net = make_workload(cfg)
+    st, extra = oracle.complete(net)
+    assert st == 0
+    sv = net.system_view(**extra)
+    x = net.flat_coords()
+    e, per, f = gpu_eval(sv, x, precision)
+    eo, pero = oracle.energy(sv, x)
+    check(e, per, f, eo, pero, oracle.forces(sv, x), FP64_TOL if precision == "fp64" else MIXED_TOL,
+          f"cfg{cfg}/{precision}")
+
+
+def test_reference_unit_inputs(gpu_lib):
+    from tests.test_oracle_pins import unit_systems
+    with open(os.path.join(GOLDEN, "reference_unit_inputs.json")) as fh:
+        unit = json.load(fh)
+    for name, sv, x in unit_systems(unit):
+        e, per, f = gpu_eval(sv, np.asarray(x, float))
+        ref = unit["results"]["reference"][name]
+        tol = 1e-4 if name == "excl_stress" else FP64_TOL
+        check(e, per, f, ref["energy"], ref["per_ff"], np.asarray(ref["force"]), tol, name)
+
+
+def test_empty_system(gpu_lib):
+    sv = SystemView(4)
+    e, per, f = gpu_eval(sv, np.zeros(12))
+    assert e == 0.0 and not per.any() and not f.any()
+
+
+def test_collinear_pair_uses_quadrature(gpu_lib, oracle):
+    # Collinear cylinders make the analytic excluded-volume formula divide by
+    # zero; the reference then integrates numerically (energyN/forceN).
+    x = np.array([0, 0, 0, 10, 0, 0, 20, 0, 0, 30, 0, 0], float)
+    sv = SystemView(4, excl_beads=[0, 3, 6, 9], excl_k=[1e5], excl_eqlen=[10.0, 10.0])
+    e, per, f = gpu_eval(sv, x)
+    eo, _ = oracle.energy(sv, x)
+    fo = oracle.forces(sv, x)
+    assert np.isfinite(e) and abs(e - eo) <= 1e-9 * abs(eo)
+    assert np.abs(f - fo).max() <= 1e-9 * np.abs(fo).max()
+
+
+def test_rejects_bad_bead_index(gpu_lib):
+    from medyan_b200.lib import MedyanError
+    sv = SystemView(2, stretch_beads=[0, 6], stretch_k=[1.0], stretch_l0=[1.0])
+    with pytest.raises(MedyanError) as e:
+        ForceFieldManager().vectorize_all_force_fields(sv)
+    assert e.value.status == 2
