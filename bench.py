@@ -1,0 +1,396 @@
+"""Benchmark: force evaluations per second on the 400k-cylinder network.
+
+A step is one force evaluation in the reference's updateMechanics sense
+(src/Controller/MController.h:214-230): the total energy and the forces of all
+force fields (filament stretching and bending, linker, motor, branching,
+cylinder excluded volume, boundary) at one set of coordinates. The workload
+is 20,000 filaments x 20 cylinders in a 10 um cube with 100k linkers, 10k
+motors and 5k branch points; excluded-volume and boundary interactions come
+from the device neighbor list (54 nm cutoff).
+
+value: steps/s with coordinates resident in HBM, L2 flushed (256 MiB write)
+before every timed step, device time from CUDA events on the library's stream.
+e2e: the same step through the C ABI (medyan_mech_evaluate) from pinned host
+buffers: coordinates in, energy and forces out, copies inside the timed region.
+
+--impl reference times the reference's own compiled CPU kernels
+(oracle/_ref/libmedyan_ref.so, one thread: the reference is single-threaded)
+on the same workload.
+
+Multi-GPU: replicas only (each rank evaluates its own copy; no collective on
+the path), value = all ranks' steps / max rank time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "CG minimizations/s & force-evals/s, mixed vs FP64 GPU at rel force err ≤1e-6"
+WORKLOAD = "cfg4_400k_cylinders_20000x20_10um"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--no-minimize", action="store_true", help="skip the minimization extras")
+    ap.add_argument("--cpu-sample-s", type=float, default=15.0)
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------- workload
+def build_network():
+    from medyan_b200.network import make_workload
+    return make_workload(4)
+
+
+def algorithmic_bytes(ff_counts: dict, n_beads: int) -> dict:
+    """Compulsory traffic of one energy pass and one force pass: each bead's
+    coordinates read once (24 B), forces written once (24 B), each
+    interaction's int32 bead offsets and FP64 parameters read once."""
+    per = {"stretch": 2 * 4 + 2 * 8, "bend": 3 * 4 + 2 * 8, "linker": 4 * 4 + 4 * 8, "motor": 4 * 4 + 4 * 8,
+           "branch": (3 * 4 + 3 * 8) + (4 * 4 + 2 * 8) + (4 * 4 + 2 * 8), "excl": 4 * 4 + 3 * 8,
+           "boundary": 1 * 4 + 2 * 8}
+    inter = sum(per[k] * ff_counts.get(k, 0) for k in per)
+    coords = 24 * n_beads
+    return {"energy": inter + coords, "forces": inter + coords + 24 * n_beads,
+            "step": 2 * inter + 2 * coords + 24 * n_beads}
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 8:
+                self.rows.append(parts)
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[4 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+# ---------------------------------------------------------------- our arm
+def run_ours(args, rank: int, world: int) -> dict:
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    from medyan_b200.forcefield import ForceFieldManager, conjugate_gradient_params
+
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    net = build_network()
+    x = net.flat_coords()
+    bp, planes = net.boundary_params()
+
+    def make(prec):
+        ff = ForceFieldManager(prec)
+        ff.vectorize_all_force_fields(net.system_view())
+        ff.set_coords(x)
+        ff.set_cylinders(net.cylinders_view(), net.nl_params(), bp)
+        ff.rebuild_neighbor_lists()
+        ff.lib.medyan_mech_synchronize(ff.handle)
+        return ff
+
+    ff = make(args.precision)
+    L, h = ff.lib, ff.handle
+    ne, nb = ff.rebuild_neighbor_lists()
+    counts = {"stretch": net.ff["stretch_beads"].shape[0], "bend": net.ff["bend_beads"].shape[0],
+              "linker": net.ff["linker_beads"].shape[0], "motor": net.ff["motor_beads"].shape[0],
+              "branch": net.ff["branch_beads"].shape[0], "excl": ne, "boundary": nb}
+    abytes = algorithmic_bytes(counts, net.n_beads)
+
+    stream = torch.cuda.ExternalStream(L.medyan_mech_stream(h))
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def step():
+        L.medyan_mech_enqueue_energy(h)
+        L.medyan_mech_enqueue_forces(h)
+
+    # warm-up
+    for _ in range(max(args.warmup, 3)):
+        step()
+    if L.medyan_mech_synchronize(h) != 0:
+        raise RuntimeError("force evaluation reported an error")
+
+    K = args.steps
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+           torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    with ClockSampler(dev) as clocks:
+        with torch.cuda.stream(stream):
+            for i in range(K):
+                flush.zero_()
+                ev[i][0].record(stream)
+                L.medyan_mech_enqueue_forces(h)
+                ev[i][1].record(stream)
+                L.medyan_mech_enqueue_energy(h)
+                ev[i][2].record(stream)
+        L.medyan_mech_synchronize(h)
+        torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    t_force = [ev[i][0].elapsed_time(ev[i][1]) / 1e3 for i in range(K)]
+    t_energy = [ev[i][1].elapsed_time(ev[i][2]) / 1e3 for i in range(K)]
+    t_step = sum(t_force) + sum(t_energy)
+    if world > 1:
+        tt = torch.tensor([t_step], device="cuda")
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        t_step = float(tt.item())
+
+    # e2e through the C ABI from pinned host buffers
+    xh = torch.from_numpy(x.copy()).pin_memory()
+    fh = torch.empty_like(xh).pin_memory()
+    xptr = C.cast(xh.data_ptr(), C.POINTER(C.c_double))
+    fptr = C.cast(fh.data_ptr(), C.POINTER(C.c_double))
+    etot = C.c_double()
+    per = (C.c_double * 10)()
+    for _ in range(2):
+        L.medyan_mech_evaluate(h, xptr, C.byref(etot), per, fptr)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(K):
+        st = L.medyan_mech_evaluate(h, xptr, C.byref(etot), per, fptr)
+        if st not in (0, 3):
+            raise RuntimeError(f"medyan_mech_evaluate status {st}")
+    e2e_t = time.perf_counter() - t0
+
+    # accuracy of this precision against the FP64 path on the same inputs
+    ff64 = make("fp64") if args.precision != "fp64" else ff
+    e64, per64, f64 = ff64.evaluate(x)
+    e_, per_, f_ = ff.evaluate(x)
+    rel_force_err = float(np.abs(f_ - f64).max() / np.abs(f64).max())
+    rel_energy_err = float(abs(e_ - e64) / abs(e64))
+
+    result = {
+        "metric": METRIC,
+        "value": world * K / t_step,
+        "unit": "force-evals/s",
+        "n_gpus": world,
+        "steps": K,
+        "warmup": max(args.warmup, 3),
+        "ms_per_step": 1e3 * t_step / K,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32+f64" if args.precision == "mixed" else "f64",
+        "data": "synthetic (seeded network generator, reference initializer rules)",
+        "config": {"workload": WORKLOAD, "precision": args.precision, "n_beads": net.n_beads,
+                   "interactions": counts, "l2": "flushed (256 MiB write) before each timed step",
+                   "step": "total energy + forces of all force fields", "parallelism": f"replicas x{world}"},
+        "e2e": {"value": world * K / e2e_t, "unit": "force-evals/s", "h2d_bytes_per_step": 8 * x.size,
+                "d2h_bytes_per_step": 8 * x.size + 8 * 11},
+        "gpu_launches": K * 6,
+        "clocks": clocks.summary(),
+        "wall_s_timed_region": wall,
+        "accuracy_vs_fp64": {"rel_force_err": rel_force_err, "rel_energy_err": rel_energy_err},
+        "breakdown_ms": {"forces": 1e3 * sum(t_force) / K, "energy": 1e3 * sum(t_energy) / K},
+    }
+    fb = abytes["forces"]
+    t_f = sum(t_force) / K
+    result["roofline"] = roofline(fb / t_f / 1e9, fb)
+    result["algorithmic_bytes"] = abytes
+
+    if not args.no_minimize and rank == 0:
+        result["minimization"] = minimize_extras(net, make)
+    for f in {id(ff): ff, id(ff64): ff64}.values():
+        f.close()
+    return result
+
+
+def roofline(achieved_gbs: float, nbytes: int) -> dict:
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak, src = 6650.0, "fallback"
+    if os.path.exists(peaks_path):
+        with open(peaks_path) as fh:
+            peak, src = float(json.load(fh)["hbm_gbs"]), "measured"
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "force_pass_traffic.json")
+    if os.path.exists(prof):
+        with open(prof) as fh:
+            traffic = json.load(fh).get("bytes_per_launch")
+    return {"bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s", "frac": achieved_gbs / peak,
+            "traffic": traffic, "peak_source": src, "kernel": "force pass (bonded + excluded-volume kernels)",
+            "algorithmic_bytes_per_launch": nbytes}
+
+
+def minimize_extras(net, make) -> dict:
+    """One timed minimization (gradTol 1 pN, reference example CG params) per
+    precision on the same network: minimizations/s and the final-energy match."""
+    import torch
+
+    from medyan_b200.forcefield import conjugate_gradient_params
+    out = {}
+    p = conjugate_gradient_params(grad_tol=1.0, max_dist=1.0, lambda_max=0.01, energy_rel_tol=1e-9)
+    x = net.flat_coords()
+    for prec in ("fp64", "mixed"):
+        ff = make(prec)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        st, xm, fm, r = ff.minimize(x, p)
+        dt = time.perf_counter() - t0
+        out[prec] = {"status": st, "seconds": dt, "minimizations_per_s": 1.0 / dt, "iterations": r.num_iter,
+                     "energy_calls": r.num_energy_call, "force_calls": r.num_force_call,
+                     "energy_before": r.energy_before_total, "energy_after": r.energy_after_total,
+                     "grad_inf_norm": r.grad_inf_norm, "energy_rel_change": r.energy_rel_change}
+        ff.close()
+    if "fp64" in out and "mixed" in out:
+        e64, em = out["fp64"]["energy_after"], out["mixed"]["energy_after"]
+        out["final_energy_rel_diff_mixed_vs_fp64"] = abs(em - e64) / abs(e64)
+    return out
+
+
+# -------------------------------------------------------- CPU (reference)
+def cpu_reference_fns(net):
+    """energy() and forces() of the reference's compiled kernels
+    (oracle/_ref/libmedyan_ref.so, -O2 -ffast-math as the reference builds)
+    on the network, or of the oracle port when that build is absent."""
+    import ctypes as C
+
+    import numpy as np
+
+    from oracle.oracle import Oracle, Reference
+    orc = Oracle()
+    st, extra = orc.complete(net)
+    sv = net.system_view(**extra)
+    x = net.flat_coords()
+    f = np.zeros_like(x)
+    pd = C.POINTER(C.c_double)
+    if Reference.available():
+        ref = Reference()
+        hnd = ref.lib.medyan_ref_prepare(sv.ref())
+        keep = (sv, x, f, ref)
+
+        def energy():
+            return ref.lib.medyan_ref_prepared_energy(hnd, keep[1].ctypes.data_as(pd), None)
+
+        def forces():
+            ref.lib.medyan_ref_prepared_forces(hnd, keep[1].ctypes.data_as(pd), keep[2].ctypes.data_as(pd))
+        return energy, forces, "reference"
+    return (lambda: orc.energy(sv, x)), (lambda: orc.forces(sv, x)), "port"
+
+
+def cpu_reference_rate(net, sample_s: float):
+    """Energy + forces per second on one host thread over a bounded sample."""
+    energy, forces, kind = cpu_reference_fns(net)
+    energy()
+    forces()
+    n = 0
+    t0 = time.perf_counter()
+    while True:
+        energy()
+        forces()
+        n += 1
+        dt = time.perf_counter() - t0
+        if dt >= sample_s or n >= 10000:
+            break
+    return n / dt, n, dt, kind
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        if args.impl == "ours":
+            torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        dist.init_process_group("nccl" if args.impl == "ours" else "gloo", timeout=timedelta(seconds=600))
+
+    if args.impl == "reference":
+        if rank == 0:
+            net = build_network()
+            energy, forces, kind = cpu_reference_fns(net)
+            for _ in range(args.warmup):
+                energy()
+                forces()
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                energy()
+                forces()
+            dt = time.perf_counter() - t0
+            rate = args.steps / dt
+            line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": "force-evals/s", "n_gpus": 0,
+                    "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+                    "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                    "data": "synthetic (seeded network generator, reference initializer rules)",
+                    "config": {"workload": WORKLOAD, "step": "total energy + forces of all force fields"},
+                    "cpu_baseline": {"value": rate, "unit": "force-evals/s", "cores": 1, "kind": kind,
+                                     "sample": f"{args.steps} energy+force evaluations of the full network "
+                                               f"in {dt:.1f} s (single-threaded, as the reference)"},
+                    "e2e": {"value": rate, "unit": "force-evals/s", "h2d_bytes_per_step": 0,
+                            "d2h_bytes_per_step": 0}}
+            print(json.dumps(line), flush=True)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+
+    result = run_ours(args, rank, world)
+    if rank == 0:
+        net = build_network()
+        rate, n, dt, kind = cpu_reference_rate(net, args.cpu_sample_s)
+        result["cpu_baseline"] = {"value": rate, "unit": "force-evals/s", "cores": 1, "kind": kind,
+                                  "sample": f"{n} energy+force evaluations of the full network in {dt:.1f} s"}
+        print(json.dumps(result), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -218,6 +218,7 @@ medyan_status refresh_device_ff(medyan_mech* h) {
     cudaError_t e = h->partial.reserve(need);
     if (e != cudaSuccess) return cuda_status(e);
     h->es.partial = h->partial.ptr();
+    h->ff_gen++;
     return MEDYAN_OK;
 }
 
@@ -229,8 +230,8 @@ medyan_status sync_status(medyan_mech* h) {
 
 // Energy at x (+ lam*d when d is set) for the lambda set in device memory;
 // results land in h->es.out.
-void enqueue_energy(medyan_mech* h, const double* x, const double* d, const LambdaSet* lam) {
-    launch_energy(h->ff, h->prec, x, d, lam, h->es, h->stream);
+void enqueue_energy(medyan_mech* h, const double* x, const double* d, const LambdaSet* lam, cudaStream_t s) {
+    launch_energy(h->ff, h->prec, x, d, lam, h->es, s);
 }
 
 void enqueue_forces(medyan_mech* h, const double* x, double* f) {
@@ -277,6 +278,7 @@ medyan_status medyan_mech::init() {
 medyan_mech::~medyan_mech() {
     cudaSetDevice(device);
     if (stream) cudaStreamSynchronize(stream);
+    if (cg_graph) cudaGraphExecDestroy(cg_graph);
     destroy_nl(this);
     if (stream) cudaStreamDestroy(stream);
 }
@@ -360,7 +362,7 @@ medyan_status medyan_mech_get_coords(medyan_mech* h, double* coord) {
 
 medyan_status medyan_mech_energy(medyan_mech* h, double* e_total, double* e_per_ff) {
     if (!h || !e_total) return MEDYAN_ERR_INVALID_ARG;
-    enqueue_energy(h, h->x.ptr(), nullptr, h->lam_zero.ptr());
+    enqueue_energy(h, h->x.ptr(), nullptr, h->lam_zero.ptr(), h->stream);
     double out[MEDYAN_FF_COUNT + 1];
     cudaError_t e = cudaMemcpyAsync(out, h->energy_out.ptr(), sizeof out, cudaMemcpyDeviceToHost, h->stream);
     if (e != cudaSuccess) return cuda_status(e);
@@ -388,7 +390,7 @@ medyan_status medyan_mech_forces(medyan_mech* h, double* force_out) {
 
 medyan_status medyan_mech_enqueue_energy(medyan_mech* h) {
     if (!h) return MEDYAN_ERR_INVALID_ARG;
-    enqueue_energy(h, h->x.ptr(), nullptr, h->lam_zero.ptr());
+    enqueue_energy(h, h->x.ptr(), nullptr, h->lam_zero.ptr(), h->stream);
     return cuda_status(cudaGetLastError());
 }
 
@@ -425,7 +427,7 @@ medyan_status medyan_mech_evaluate(medyan_mech* h, const double* coord, double* 
     const size_t bytes = sizeof(double) * 3 * (size_t)h->n_beads;
     cudaError_t e = cudaMemcpyAsync(h->x.ptr(), coord, bytes, cudaMemcpyHostToDevice, h->stream);
     if (e != cudaSuccess) return cuda_status(e);
-    enqueue_energy(h, h->x.ptr(), nullptr, h->lam_zero.ptr());
+    enqueue_energy(h, h->x.ptr(), nullptr, h->lam_zero.ptr(), h->stream);
     enqueue_forces(h, h->x.ptr(), h->f.ptr());
     double out[MEDYAN_FF_COUNT + 1];
     int status = 0;

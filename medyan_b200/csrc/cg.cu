@@ -1,8 +1,620 @@
-// cg.cu — device-resident conjugate-gradient minimizer (placeholder).
+// cg.cu — the conjugate-gradient minimizer on the device.
+//
+// CGMethod::minimize (src/Mechanics/Minimizer/CGMethod.hpp:826-1743) with its
+// backtracking line search (:238-373), safe mode and MController's recovery
+// step (src/Controller/MController.h:273-339). Every scalar of the method
+// (lambda, beta, the dot products, counters and flags) lives in a device
+// CGState; single-thread logic runs in the last block of each vector pass or in
+// a one-thread kernel, so an iteration never waits on the host.
+//
+// One iteration:
+//   line-search passes: energy at up to kMaxLambda step sizes lam_k = lam*2^-k
+//     from one read of x and d, then `decide` replays the reference's
+//     sequential Armijo loop over them (so the accepted lambda and the energy
+//     call count are the reference's);
+//   force pass at x + lam*d into the force buffer that does not hold the
+//     current force;
+//   dots pass: commit x += lam*d, F.F, F.Fprev, max|F|, zero the old buffer;
+//     its last block computes beta (PR: max(0, (F.F - F.Fprev)/lastF.F));
+//   direction pass: d = F + beta*d (or F), d.F, max|d|; its last block checks
+//     d.F <= 0 (reset), convergence and call limits, and prepares the next
+//     line search;
+//   reset pass (only when flagged): d = F.
+// Energy at the start of a line search is the accepted energy of the
+// previous one (same coordinates, same deterministic reduction); it is
+// counted as an energy call as in the reference.
+//
+// The iteration runs as a CUDA graph whose loops are conditional WHILE nodes
+// (line-search passes inside, iterations outside), so a whole minimization is
+// one graph launch. The host only reads the result.
+#include <cstring>
+#include <vector>
+
+#include "device_math.cuh"
 #include "handle.h"
 
-extern "C" {
-medyan_status medyan_cg_minimize(medyan_mech*, const medyan_cg_params*, double*, double*, medyan_min_result*) {
-    return MEDYAN_ERR_UNSUPPORTED;
+namespace mb {
+
+namespace {
+
+constexpr int kVecThreads = 256;
+constexpr double kLambdaTol = 1e-8;      // CGMethod::LAMBDATOL (double build)
+constexpr double kBacktrackSlope = 0.4;  // CGMethod::BACKTRACKSLOPE
+constexpr int kOut = MEDYAN_FF_COUNT + 1;
+
+int vec_blocks(int n3) {
+    int b = (n3 + kVecThreads - 1) / kVecThreads;
+    if (b > 148 * 8) b = 148 * 8;
+    return b < 1 ? 1 : b;
 }
+
+// ---------------------------------------------------------------- scalars
+__device__ __forceinline__ double dmin_ref(double a, double b) { return (b < a) ? b : a; }  // std::min
+__device__ __forceinline__ double dmax_ref(double a, double b) { return (a < b) ? b : a; }  // std::max
+
+__device__ void fill_pass(CGState& s, LambdaSet& L) {
+    int k = 0;
+    if (s.need_e0) L.lam[k++] = 0.0;
+    const int want = s.ls_first_pass ? max(1, s.last_backtracks + 1) : kMaxLambda;
+    double lam = s.lam_next;
+    int trials = 0;
+    while (k < kMaxLambda && trials < want) {
+        L.lam[k++] = lam;
+        ++trials;
+        lam *= 0.5;
+        if (lam <= 0.0 || lam <= kLambdaTol) break;  // a further trial would already be a failure
+    }
+    L.K = k;
+    s.k_trials = trials;
+}
+
+// Start of a line search (CGMethod.hpp:1316-1324 and :238-262).
+__device__ void begin_line_search(CGState& s, LambdaSet& L) {
+    s.num_iter++;
+    s.ls_active = 1;
+    s.ls_first_pass = 1;
+    s.backtracks = 0;
+    s.skip_force = 1;
+    s.move_kind = 0;
+    s.reduced_slope = (s.safe_mode ? 0.0 : kBacktrackSlope) * s.slope;
+    if (s.grad_inf_norm == 0.0) {  // "return zero if no forces": lambda 0, no energy call
+        s.ls_immediate_fail = 1;
+        L.K = 0;
+        return;
+    }
+    s.lam_next = dmin_ref(s.lambda_max, s.max_dist / s.grad_inf_norm);
+    fill_pass(s, L);
+}
+
+// Line search returned lambda = 0 (CGMethod.hpp:1337-1367).
+__device__ void line_search_failed(CGState& s) {
+    if (!s.try_to_recover) {
+        s.error_flags |= 1;
+        s.status = MEDYAN_ERR_LINE_SEARCH;
+        s.done = 1;
+        s.skip_force = 1;
+        return;
+    }
+    if (s.safe_mode) {
+        // funcRecoveryOnError: step = min over coordinates of maxDist/|d_i|
+        // = maxDist / max|d_i| (division is monotone), then reset, safe mode off.
+        if (!(s.dmax > 0.0)) {
+            s.status = MEDYAN_ERR_NONFINITE;  // the reference throws "Invalid step size"
+            s.done = 1;
+            s.skip_force = 1;
+            return;
+        }
+        s.lam_move = s.max_dist / s.dmax;
+        s.move_kind = 2;
+        s.skip_force = 0;
+    } else {
+        s.skip_force = 1;  // resetCGParams, safe mode on; no new force needed
+        s.move_kind = 0;
+        s.dir_mode = 1;
+        s.safe_mode = 1;
+    }
+}
+
+// After an energy pass: the reference's backtracking loop over the evaluated
+// trial lambdas (CGMethod.hpp:264-362).
+__global__ void k_ls_decide(CGState* __restrict__ st, LambdaSet* __restrict__ L, const double* __restrict__ out) {
+    CGState& s = *st;
+    s.reset_after_dir = 0;
+    if (s.done || !s.ls_active) {
+        L->K = 0;
+        return;
+    }
+    if (s.ls_immediate_fail) {
+        s.ls_immediate_fail = 0;
+        s.ls_active = 0;
+        s.last_backtracks = 0;
+        line_search_failed(s);
+        L->K = 0;
+        return;
+    }
+    int slot = 0;
+    if (s.need_e0) {
+        s.E_cur = out[kOut - 1];
+        s.need_e0 = 0;
+        slot = 1;
+    }
+    if (s.ls_first_pass) {
+        s.num_energy_call++;  // currentEnergy = energyFunc(coord)
+        s.ls_first_pass = 0;
+    }
+    for (; slot < L->K; ++slot) {
+        double lam = L->lam[slot];
+        double E_lam = out[slot * kOut + kOut - 1];
+        s.num_energy_call++;
+        const double ideal = -s.reduced_slope * lam;
+        bool decided = false;
+        if (lam < 0 || ideal > 0) {
+            decided = true;
+            lam = 0.0;
+        }
+        const double dE = E_lam - s.E_cur;
+        if (dE <= ideal) decided = true;
+        else lam *= 0.5;
+        if (lam <= 0.0 || lam <= kLambdaTol) {
+            decided = true;
+            lam = 0.0;
+            E_lam = s.E_cur;
+        }
+        if (decided) {
+            s.total_energy = E_lam;
+            s.ls_active = 0;
+            s.last_backtracks = s.backtracks;
+            L->K = 0;
+            if (lam == 0.0) {
+                line_search_failed(s);
+            } else {
+                s.lam_move = lam;
+                s.E_new = E_lam;
+                s.move_kind = 1;
+                s.skip_force = 0;
+            }
+            return;
+        }
+        s.backtracks++;
+        s.lam_next = lam;
+    }
+    fill_pass(s, *L);  // undecided: evaluate the next halvings
+}
+
+// ----------------------------------------------------------- vector passes
+__device__ __forceinline__ void block_reduce3(double& a, double& b, double& m, double* sm) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_down_sync(0xffffffffu, a, o);
+        b += __shfl_down_sync(0xffffffffu, b, o);
+        m = dmax_ref(m, __shfl_down_sync(0xffffffffu, m, o));
+    }
+    if (lane == 0) {
+        sm[warp] = a;
+        sm[32 + warp] = b;
+        sm[64 + warp] = m;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        a = lane < nw ? sm[lane] : 0.0;
+        b = lane < nw ? sm[32 + lane] : 0.0;
+        m = lane < nw ? sm[64 + lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_down_sync(0xffffffffu, a, o);
+            b += __shfl_down_sync(0xffffffffu, b, o);
+            m = dmax_ref(m, __shfl_down_sync(0xffffffffu, m, o));
+        }
+    }
+    __syncthreads();
+}
+
+// Returns true in exactly one block: the last to finish (sums then visible).
+__device__ __forceinline__ bool last_block(unsigned int* ticket) {
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    __syncthreads();
+    return last;
+}
+
+// Sums the per-block partials in block order (deterministic).
+__device__ void reduce_partials(const double* __restrict__ part, int nblk, double& a, double& b, double& m,
+                                double* sm) {
+    a = 0.0;
+    b = 0.0;
+    m = 0.0;
+    for (int q = threadIdx.x; q < nblk; q += blockDim.x) {
+        a += __ldcg(part + 4 * q);
+        b += __ldcg(part + 4 * q + 1);
+        m = dmax_ref(m, __ldcg(part + 4 * q + 2));
+    }
+    block_reduce3(a, b, m, sm);
+}
+
+// dots pass: commit the move, F.F, F.Fprev, max|F|, zero the old force buffer.
+__global__ void __launch_bounds__(kVecThreads) k_cg_dots(int n3, double* __restrict__ x, const double* __restrict__ d,
+                                                         double* __restrict__ f0, double* __restrict__ f1,
+                                                         CGState* __restrict__ st, double* __restrict__ part) {
+    __shared__ double sm[96];
+    if (st->done || st->skip_force) return;
+    const int parity = st->parity;
+    const double* __restrict__ Fn = parity ? f0 : f1;  // new force (written by the force pass)
+    double* __restrict__ Fo = parity ? f1 : f0;        // force at the previous point
+    const double lam = st->lam_move;
+    double a = 0.0, b = 0.0, m = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x) {
+        x[i] = move1(x[i], lam, d[i]);
+        const double fn = Fn[i], fo = Fo[i];
+        a += fn * fn;
+        b += fn * fo;
+        m = dmax_ref(m, fabs(fn));
+        Fo[i] = 0.0;
+    }
+    block_reduce3(a, b, m, sm);
+    if (threadIdx.x == 0) {
+        part[4 * blockIdx.x] = a;
+        part[4 * blockIdx.x + 1] = b;
+        part[4 * blockIdx.x + 2] = m;
+    }
+    if (!last_block(&st->ticket_dots)) return;
+    reduce_partials(part, gridDim.x, a, b, m, sm);
+    if (threadIdx.x != 0) return;
+    CGState& s = *st;
+    s.ticket_dots = 0;
+    s.num_force_call++;
+    s.grad_inf_norm = m;  // maxF (CGMethod.hpp:202-212)
+    if (isinf(m)) {
+        s.status = MEDYAN_ERR_NONFINITE;  // "maxF is infinity"
+        s.done = 1;
+    }
+    s.new_grad = a;
+    s.prev_grad = b;
+    if (s.move_kind == 1) {
+        s.energy_rel_change = fabs(s.E_new - s.prev_energy) / fabs(s.prev_energy);
+        s.prev_energy = s.E_new;
+        s.E_cur = s.E_new;
+        s.need_e0 = 0;
+        if (s.method == MEDYAN_CG_POLAK_RIBIERE) s.beta = dmax_ref(0.0, (s.new_grad - s.prev_grad) / s.last_fdotf);
+        else if (s.method == MEDYAN_CG_FLETCHER_RIEVES) s.beta = s.new_grad / s.last_fdotf;
+        else s.beta = 0.0;
+        s.dir_mode = 0;
+        // copycoordsifminimumE (CGMethod.hpp:1564-1566)
+        s.copy_min_e = 0;
+        if (m <= 10 * s.grad_tol && s.num_iter > s.force_call_limit / 2 && s.total_energy <= s.min_e) {
+            s.min_e = s.total_energy;
+            s.copy_min_e = 1;
+            s.have_min_e = 1;
+        }
+    } else {
+        // setup (move_kind 0) or recovery step (2): resetCGParams follows
+        if (s.move_kind == 2) {
+            s.need_e0 = 1;
+            s.safe_mode = 0;
+        }
+        s.dir_mode = 1;
+        s.copy_min_e = 0;
+    }
+    s.parity ^= 1;
+    s.skip_force = 1;
+}
+
+// direction pass: d = F + beta*d (dir_mode 0) or d = F + 0*d (1), d.F, max|d|.
+__global__ void __launch_bounds__(kVecThreads) k_cg_dir(int n3, const double* __restrict__ x, double* __restrict__ d,
+                                                        const double* __restrict__ f0, const double* __restrict__ f1,
+                                                        CGState* __restrict__ st, double* __restrict__ part,
+                                                        double* __restrict__ min_e, LambdaSet* __restrict__ L) {
+    __shared__ double sm[96];
+    if (st->done || st->ls_active) return;
+    const double* __restrict__ F = st->parity ? f1 : f0;
+    const double beta = st->dir_mode ? 0.0 : st->beta;
+    const bool copy = st->copy_min_e;
+    double a = 0.0, b = 0.0, m = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x) {
+        const double fi = F[i];
+        const double dn = fi + beta * d[i];  // shiftSearchDir (CGMethod.cpp:356-360)
+        d[i] = dn;
+        a += dn * fi;
+        m = dmax_ref(m, fabs(dn));
+        if (copy) min_e[i] = x[i];
+    }
+    block_reduce3(a, b, m, sm);
+    if (threadIdx.x == 0) {
+        part[4 * blockIdx.x] = a;
+        part[4 * blockIdx.x + 1] = 0.0;
+        part[4 * blockIdx.x + 2] = m;
+    }
+    if (!last_block(&st->ticket_dir)) return;
+    reduce_partials(part, gridDim.x, a, b, m, sm);
+    if (threadIdx.x != 0) return;
+    CGState& s = *st;
+    s.ticket_dir = 0;
+    s.copy_min_e = 0;
+    s.dmax = m;
+    if (s.dir_mode == 0 && a <= 0) {
+        // conjugacy lost: resetCGParams (d = F; its d.F is F.F)
+        s.reset_after_dir = 1;
+        s.slope = s.new_grad;
+        s.dmax = s.grad_inf_norm;
+    } else {
+        s.slope = a;
+    }
+    if (s.method != MEDYAN_CG_STEEPEST) s.last_fdotf = s.new_grad;
+    s.dir_mode = 0;
+    // loop condition (CGMethod.hpp:1279-1282)
+    const bool limit = (s.energy_call_limit != 0 && s.num_energy_call > s.energy_call_limit) ||
+                       (s.force_call_limit != 0 && s.num_force_call > s.force_call_limit);
+    const bool conv = s.grad_inf_norm < s.grad_tol || s.energy_rel_change < s.energy_rel_tol;
+    if (limit || conv) {
+        s.done = 1;
+        s.call_limit = limit;
+        L->K = 0;
+    } else {
+        begin_line_search(s, *L);
+    }
+}
+
+__global__ void __launch_bounds__(kVecThreads) k_cg_reset_dir(int n3, double* __restrict__ d,
+                                                              const double* __restrict__ f0,
+                                                              const double* __restrict__ f1,
+                                                              const CGState* __restrict__ st) {
+    if (!st->reset_after_dir) return;
+    const double* __restrict__ F = st->parity ? f1 : f0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x)
+        d[i] = F[i] + 0.0 * d[i];
+}
+
+// energiesBefore / energiesAfter from a standalone energy pass.
+__global__ void k_cg_record_energy(CGState* __restrict__ st, const double* __restrict__ out,
+                                   double* __restrict__ dst, int before) {
+    CGState& s = *st;
+    double tot = 0.0;
+    for (int i = 0; i < MEDYAN_FF_COUNT; ++i) {
+        dst[i] = out[i];
+        tot += out[i];  // computeIndividualEnergies sums without the -1 rule
+    }
+    dst[MEDYAN_FF_COUNT] = tot;
+    s.num_energy_call++;
+    if (before) {
+        s.prev_energy = tot;
+        s.need_e0 = 1;
+    }
+}
+
+// Condition kernels for the graph's WHILE nodes.
+__global__ void k_cond_ls(const CGState* __restrict__ st, cudaGraphConditionalHandle h) {
+    cudaGraphSetConditional(h, (!st->done && st->ls_active) ? 1u : 0u);
+}
+__global__ void k_cond_arm_ls(const CGState* __restrict__ st, cudaGraphConditionalHandle h) {
+    cudaGraphSetConditional(h, (!st->done && st->ls_active) ? 1u : 0u);
+}
+__global__ void k_cond_iter(const CGState* __restrict__ st, cudaGraphConditionalHandle h) {
+    cudaGraphSetConditional(h, st->done ? 0u : 1u);
+}
+
+}  // namespace
+
+// ----------------------------------------------------------------- host side
+namespace {
+
+struct CGLaunch {
+    medyan_mech* h;
+    int n3, vb;
+    double *x, *d, *f0, *f1, *part, *minE;
+    CGState* st;
+    LambdaSet* L;
+    ForceTarget tgt;
+};
+
+CGLaunch make_launch(medyan_mech* h) {
+    CGLaunch c{};
+    c.h = h;
+    c.n3 = 3 * h->n_beads;
+    c.vb = vec_blocks(c.n3);
+    c.x = h->x.raw();
+    c.d = h->cg_dir.raw();
+    c.f0 = h->f.raw();
+    c.f1 = h->cg_force2.raw();
+    c.part = h->cg_part.raw();
+    c.minE = h->cg_min_coords.raw();
+    c.st = h->cg_state.raw();
+    c.L = h->cg_lam.raw();
+    c.tgt = ForceTarget{c.f0, c.f1, &c.st->parity, &c.st->skip_force, c.d, &c.st->lam_move};
+    return c;
+}
+
+void enqueue_ls_pass(const CGLaunch& c, cudaStream_t s) {
+    enqueue_energy(c.h, c.x, c.d, c.L, s);
+    k_ls_decide<<<1, 1, 0, s>>>(c.st, c.L, c.h->energy_out.raw());
+}
+
+void enqueue_step(const CGLaunch& c, cudaStream_t s) {
+    launch_forces_target(c.h->ff, c.h->prec, c.x, c.tgt, c.h->fs, s);
+    k_cg_dots<<<c.vb, kVecThreads, 0, s>>>(c.n3, c.x, c.d, c.f0, c.f1, c.st, c.part);
+    k_cg_dir<<<c.vb, kVecThreads, 0, s>>>(c.n3, c.x, c.d, c.f0, c.f1, c.st, c.part, c.minE, c.L);
+    k_cg_reset_dir<<<c.vb, kVecThreads, 0, s>>>(c.n3, c.d, c.f0, c.f1, c.st);
+}
+
+// Whole minimization loop as one graph: WHILE(iter) { WHILE(ls) { pass }; step }.
+cudaError_t build_graph(const CGLaunch& c, cudaGraphExec_t* exec) {
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaGraphCreate(&g, 0);
+    if (e != cudaSuccess) return e;
+    cudaGraphConditionalHandle h_iter, h_ls;
+    e = cudaGraphConditionalHandleCreate(&h_iter, g, 1, cudaGraphCondAssignDefault);
+    cudaGraphNode_t n_iter;
+    cudaGraphNodeParams p_iter = {};
+    if (e == cudaSuccess) {
+        p_iter.type = cudaGraphNodeTypeConditional;
+        p_iter.conditional.handle = h_iter;
+        p_iter.conditional.type = cudaGraphCondTypeWhile;
+        p_iter.conditional.size = 1;
+        e = cudaGraphAddNode(&n_iter, g, nullptr, 0, &p_iter);
+    }
+    cudaGraph_t body = e == cudaSuccess ? p_iter.conditional.phGraph_out[0] : nullptr;
+    cudaStream_t s = nullptr;
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    // iteration body: arm the line-search condition, the line-search loop,
+    // then the step kernels and the iteration condition
+    if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&h_ls, body, 0, 0);
+    cudaGraphNode_t n_arm = nullptr;
+    if (e == cudaSuccess) {
+        e = cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed);
+        if (e == cudaSuccess) {
+            k_cond_arm_ls<<<1, 1, 0, s>>>(c.st, h_ls);
+            cudaGraph_t tmp;
+            e = cudaStreamEndCapture(s, &tmp);
+        }
+        size_t nn = 0;
+        if (e == cudaSuccess) e = cudaGraphGetNodes(body, nullptr, &nn);
+        if (e == cudaSuccess && nn == 1) e = cudaGraphGetNodes(body, &n_arm, &nn);
+        if (e == cudaSuccess && !n_arm) e = cudaErrorUnknown;
+    }
+    cudaGraphNode_t n_ls;
+    cudaGraphNodeParams p_ls = {};
+    if (e == cudaSuccess) {
+        p_ls.type = cudaGraphNodeTypeConditional;
+        p_ls.conditional.handle = h_ls;
+        p_ls.conditional.type = cudaGraphCondTypeWhile;
+        p_ls.conditional.size = 1;
+        e = cudaGraphAddNode(&n_ls, body, &n_arm, 1, &p_ls);
+    }
+    if (e == cudaSuccess) {
+        cudaGraph_t ls_body = p_ls.conditional.phGraph_out[0];
+        e = cudaStreamBeginCaptureToGraph(s, ls_body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed);
+        if (e == cudaSuccess) {
+            enqueue_ls_pass(c, s);
+            k_cond_ls<<<1, 1, 0, s>>>(c.st, h_ls);
+            cudaGraph_t tmp;
+            e = cudaStreamEndCapture(s, &tmp);
+        }
+    }
+    if (e == cudaSuccess) {
+        const cudaGraphNode_t deps[1] = {n_ls};
+        e = cudaStreamBeginCaptureToGraph(s, body, deps, nullptr, 1, cudaStreamCaptureModeRelaxed);
+        if (e == cudaSuccess) {
+            enqueue_step(c, s);
+            k_cond_iter<<<1, 1, 0, s>>>(c.st, h_iter);
+            cudaGraph_t tmp;
+            e = cudaStreamEndCapture(s, &tmp);
+        }
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(exec, g, 0);
+    if (s) cudaStreamDestroy(s);
+    cudaGraphDestroy(g);
+    return e;
+}
+
+}  // namespace
+
+}  // namespace mb
+
+using namespace mb;
+
+extern "C" medyan_status medyan_cg_minimize(medyan_mech* h, const medyan_cg_params* p, double* coord_inout,
+                                            double* force_out, medyan_min_result* out) {
+    if (!h || !p || !coord_inout) return MEDYAN_ERR_INVALID_ARG;
+    if (p->method < 0 || p->method > 2 || !(p->max_dist > 0) || !(p->lambda_max > 0)) return MEDYAN_ERR_INVALID_ARG;
+    const int n3 = 3 * h->n_beads;
+    cudaStream_t s = h->stream;
+    cudaError_t e = h->cg_dir.reserve(n3 ? n3 : 1);
+    if (e == cudaSuccess) e = h->cg_force2.reserve(n3 ? n3 : 1);
+    if (e == cudaSuccess) e = h->cg_min_coords.reserve(n3 ? n3 : 1);
+    if (e == cudaSuccess) e = h->cg_part.reserve(4 * (size_t)vec_blocks(n3) + 4);
+    if (e == cudaSuccess) e = h->cg_eout.reserve(2 * kOut);
+    if (e == cudaSuccess) e = h->cg_state.reserve(1);
+    if (e == cudaSuccess) e = h->cg_lam.reserve(1);
+    if (e != cudaSuccess) return cuda_status(e);
+    const size_t bytes = sizeof(double) * (size_t)n3;
+    CGLaunch c = make_launch(h);
+
+    CGState s0{};
+    s0.method = p->method;
+    s0.try_to_recover = p->try_to_recover;
+    s0.energy_call_limit = p->energy_call_limit;
+    s0.force_call_limit = p->force_call_limit > 3 * h->n_beads ? p->force_call_limit : 3 * h->n_beads;
+    s0.max_dist = p->max_dist;
+    s0.lambda_max = p->lambda_max;
+    s0.grad_tol = p->grad_tol;
+    s0.energy_rel_tol = p->energy_rel_tol;
+    s0.status = MEDYAN_OK;
+    s0.parity = 1;  // the first force lands in f0
+    s0.grad_inf_norm = __builtin_inf();
+    s0.energy_rel_change = __builtin_inf();
+    s0.min_e = __builtin_inf();
+    s0.lam_move = 0.0;
+    s0.skip_force = 0;
+    s0.move_kind = 0;
+    LambdaSet l0{};
+    e = cudaMemcpyAsync(c.x, coord_inout, bytes, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(c.st, &s0, sizeof s0, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(c.L, &l0, sizeof l0, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c.d, 0, bytes ? bytes : 8, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c.f0, 0, bytes ? bytes : 8, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c.f1, 0, bytes ? bytes : 8, s);
+    if (e != cudaSuccess) return cuda_status(e);
+
+    // energiesBefore, then the first force (parity 1 -> f0), F.F, d = F.
+    enqueue_energy(h, c.x, nullptr, h->lam_zero.raw(), s);
+    k_cg_record_energy<<<1, 1, 0, s>>>(c.st, h->energy_out.raw(), h->cg_eout.raw(), 1);
+    enqueue_step(c, s);
+
+    // main loop: one graph launch
+    // the graph captures the force-field records by value: rebuild it after
+    // any re-vectorization (generation counter) or precision change
+    if (h->cg_graph && (h->cg_graph_gen != h->ff_gen || h->cg_graph_prec != h->prec)) {
+        cudaGraphExecDestroy(h->cg_graph);
+        h->cg_graph = nullptr;
+    }
+    if (!h->cg_graph) {
+        e = build_graph(c, &h->cg_graph);
+        if (e != cudaSuccess) return cuda_status(e);
+        h->cg_graph_gen = h->ff_gen;
+        h->cg_graph_prec = h->prec;
+    }
+    e = cudaGraphLaunch(h->cg_graph, s);
+    if (e != cudaSuccess) return cuda_status(e);
+
+    CGState sf{};
+    e = cudaMemcpyAsync(&sf, c.st, sizeof sf, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_status(e);
+    if (sf.status == MEDYAN_ERR_LINE_SEARCH) {
+        // errorLineSearch: return at once, coordinates as they are
+        cudaMemcpyAsync(coord_inout, c.x, bytes, cudaMemcpyDeviceToHost, s);
+        if (force_out) cudaMemcpyAsync(force_out, sf.parity ? c.f1 : c.f0, bytes, cudaMemcpyDeviceToHost, s);
+    } else {
+        if (sf.call_limit && sf.have_min_e) cudaMemcpyAsync(c.x, c.minE, bytes, cudaMemcpyDeviceToDevice, s);
+        enqueue_energy(h, c.x, nullptr, h->lam_zero.raw(), s);
+        k_cg_record_energy<<<1, 1, 0, s>>>(c.st, h->energy_out.raw(), h->cg_eout.raw() + kOut, 0);
+        cudaMemcpyAsync(coord_inout, c.x, bytes, cudaMemcpyDeviceToHost, s);
+        if (force_out) cudaMemcpyAsync(force_out, sf.parity ? c.f1 : c.f0, bytes, cudaMemcpyDeviceToHost, s);
+    }
+    double eo[2 * kOut];
+    e = cudaMemcpyAsync(eo, h->cg_eout.raw(), sizeof eo, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&sf, c.st, sizeof sf, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_status(e);
+    if (out) {
+        std::memset(out, 0, sizeof *out);
+        for (int i = 0; i < MEDYAN_FF_COUNT; ++i) {
+            out->energy_before[i] = eo[i];
+            out->energy_after[i] = sf.status == MEDYAN_ERR_LINE_SEARCH ? 0.0 : eo[kOut + i];
+        }
+        out->energy_before_total = eo[MEDYAN_FF_COUNT];
+        out->energy_after_total = sf.status == MEDYAN_ERR_LINE_SEARCH ? 0.0 : eo[kOut + MEDYAN_FF_COUNT];
+        out->error_flags = (uint32_t)sf.error_flags;
+        out->num_energy_call = sf.num_energy_call;
+        out->energy_call_limit = sf.energy_call_limit;
+        out->num_force_call = sf.num_force_call;
+        out->force_call_limit = sf.force_call_limit;
+        out->num_iter = sf.num_iter;
+        out->grad_inf_norm = sf.grad_inf_norm;
+        out->grad_tol = sf.grad_tol;
+        out->energy_rel_change = sf.energy_rel_change;
+        out->energy_rel_tol = sf.energy_rel_tol;
+    }
+    return (medyan_status)sf.status;
 }

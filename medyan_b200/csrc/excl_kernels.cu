@@ -64,15 +64,24 @@ __global__ void __launch_bounds__(kBlock) k_excl_energy(const DeviceFF ff, const
     }
 }
 
+__device__ __forceinline__ V3 pos_at(const double* __restrict__ x, const ForceTarget& t, double lam, int o) {
+    V3 p = load3(x + o);
+    return t.d ? move3(p, lam, load3(t.d + o)) : p;
+}
+
 template <class R>
 __global__ void __launch_bounds__(kBlock) k_excl_forces(const DeviceFF ff, const double* __restrict__ x,
-                                                        double* __restrict__ f, int* __restrict__ fb_count,
+                                                        const ForceTarget tgt, int* __restrict__ fb_count,
                                                         int* __restrict__ fb_list, int* __restrict__ status) {
+    if (tgt.skip && *tgt.skip) return;
     const int i = blockIdx.x * kBlock + threadIdx.x;
     if (i >= ff.n_excl) return;
+    double* __restrict__ f = target_force(tgt);
+    const double lam = tgt.lam ? *tgt.lam : 0.0;
     int4 q = ff.excl_bs[i];
     T3<R> fo[4];
-    if (excl_force<R>(load3(x + q.x), load3(x + q.y), load3(x + q.z), load3(x + q.w), ff.excl_krs[i], fo)) {
+    if (excl_force<R>(pos_at(x, tgt, lam, q.x), pos_at(x, tgt, lam, q.y), pos_at(x, tgt, lam, q.z),
+                      pos_at(x, tgt, lam, q.w), ff.excl_krs[i], fo)) {
         add_force(f, q.x, fo[0].x, fo[0].y, fo[0].z);
         add_force(f, q.y, fo[1].x, fo[1].y, fo[1].z);
         add_force(f, q.z, fo[2].x, fo[2].y, fo[2].z);
@@ -209,16 +218,20 @@ __device__ bool forceN_block(V3 c1, V3 c2, const V3& c3, const V3& c4, double kR
 }
 
 __global__ void __launch_bounds__(kBlock) k_excl_force_fallback(const DeviceFF ff, const double* __restrict__ x,
-                                                                double* __restrict__ f, int* __restrict__ fb_count,
+                                                                const ForceTarget tgt, int* __restrict__ fb_count,
                                                                 const int* __restrict__ fb_list,
                                                                 int* __restrict__ status) {
     extern __shared__ double grid[];  // 10001 abscissae
     __shared__ double red[6 * 32];
     const int n = min(*fb_count, kFallbackCap);
+    if (n == 0) return;
+    double* __restrict__ f = target_force(tgt);
+    const double lam = tgt.lam ? *tgt.lam : 0.0;
     for (int e = 0; e < n; ++e) {
         const int i = fb_list[e];
         const int4 q = ff.excl_bs[i];
-        const V3 c1 = load3(x + q.x), c2 = load3(x + q.y), c3 = load3(x + q.z), c4 = load3(x + q.w);
+        const V3 c1 = pos_at(x, tgt, lam, q.x), c2 = pos_at(x, tgt, lam, q.y), c3 = pos_at(x, tgt, lam, q.z),
+                 c4 = pos_at(x, tgt, lam, q.w);
         double out[4][3];
         bool ok = forceN_block(c1, c2, c3, c4, ff.excl_krs[i], false, grid, red, out);
         if (!ok) ok = forceN_block(c1, c2, c3, c4, ff.excl_krs[i], true, grid, red, out);
@@ -352,13 +365,13 @@ void launch_excl_energy_fallback_and_finish(const DeviceFF& ff, const double* x,
                                          es.fb_count, es.fb_list, es.bad, es.out);
 }
 
-void launch_excl_forces(const DeviceFF& ff, int prec, const double* x, double* f, const ForceScratch& fs,
+void launch_excl_forces(const DeviceFF& ff, int prec, const double* x, const ForceTarget& t, const ForceScratch& fs,
                         cudaStream_t s) {
     const int nbe = excl_blocks(ff);
     if (nbe <= 0) return;
     (void)prec;  // FP64 in both modes, as for the energy
-    k_excl_forces<double><<<nbe, kBlock, 0, s>>>(ff, x, f, fs.fb_count, fs.fb_list, fs.status);
-    k_excl_force_fallback<<<1, kBlock, kForceNGridBytes, s>>>(ff, x, f, fs.fb_count, fs.fb_list, fs.status);
+    k_excl_forces<double><<<nbe, kBlock, 0, s>>>(ff, x, t, fs.fb_count, fs.fb_list, fs.status);
+    k_excl_force_fallback<<<1, kBlock, kForceNGridBytes, s>>>(ff, x, t, fs.fb_count, fs.fb_list, fs.status);
 }
 
 cudaError_t init_excl_kernels() {

@@ -141,9 +141,23 @@ __global__ void __launch_bounds__(kBlock) k_bonded_energy(const DeviceFF ff, con
     }
 }
 
+// Position of the bead at coordinate offset o for a force pass.
+struct PosLoader {
+    const double* __restrict__ x;
+    const double* __restrict__ d;
+    double lam;
+    __device__ __forceinline__ V3 operator()(int o) const {
+        V3 p = load3(x + o);
+        return d ? move3(p, lam, load3(d + o)) : p;
+    }
+};
+
 template <class R>
 __global__ void __launch_bounds__(kBlock) k_bonded_forces(const DeviceFF ff, const double* __restrict__ x,
-                                                          double* __restrict__ f) {
+                                                          const ForceTarget tgt) {
+    if (tgt.skip && *tgt.skip) return;
+    double* __restrict__ f = target_force(tgt);
+    const PosLoader P{x, tgt.d, tgt.lam ? *tgt.lam : 0.0};
     const int b = blockIdx.x;
     const int s = segment_of(ff, b);
     const int i = (b - ff.seg[s]) * kBlock + threadIdx.x;
@@ -152,7 +166,7 @@ __global__ void __launch_bounds__(kBlock) k_bonded_forces(const DeviceFF ff, con
             if (i < ff.n_stretch) {
                 int2 q = ff.stretch_bs[i];
                 double2 p = ff.stretch_p[i];
-                T3<R> F = stretch_force<R>(load3(x + q.x), load3(x + q.y), p.x, p.y);
+                T3<R> F = stretch_force<R>(P(q.x), P(q.y), p.x, p.y);
                 add_force(f, q.y, F.x, F.y, F.z);
                 add_force(f, q.x, -F.x, -F.y, -F.z);
             }
@@ -161,7 +175,7 @@ __global__ void __launch_bounds__(kBlock) k_bonded_forces(const DeviceFF ff, con
             if (i < ff.n_bend) {
                 int4 q = ff.bend_bs[i];
                 double2 p = ff.bend_p[i];
-                V3 c1 = load3(x + q.x), c2 = load3(x + q.y), c3 = load3(x + q.z);
+                V3 c1 = P(q.x), c2 = P(q.y), c3 = P(q.z);
                 T3<R> Fr1, Fr2;
                 bend_force<R>(diff<R>(c1, c2), diff<R>(c2, c3), p.x, p.y, Fr1, Fr2);
                 add_force(f, q.x, -Fr1.x, -Fr1.y, -Fr1.z);
@@ -175,8 +189,7 @@ __global__ void __launch_bounds__(kBlock) k_bonded_forces(const DeviceFF ff, con
             if (i < n) {
                 int4 q = s == 2 ? ff.linker_bs[i] : ff.motor_bs[i];
                 double4 p = s == 2 ? ff.linker_p[i] : ff.motor_p[i];
-                T3<R> Fl = spring_force<R>(load3(x + q.x), load3(x + q.y), load3(x + q.z), load3(x + q.w), p.x, p.y,
-                                           p.z, p.w);
+                T3<R> Fl = spring_force<R>(P(q.x), P(q.y), P(q.z), P(q.w), p.x, p.y, p.z, p.w);
                 const R a1 = R(1) - R(p.z), a2 = R(p.z), b1 = R(1) - R(p.w), b2 = R(p.w);
                 add_force(f, q.x, -Fl.x * a1, -Fl.y * a1, -Fl.z * a1);
                 add_force(f, q.y, -Fl.x * a2, -Fl.y * a2, -Fl.z * a2);
@@ -189,7 +202,7 @@ __global__ void __launch_bounds__(kBlock) k_bonded_forces(const DeviceFF ff, con
             if (i < ff.n_branch) {
                 int4 q = ff.branch_bs[i];
                 double4 pa = ff.branch_pa[i], pb = ff.branch_pb[i];
-                V3 c1 = load3(x + q.x), c2 = load3(x + q.y), c3 = load3(x + q.z), c4 = load3(x + q.w);
+                V3 c1 = P(q.x), c2 = P(q.y), c3 = P(q.z), c4 = P(q.w);
                 T3<R> F1{0, 0, 0}, F2{0, 0, 0}, F3{0, 0, 0}, F4{0, 0, 0};
                 if (ff.branch_mask & 1) {
                     T3<R> g = branch_stretch_force<R>(c1, c2, c3, pa.y, pa.z, pa.x);
@@ -232,7 +245,7 @@ __global__ void __launch_bounds__(kBlock) k_bonded_forces(const DeviceFF ff, con
                 int o = ff.boundary_bs[i];
                 double2 p = ff.boundary_p[i];
                 double4 pl = ff.planes[ff.boundary_plane[i]];
-                R f0 = boundary_force_mag<R>(pl, load3(x + o), p.x, p.y);
+                R f0 = boundary_force_mag<R>(pl, P(o), p.x, p.y);
                 add_force(f, o, f0 * R(pl.x), f0 * R(pl.y), f0 * R(pl.z));
             }
             break;
@@ -257,16 +270,21 @@ void launch_energy(const DeviceFF& ff, int prec, const double* x, const double* 
     launch_excl_energy_fallback_and_finish(ff, x, d, lam, es, s);
 }
 
-void launch_forces(const DeviceFF& ff, int prec, const double* x, double* f, const ForceScratch& fs, cudaStream_t s) {
-    cudaMemsetAsync(f, 0, sizeof(double) * 3 * (size_t)ff.n_beads, s);
+void launch_forces_target(const DeviceFF& ff, int prec, const double* x, const ForceTarget& t, const ForceScratch& fs,
+                          cudaStream_t s) {
     const int nbb = bonded_blocks(ff);
     if (nbb > 0) {
         if (prec == MEDYAN_PREC_MIXED)
-            k_bonded_forces<float><<<nbb, kBlock, 0, s>>>(ff, x, f);
+            k_bonded_forces<float><<<nbb, kBlock, 0, s>>>(ff, x, t);
         else
-            k_bonded_forces<double><<<nbb, kBlock, 0, s>>>(ff, x, f);
+            k_bonded_forces<double><<<nbb, kBlock, 0, s>>>(ff, x, t);
     }
-    launch_excl_forces(ff, prec, x, f, fs, s);
+    launch_excl_forces(ff, prec, x, t, fs, s);
+}
+
+void launch_forces(const DeviceFF& ff, int prec, const double* x, double* f, const ForceScratch& fs, cudaStream_t s) {
+    cudaMemsetAsync(f, 0, sizeof(double) * 3 * (size_t)ff.n_beads, s);
+    launch_forces_target(ff, prec, x, ForceTarget{f, nullptr, nullptr, nullptr, nullptr, nullptr}, fs, s);
 }
 
 }  // namespace mb

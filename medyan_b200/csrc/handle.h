@@ -54,50 +54,47 @@ struct DevBuf {
     T* raw() const { return p; }
 };
 
-// Device-resident state of one conjugate-gradient minimization
-// (the scalars of CGMethod::minimize, CGMethod.hpp:826-1743).
+// Device-resident state of one conjugate-gradient minimization: the scalars
+// of CGMethod::minimize (src/Mechanics/Minimizer/CGMethod.hpp:826-1743) plus
+// the flags that steer the per-iteration kernels without the host.
 struct CGState {
-    // parameters
-    int method;
-    int try_to_recover;
-    int energy_call_limit;
-    int force_call_limit;
+    // parameters (ConjugateGradientParams)
+    int method, try_to_recover, energy_call_limit, force_call_limit;
     double max_dist, lambda_max, grad_tol, energy_rel_tol;
-    // counters and flags
+    // MinimizationResult counters
     int num_energy_call, num_force_call, num_iter;
+    int error_flags;
+    int status;            // medyan_status of the run
+    int done;              // loop finished
     int safe_mode;
-    int done;            // loop finished (converged, call limit, error)
-    int status;          // medyan_status of the run
-    int error_flags;     // MinimizationResult::errorLineSearch
-    int parity;          // force[parity] holds the current force
-    int ls_active;       // a line search is in progress
-    int ls_need_e0;      // E(x) must be evaluated in the next pass
-    int ls_result;       // 0 pending, 1 accepted, 2 failed
+    int parity;            // force[parity] holds the current force
+    // line search
+    int ls_active;         // a line search is in progress
+    int ls_first_pass;     // the next pass is the first of its line search
+    int need_e0;           // E(x) is not known and must be evaluated
+    int ls_immediate_fail; // maxF == 0: the line search returns lambda = 0 at once
+    int backtracks;        // halvings in the current line search
+    int last_backtracks;   // halvings of the previous line search
+    int k_trials;          // trial slots in the current pass
+    // step bookkeeping
+    int skip_force;        // 1: no force pass this iteration
+    int move_kind;         // 1: line-search step, 2: recovery step
+    int dir_mode;          // 0: d = F + beta*d, 1: d = F
+    int reset_after_dir;   // d.F <= 0 after the update: reset to d = F
+    int copy_min_e;        // copy x to the lowest-energy backup
     int have_min_e;
-    int ls_passes;       // passes used by the current line search
-    int last_backtracks; // halvings needed by the previous line search
+    int call_limit;        // loop left because a call limit was exceeded
+    // reduction tickets (last-block-done)
+    unsigned int ticket_dots, ticket_dir;
     // reals
-    double E_cur;        // energy at x
-    double grad_inf_norm;
-    double energy_rel_change;
-    double prev_energy;
-    double last_fdotf;
-    double slope;        // searchDir . force at the start of the line search
-    double lambda;       // next lambda to try / accepted lambda
-    double lambda_next;  // first lambda of the next pass
-    double E_new;        // energy at the accepted lambda
-    double beta;
-    double new_grad, prev_grad;
+    double E_cur, E_new, prev_energy, total_energy;
+    double grad_inf_norm, energy_rel_change;
+    double last_fdotf, new_grad, prev_grad, beta;
+    double slope, reduced_slope;
+    double lam_next;       // first trial lambda of the next pass
+    double lam_move;       // step taken by the pending force pass
+    double dmax;           // max |d_i| of the current search direction
     double min_e;
-    double total_energy; // CGMethod::TotalEnergy (energy of the last line search)
-    double recovery_step;
-    double dot_sf;       // searchDir . force after the direction update
-};
-
-// Per-block partials of the CG vector passes.
-struct CGScratch {
-    double* part;        // [blocks][4]
-    int nblocks;
 };
 
 }  // namespace mb
@@ -129,11 +126,14 @@ struct medyan_mech {
     mb::DevBuf<int2> e_fb_list;
     mb::DevBuf<mb::LambdaSet> lam_zero;
 
-    // conjugate gradient
-    mb::DevBuf<double> cg_dir, cg_force2, cg_min_coords, cg_part;
+    // conjugate gradient (cg.cu)
+    mb::DevBuf<double> cg_dir, cg_force2, cg_min_coords, cg_part, cg_eout;
     mb::DevBuf<mb::CGState> cg_state;
     mb::DevBuf<mb::LambdaSet> cg_lam;
-    mb::DevBuf<double> cg_eout;   // energy outputs of the first/last individual energy calls
+    cudaGraphExec_t cg_graph = nullptr;   // instantiated minimization graph
+    int cg_graph_prec = -1;
+    long long cg_graph_gen = -1;          // ff_gen the graph was captured with
+    long long ff_gen = 0;                 // bumped whenever DeviceFF changes
 
     // neighbor list (nl.cu)
     struct NL;
@@ -149,7 +149,7 @@ medyan_status validate_system(const medyan_system* s);
 medyan_status upload_system(medyan_mech* h, const medyan_system* s);
 medyan_status refresh_device_ff(medyan_mech* h);
 medyan_status sync_status(medyan_mech* h);
-void enqueue_energy(medyan_mech* h, const double* x, const double* d, const LambdaSet* lam);
+void enqueue_energy(medyan_mech* h, const double* x, const double* d, const LambdaSet* lam, cudaStream_t s);
 void enqueue_forces(medyan_mech* h, const double* x, double* f);
 void destroy_nl(medyan_mech* h);
 }  // namespace mb

@@ -52,6 +52,23 @@ struct EnergyScratch {
     int n_blocks_excl;
 };
 
+// Where a force pass writes and at which positions it evaluates. The
+// standalone path uses f0 at x. The minimizer passes both force buffers and
+// a device-side parity (the new force goes to the buffer not holding the
+// current one), a skip flag, and a move x + (*lam)*d evaluated on the fly.
+struct ForceTarget {
+    double* f0;
+    double* f1;
+    const int* parity;   // nullable: write f0
+    const int* skip;     // nullable: nonzero -> the pass does nothing
+    const double* d;     // nullable: positions are x
+    const double* lam;   // step along d
+};
+
+__device__ __forceinline__ double* target_force(const ForceTarget& t) {
+    return t.parity ? (*t.parity ? t.f0 : t.f1) : t.f0;
+}
+
 struct ForceScratch {
     int* fb_count;        // excluded-volume pairs needing forceN
     int* fb_list;
@@ -62,10 +79,14 @@ struct ForceScratch {
 void launch_energy(const DeviceFF& ff, int prec, const double* x, const double* d, const LambdaSet* lam,
                    const EnergyScratch& es, cudaStream_t s);
 void launch_forces(const DeviceFF& ff, int prec, const double* x, double* f, const ForceScratch& fs, cudaStream_t s);
+// Force pass for the minimizer: no memset (the target buffer was zeroed by the
+// previous vector pass).
+void launch_forces_target(const DeviceFF& ff, int prec, const double* x, const ForceTarget& t, const ForceScratch& fs,
+                          cudaStream_t s);
 
 void launch_excl_energy(const DeviceFF& ff, int prec, const double* x, const double* d, const LambdaSet* lam,
                         const EnergyScratch& es, cudaStream_t s);
-void launch_excl_forces(const DeviceFF& ff, int prec, const double* x, double* f, const ForceScratch& fs,
+void launch_excl_forces(const DeviceFF& ff, int prec, const double* x, const ForceTarget& t, const ForceScratch& fs,
                         cudaStream_t s);
 void launch_excl_energy_fallback_and_finish(const DeviceFF& ff, const double* x, const double* d,
                                             const LambdaSet* lam, const EnergyScratch& es, cudaStream_t s);
