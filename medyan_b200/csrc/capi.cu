@@ -97,22 +97,34 @@ medyan_status upload_system(medyan_mech* h, const medyan_system* s) {
         if (e != cudaSuccess) return cuda_status(e);                                  \
     } while (0)
 
-    ff.n_stretch = s->n_stretch;
-    i2.resize(s->n_stretch);
-    d2.resize(s->n_stretch);
-    for (int i = 0; i < s->n_stretch; ++i) {
-        i2[i] = make_int2(s->stretch_beads[2 * i], s->stretch_beads[2 * i + 1]);
-        d2[i] = make_double2(s->stretch_k[i], s->stretch_l0[i]);
+    // filament chains take every stretching link and bend that fits; the rest
+    // stays on the generic path
+    ChainHost chs;
+    build_chains(s, chs);
+    UPLOAD(h->chain_bead, chs.bead);
+    UPLOAD(h->chain_flags, chs.flags);
+    UPLOAD(h->chain_link_p, chs.link_p);
+    UPLOAD(h->chain_bend_p, chs.bend_p);
+    h->chain.n_pos = (int)chs.bead.size();
+
+    ff.n_stretch = (int)chs.left_stretch.size();
+    i2.resize(ff.n_stretch);
+    d2.resize(ff.n_stretch);
+    for (int q = 0; q < ff.n_stretch; ++q) {
+        const int i = chs.left_stretch[q];
+        i2[q] = make_int2(s->stretch_beads[2 * i], s->stretch_beads[2 * i + 1]);
+        d2[q] = make_double2(s->stretch_k[i], s->stretch_l0[i]);
     }
     UPLOAD(h->stretch_bs, i2);
     UPLOAD(h->stretch_p, d2);
 
-    ff.n_bend = s->n_bend;
-    i4.resize(s->n_bend);
-    d2.resize(s->n_bend);
-    for (int i = 0; i < s->n_bend; ++i) {
-        i4[i] = make_int4(s->bend_beads[3 * i], s->bend_beads[3 * i + 1], s->bend_beads[3 * i + 2], 0);
-        d2[i] = make_double2(s->bend_k[i], s->bend_theta0[i]);
+    ff.n_bend = (int)chs.left_bend.size();
+    i4.resize(ff.n_bend);
+    d2.resize(ff.n_bend);
+    for (int q = 0; q < ff.n_bend; ++q) {
+        const int i = chs.left_bend[q];
+        i4[q] = make_int4(s->bend_beads[3 * i], s->bend_beads[3 * i + 1], s->bend_beads[3 * i + 2], 0);
+        d2[q] = make_double2(s->bend_k[i], s->bend_theta0[i]);
     }
     UPLOAD(h->bend_bs, i4);
     UPLOAD(h->bend_p, d2);
@@ -209,12 +221,17 @@ medyan_status refresh_device_ff(medyan_mech* h) {
     ff.boundary_p = h->boundary_p.ptr();
     ff.boundary_plane = h->boundary_plane.ptr();
     ff.planes = h->planes.ptr();
+    h->chain.bead = h->chain_bead.raw();
+    h->chain.flags = h->chain_flags.raw();
+    h->chain.link_p = h->chain_link_p.raw();
+    h->chain.bend_p = h->chain_bend_p.raw();
     const int counts[6] = {ff.n_stretch, ff.n_bend, ff.n_linker, ff.n_motor, ff.n_branch, ff.n_boundary};
     ff.seg[0] = 0;
     for (int q = 0; q < 6; ++q) ff.seg[q + 1] = ff.seg[q] + (counts[q] + kBlock - 1) / kBlock;
+    h->es.n_blocks_chain = h->chain.n_pos > 0 ? chain_blocks(h->chain) : 0;
     h->es.n_blocks_bonded = ff.seg[6];
     h->es.n_blocks_excl = excl_blocks(ff);
-    const size_t need = (size_t)kMaxLambda * (h->es.n_blocks_bonded + h->es.n_blocks_excl + 1) * 4;
+    const size_t need = (size_t)kMaxLambda * (h->es.total() + 1) * 4;
     cudaError_t e = h->partial.reserve(need);
     if (e != cudaSuccess) return cuda_status(e);
     h->es.partial = h->partial.ptr();
@@ -231,11 +248,11 @@ medyan_status sync_status(medyan_mech* h) {
 // Energy at x (+ lam*d when d is set) for the lambda set in device memory;
 // results land in h->es.out.
 void enqueue_energy(medyan_mech* h, const double* x, const double* d, const LambdaSet* lam, cudaStream_t s) {
-    launch_energy(h->ff, h->prec, x, d, lam, h->es, s);
+    launch_energy(h->chain, h->ff, h->prec, x, d, lam, h->es, s);
 }
 
-void enqueue_forces(medyan_mech* h, const double* x, double* f) {
-    launch_forces(h->ff, h->prec, x, f, h->fs, h->stream);
+void enqueue_forces(medyan_mech* h, const double* x, double* f, cudaStream_t s) {
+    launch_forces(h->chain, h->ff, h->prec, x, ForceTarget{f, nullptr, nullptr, nullptr, nullptr, nullptr}, h->fs, s);
 }
 
 }  // namespace mb
@@ -376,7 +393,7 @@ medyan_status medyan_mech_energy(medyan_mech* h, double* e_total, double* e_per_
 
 medyan_status medyan_mech_forces(medyan_mech* h, double* force_out) {
     if (!h || (!force_out && h->n_beads)) return MEDYAN_ERR_INVALID_ARG;
-    enqueue_forces(h, h->x.ptr(), h->f.ptr());
+    enqueue_forces(h, h->x.ptr(), h->f.ptr(), h->stream);
     int status = 0;
     cudaError_t e = cudaMemcpyAsync(force_out, h->f.ptr(), sizeof(double) * 3 * (size_t)h->n_beads,
                                     cudaMemcpyDeviceToHost, h->stream);
@@ -396,7 +413,7 @@ medyan_status medyan_mech_enqueue_energy(medyan_mech* h) {
 
 medyan_status medyan_mech_enqueue_forces(medyan_mech* h) {
     if (!h) return MEDYAN_ERR_INVALID_ARG;
-    enqueue_forces(h, h->x.ptr(), h->f.ptr());
+    enqueue_forces(h, h->x.ptr(), h->f.ptr(), h->stream);
     return cuda_status(cudaGetLastError());
 }
 
@@ -428,7 +445,7 @@ medyan_status medyan_mech_evaluate(medyan_mech* h, const double* coord, double* 
     cudaError_t e = cudaMemcpyAsync(h->x.ptr(), coord, bytes, cudaMemcpyHostToDevice, h->stream);
     if (e != cudaSuccess) return cuda_status(e);
     enqueue_energy(h, h->x.ptr(), nullptr, h->lam_zero.ptr(), h->stream);
-    enqueue_forces(h, h->x.ptr(), h->f.ptr());
+    enqueue_forces(h, h->x.ptr(), h->f.ptr(), h->stream);
     double out[MEDYAN_FF_COUNT + 1];
     int status = 0;
     e = cudaMemcpyAsync(out, h->energy_out.ptr(), sizeof out, cudaMemcpyDeviceToHost, h->stream);

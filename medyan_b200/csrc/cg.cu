@@ -234,7 +234,7 @@ __device__ void reduce_partials(const double* __restrict__ part, int nblk, doubl
     block_reduce3(a, b, m, sm);
 }
 
-// dots pass: commit the move, F.F, F.Fprev, max|F|, zero the old force buffer.
+// dots pass: commit the move, F.F, F.Fprev, max|F|.
 __global__ void __launch_bounds__(kVecThreads) k_cg_dots(int n3, double* __restrict__ x, const double* __restrict__ d,
                                                          double* __restrict__ f0, double* __restrict__ f1,
                                                          CGState* __restrict__ st, double* __restrict__ part) {
@@ -242,7 +242,7 @@ __global__ void __launch_bounds__(kVecThreads) k_cg_dots(int n3, double* __restr
     if (st->done || st->skip_force) return;
     const int parity = st->parity;
     const double* __restrict__ Fn = parity ? f0 : f1;  // new force (written by the force pass)
-    double* __restrict__ Fo = parity ? f1 : f0;        // force at the previous point
+    const double* __restrict__ Fo = parity ? f1 : f0;  // force at the previous point
     const double lam = st->lam_move;
     double a = 0.0, b = 0.0, m = 0.0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x) {
@@ -251,7 +251,6 @@ __global__ void __launch_bounds__(kVecThreads) k_cg_dots(int n3, double* __restr
         a += fn * fn;
         b += fn * fo;
         m = dmax_ref(m, fabs(fn));
-        Fo[i] = 0.0;
     }
     block_reduce3(a, b, m, sm);
     if (threadIdx.x == 0) {
@@ -431,7 +430,7 @@ void enqueue_ls_pass(const CGLaunch& c, cudaStream_t s) {
 }
 
 void enqueue_step(const CGLaunch& c, cudaStream_t s) {
-    launch_forces_target(c.h->ff, c.h->prec, c.x, c.tgt, c.h->fs, s);
+    launch_forces(c.h->chain, c.h->ff, c.h->prec, c.x, c.tgt, c.h->fs, s);
     k_cg_dots<<<c.vb, kVecThreads, 0, s>>>(c.n3, c.x, c.d, c.f0, c.f1, c.st, c.part);
     k_cg_dir<<<c.vb, kVecThreads, 0, s>>>(c.n3, c.x, c.d, c.f0, c.f1, c.st, c.part, c.minE, c.L);
     k_cg_reset_dir<<<c.vb, kVecThreads, 0, s>>>(c.n3, c.d, c.f0, c.f1, c.st);

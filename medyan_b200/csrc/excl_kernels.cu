@@ -20,14 +20,14 @@ namespace {
 __device__ __forceinline__ V3 at(const V3& x, const V3& d, double lam, bool move) { return move ? move3(x, lam, d) : x; }
 
 template <class R>
-__global__ void __launch_bounds__(kBlock) k_excl_energy(const DeviceFF ff, const double* __restrict__ x,
+__global__ void __launch_bounds__(kExclBlock) k_excl_energy(const DeviceFF ff, const double* __restrict__ x,
                                                         const double* __restrict__ d,
                                                         const LambdaSet* __restrict__ lset,
                                                         double* __restrict__ partial, int nblk_total, int blk_off,
                                                         int* __restrict__ fb_count, int2* __restrict__ fb_list,
                                                         int* __restrict__ bad) {
     __shared__ double smem[4 * 32];
-    const int i = blockIdx.x * kBlock + threadIdx.x;
+    const int i = blockIdx.x * kExclBlock + threadIdx.x;
     const bool move = d != nullptr;
     const bool valid = i < ff.n_excl;
     V3 X[4] = {}, D[4] = {};
@@ -70,11 +70,11 @@ __device__ __forceinline__ V3 pos_at(const double* __restrict__ x, const ForceTa
 }
 
 template <class R>
-__global__ void __launch_bounds__(kBlock) k_excl_forces(const DeviceFF ff, const double* __restrict__ x,
-                                                        const ForceTarget tgt, int* __restrict__ fb_count,
-                                                        int* __restrict__ fb_list, int* __restrict__ status) {
+__global__ void __launch_bounds__(kExclBlock) k_excl_forces(const DeviceFF ff, const double* __restrict__ x,
+                                                            const ForceTarget tgt, int* __restrict__ fb_count,
+                                                            int* __restrict__ fb_list, int* __restrict__ status) {
     if (tgt.skip && *tgt.skip) return;
-    const int i = blockIdx.x * kBlock + threadIdx.x;
+    const int i = blockIdx.x * kExclBlock + threadIdx.x;
     if (i >= ff.n_excl) return;
     double* __restrict__ f = target_force(tgt);
     const double lam = tgt.lam ? *tgt.lam : 0.0;
@@ -259,16 +259,17 @@ __global__ void __launch_bounds__(kBlock) k_excl_force_fallback(const DeviceFF f
 __global__ void __launch_bounds__(kBlock) k_energy_finish(const DeviceFF ff, const double* __restrict__ x,
                                                           const double* __restrict__ d,
                                                           const LambdaSet* __restrict__ lset,
-                                                          const double* __restrict__ partial, int nbb, int nbe,
-                                                          int* __restrict__ fb_count, int2* __restrict__ fb_list,
-                                                          int* __restrict__ bad, double* __restrict__ out) {
+                                                          const double* __restrict__ partial, int nch, int nbb,
+                                                          int nbe, int* __restrict__ fb_count,
+                                                          int2* __restrict__ fb_list, int* __restrict__ bad,
+                                                          double* __restrict__ out) {
     __shared__ double grid[401];
     __shared__ double red[4 * 32];
     __shared__ double sums[kMaxLambda][MEDYAN_FF_COUNT];
     __shared__ double fbE[kMaxLambda];
     __shared__ int nfb;
     const int K = lset ? lset->K : 1;
-    const int total_blocks = nbb + nbe;
+    const int total_blocks = nch + nbb + nbe;
     if (threadIdx.x == 0) {
         int n = min(*fb_count, kFallbackCap);
         // deterministic order: sort queued (pair, slot) by slot, then pair
@@ -306,18 +307,22 @@ __global__ void __launch_bounds__(kBlock) k_energy_finish(const DeviceFF ff, con
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
     for (int combo = warp; combo < K * MEDYAN_FF_COUNT; combo += nwarp) {
         const int k = combo / MEDYAN_FF_COUNT, slot = combo % MEDYAN_FF_COUNT;
-        int b0 = 0, b1 = 0, j = 0;
+        // row ranges: chain rows [0, nch), bonded rows nch + seg[], excluded-volume rows after
+        int b0 = 0, b1 = 0, j = 0, c0 = 0, c1 = 0, cj = 0;
         switch (slot) {
-            case 0: b0 = ff.seg[0]; b1 = ff.seg[1]; break;
-            case 1: b0 = ff.seg[1]; b1 = ff.seg[2]; break;
-            case 2: b0 = ff.seg[2]; b1 = ff.seg[3]; break;
-            case 3: b0 = ff.seg[3]; b1 = ff.seg[4]; break;
-            case 4: case 5: case 6: case 7: b0 = ff.seg[4]; b1 = ff.seg[5]; j = slot - 4; break;
-            case 8: b0 = nbb; b1 = nbb + nbe; break;
-            default: b0 = ff.seg[5]; b1 = ff.seg[6]; break;
+            case 0: c0 = 0; c1 = nch; cj = 0; b0 = nch + ff.seg[0]; b1 = nch + ff.seg[1]; break;
+            case 1: c0 = 0; c1 = nch; cj = 1; b0 = nch + ff.seg[1]; b1 = nch + ff.seg[2]; break;
+            case 2: b0 = nch + ff.seg[2]; b1 = nch + ff.seg[3]; break;
+            case 3: b0 = nch + ff.seg[3]; b1 = nch + ff.seg[4]; break;
+            case 4: case 5: case 6: case 7: b0 = nch + ff.seg[4]; b1 = nch + ff.seg[5]; j = slot - 4; break;
+            case 8: b0 = nch + nbb; b1 = nch + nbb + nbe; break;
+            default: b0 = nch + ff.seg[5]; b1 = nch + ff.seg[6]; break;
         }
-        double s = 0.0;
-        for (int b = b0 + lane; b < b1; b += 32) s += partial[((size_t)k * total_blocks + b) * 4 + j];
+        const double* base = partial + (size_t)k * total_blocks * 4;
+        double s = 0.0, s2 = 0.0;
+        for (int b = c0 + lane; b < c1; b += 32) s2 += base[(size_t)b * 4 + cj];
+        for (int b = b0 + lane; b < b1; b += 32) s += base[(size_t)b * 4 + j];
+        s += s2;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
         if (lane == 0) sums[k][slot] = s;
@@ -351,18 +356,19 @@ void launch_excl_energy(const DeviceFF& ff, int prec, const double* x, const dou
                         const EnergyScratch& es, cudaStream_t s) {
     const int nbe = es.n_blocks_excl;
     if (nbe <= 0) return;
-    const int total = es.n_blocks_bonded + nbe;
+    const int total = es.total();
     // FP64 in both precision modes: the analytic integral (differences of
     // arctangents, JJ = -(triple product)^2) loses ~1e-6 relative in float.
     (void)prec;
-    k_excl_energy<double><<<nbe, kBlock, 0, s>>>(ff, x, d, lam, es.partial, total, es.n_blocks_bonded, es.fb_count,
-                                                 es.fb_list, es.bad);
+    k_excl_energy<double><<<nbe, kExclBlock, 0, s>>>(ff, x, d, lam, es.partial, total,
+                                                     es.n_blocks_chain + es.n_blocks_bonded, es.fb_count, es.fb_list,
+                                                     es.bad);
 }
 
 void launch_excl_energy_fallback_and_finish(const DeviceFF& ff, const double* x, const double* d,
                                             const LambdaSet* lam, const EnergyScratch& es, cudaStream_t s) {
-    k_energy_finish<<<1, kBlock, 0, s>>>(ff, x, d, lam, es.partial, es.n_blocks_bonded, es.n_blocks_excl,
-                                         es.fb_count, es.fb_list, es.bad, es.out);
+    k_energy_finish<<<1, kBlock, 0, s>>>(ff, x, d, lam, es.partial, es.n_blocks_chain, es.n_blocks_bonded,
+                                         es.n_blocks_excl, es.fb_count, es.fb_list, es.bad, es.out);
 }
 
 void launch_excl_forces(const DeviceFF& ff, int prec, const double* x, const ForceTarget& t, const ForceScratch& fs,
@@ -370,7 +376,7 @@ void launch_excl_forces(const DeviceFF& ff, int prec, const double* x, const For
     const int nbe = excl_blocks(ff);
     if (nbe <= 0) return;
     (void)prec;  // FP64 in both modes, as for the energy
-    k_excl_forces<double><<<nbe, kBlock, 0, s>>>(ff, x, t, fs.fb_count, fs.fb_list, fs.status);
+    k_excl_forces<double><<<nbe, kExclBlock, 0, s>>>(ff, x, t, fs.fb_count, fs.fb_list, fs.status);
     k_excl_force_fallback<<<1, kBlock, kForceNGridBytes, s>>>(ff, x, t, fs.fb_count, fs.fb_list, fs.status);
 }
 

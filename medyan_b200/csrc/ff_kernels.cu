@@ -29,7 +29,7 @@ template <class R>
 __global__ void __launch_bounds__(kBlock) k_bonded_energy(const DeviceFF ff, const double* __restrict__ x,
                                                           const double* __restrict__ d,
                                                           const LambdaSet* __restrict__ lset,
-                                                          double* __restrict__ partial, int nblk_total) {
+                                                          double* __restrict__ partial, int nblk_total, int blk_off) {
     __shared__ double smem[4 * 32];
     const int b = blockIdx.x;
     const int s = segment_of(ff, b);
@@ -132,7 +132,7 @@ __global__ void __launch_bounds__(kBlock) k_bonded_energy(const DeviceFF ff, con
         }
         block_sum<4>(e, smem);
         if (threadIdx.x == 0) {
-            double* o = partial + ((size_t)k * nblk_total + b) * 4;
+            double* o = partial + ((size_t)k * nblk_total + blk_off + b) * 4;
             o[0] = e[0];
             o[1] = e[1];
             o[2] = e[2];
@@ -256,22 +256,25 @@ __global__ void __launch_bounds__(kBlock) k_bonded_forces(const DeviceFF ff, con
 
 int bonded_blocks(const DeviceFF& ff) { return ff.seg[6]; }
 
-void launch_energy(const DeviceFF& ff, int prec, const double* x, const double* d, const LambdaSet* lam,
-                   const EnergyScratch& es, cudaStream_t s) {
-    const int nbb = es.n_blocks_bonded, nbe = es.n_blocks_excl;
-    const int total = nbb + nbe;
+void launch_energy(const ChainDev& ch, const DeviceFF& ff, int prec, const double* x, const double* d,
+                   const LambdaSet* lam, const EnergyScratch& es, cudaStream_t s) {
+    const int nbb = es.n_blocks_bonded;
+    const int total = es.total();
+    launch_chain_energy(ch, prec, x, d, lam, es.partial, total, 0, s);
     if (nbb > 0) {
         if (prec == MEDYAN_PREC_MIXED)
-            k_bonded_energy<float><<<nbb, kBlock, 0, s>>>(ff, x, d, lam, es.partial, total);
+            k_bonded_energy<float><<<nbb, kBlock, 0, s>>>(ff, x, d, lam, es.partial, total, es.n_blocks_chain);
         else
-            k_bonded_energy<double><<<nbb, kBlock, 0, s>>>(ff, x, d, lam, es.partial, total);
+            k_bonded_energy<double><<<nbb, kBlock, 0, s>>>(ff, x, d, lam, es.partial, total, es.n_blocks_chain);
     }
     launch_excl_energy(ff, prec, x, d, lam, es, s);
     launch_excl_energy_fallback_and_finish(ff, x, d, lam, es, s);
 }
 
-void launch_forces_target(const DeviceFF& ff, int prec, const double* x, const ForceTarget& t, const ForceScratch& fs,
-                          cudaStream_t s) {
+void launch_forces(const ChainDev& ch, const DeviceFF& ff, int prec, const double* x, const ForceTarget& t,
+                   const ForceScratch& fs, cudaStream_t s) {
+    // the chain pass stores every bead's force; everything after adds
+    launch_chain_forces(ch, prec, x, t, s);
     const int nbb = bonded_blocks(ff);
     if (nbb > 0) {
         if (prec == MEDYAN_PREC_MIXED)
@@ -280,11 +283,6 @@ void launch_forces_target(const DeviceFF& ff, int prec, const double* x, const F
             k_bonded_forces<double><<<nbb, kBlock, 0, s>>>(ff, x, t);
     }
     launch_excl_forces(ff, prec, x, t, fs, s);
-}
-
-void launch_forces(const DeviceFF& ff, int prec, const double* x, double* f, const ForceScratch& fs, cudaStream_t s) {
-    cudaMemsetAsync(f, 0, sizeof(double) * 3 * (size_t)ff.n_beads, s);
-    launch_forces_target(ff, prec, x, ForceTarget{f, nullptr, nullptr, nullptr, nullptr, nullptr}, fs, s);
 }
 
 }  // namespace mb

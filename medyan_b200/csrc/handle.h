@@ -109,6 +109,12 @@ struct medyan_mech {
     mb::EnergyScratch es{};
     mb::ForceScratch fs{};
 
+    // filament chains (chain.cu)
+    mb::ChainDev chain{};
+    mb::DevBuf<int> chain_bead;
+    mb::DevBuf<unsigned char> chain_flags;
+    mb::DevBuf<double2> chain_link_p, chain_bend_p;
+
     // force-field records
     mb::DevBuf<int2> stretch_bs;
     mb::DevBuf<double2> stretch_p;
@@ -150,6 +156,6 @@ medyan_status upload_system(medyan_mech* h, const medyan_system* s);
 medyan_status refresh_device_ff(medyan_mech* h);
 medyan_status sync_status(medyan_mech* h);
 void enqueue_energy(medyan_mech* h, const double* x, const double* d, const LambdaSet* lam, cudaStream_t s);
-void enqueue_forces(medyan_mech* h, const double* x, double* f);
+void enqueue_forces(medyan_mech* h, const double* x, double* f, cudaStream_t s);
 void destroy_nl(medyan_mech* h);
 }  // namespace mb

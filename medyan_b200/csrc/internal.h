@@ -4,12 +4,13 @@
 
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <vector>
 
 #include "medyan_b200.h"
 
 namespace mb {
 
-constexpr int kMaxLambda = 8;   // step sizes evaluated per line-search energy pass
+constexpr int kMaxLambda = 4;   // step sizes evaluated per line-search energy pass
 constexpr int kBlock = 256;     // threads per block for interaction kernels
 constexpr int kFallbackCap = 256;
 
@@ -34,6 +35,23 @@ struct DeviceFF {
     int seg[7];
 };
 
+// Filament chains (chain.cu): one position per bead, links between
+// consecutive positions, bends centred on positions.
+struct ChainDev {
+    int n_pos;
+    const int* bead;             // coordinate offset of each position
+    const unsigned char* flags;  // bit 0: link (p, p+1); bit 1: bend centred at p
+    const double2* link_p;       // (k, l0) of link (p, p+1)
+    const double2* bend_p;       // (k, theta0) of the bend centred at p
+};
+
+struct ChainHost {
+    std::vector<int> bead;
+    std::vector<unsigned char> flags;
+    std::vector<double2> link_p, bend_p;
+    std::vector<int> left_stretch, left_bend;  // interactions kept on the generic path
+};
+
 // Step sizes for one energy pass: positions are x + lam[k]*d.
 struct LambdaSet {
     int K;
@@ -43,13 +61,15 @@ struct LambdaSet {
 
 // Energy pass scratch: per-block partial sums and the quadrature fallback queue.
 struct EnergyScratch {
-    double* partial;      // [kMaxLambda][n_blocks_total][4]
+    double* partial;      // [kMaxLambda][n_blocks_total][4]: chain rows, bonded rows, excluded-volume rows
     int* fb_count;        // excluded-volume pairs needing energyN
     int2* fb_list;        // (pair, lambda slot)
     int* bad;             // per lambda slot: fallback failed / queue overflow
     double* out;          // [kMaxLambda][MEDYAN_FF_COUNT + 1]: per FF, then total
+    int n_blocks_chain;
     int n_blocks_bonded;
     int n_blocks_excl;
+    int total() const { return n_blocks_chain + n_blocks_bonded + n_blocks_excl; }
 };
 
 // Where a force pass writes and at which positions it evaluates. The
@@ -75,14 +95,17 @@ struct ForceScratch {
     int* status;          // bit 0: fallback failed, bit 1: queue overflow
 };
 
-// Launchers (ff_kernels.cu / excl_kernels.cu). prec: MEDYAN_PREC_*.
-void launch_energy(const DeviceFF& ff, int prec, const double* x, const double* d, const LambdaSet* lam,
-                   const EnergyScratch& es, cudaStream_t s);
-void launch_forces(const DeviceFF& ff, int prec, const double* x, double* f, const ForceScratch& fs, cudaStream_t s);
-// Force pass for the minimizer: no memset (the target buffer was zeroed by the
-// previous vector pass).
-void launch_forces_target(const DeviceFF& ff, int prec, const double* x, const ForceTarget& t, const ForceScratch& fs,
-                          cudaStream_t s);
+// Launchers (ff_kernels.cu / excl_kernels.cu / chain.cu). prec: MEDYAN_PREC_*.
+// The chain pass writes every bead's force first; the other passes add.
+void launch_energy(const ChainDev& ch, const DeviceFF& ff, int prec, const double* x, const double* d,
+                   const LambdaSet* lam, const EnergyScratch& es, cudaStream_t s);
+void launch_forces(const ChainDev& ch, const DeviceFF& ff, int prec, const double* x, const ForceTarget& t,
+                   const ForceScratch& fs, cudaStream_t s);
+void launch_chain_forces(const ChainDev& ch, int prec, const double* x, const ForceTarget& t, cudaStream_t s);
+void launch_chain_energy(const ChainDev& ch, int prec, const double* x, const double* d, const LambdaSet* lam,
+                         double* partial, int nblk_total, int blk_off, cudaStream_t s);
+int chain_blocks(const ChainDev& ch);
+void build_chains(const medyan_system* s, ChainHost& out);
 
 void launch_excl_energy(const DeviceFF& ff, int prec, const double* x, const double* d, const LambdaSet* lam,
                         const EnergyScratch& es, cudaStream_t s);
@@ -96,6 +119,7 @@ constexpr int kForceNGridBytes = (10000 + 1) * (int)sizeof(double);
 cudaError_t init_excl_kernels();
 
 int bonded_blocks(const DeviceFF& ff);
-inline int excl_blocks(const DeviceFF& ff) { return (ff.n_excl + kBlock - 1) / kBlock; }
+constexpr int kExclBlock = 64;  // small blocks: the pair count is low and each pair is heavy
+inline int excl_blocks(const DeviceFF& ff) { return (ff.n_excl + kExclBlock - 1) / kExclBlock; }
 
 }  // namespace mb
