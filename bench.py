@@ -183,6 +183,15 @@ def run_ours(args, rank: int, world: int) -> dict:
     wall = time.perf_counter() - t0
     t_force = [ev[i][0].elapsed_time(ev[i][1]) / 1e3 for i in range(K)]
     t_energy = [ev[i][1].elapsed_time(ev[i][2]) / 1e3 for i in range(K)]
+    # the same steps back to back without the L2 flush (working set L2-resident)
+    with torch.cuda.stream(stream):
+        w0, w1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        w0.record(stream)
+        for i in range(K):
+            step()
+        w1.record(stream)
+    L.medyan_mech_synchronize(h)
+    t_warm = w0.elapsed_time(w1) / 1e3 / K
     t_step = sum(t_force) + sum(t_energy)
     if world > 1:
         tt = torch.tensor([t_step], device="cuda")
@@ -231,11 +240,12 @@ def run_ours(args, rank: int, world: int) -> dict:
                    "step": "total energy + forces of all force fields", "parallelism": f"replicas x{world}"},
         "e2e": {"value": world * K / e2e_t, "unit": "force-evals/s", "h2d_bytes_per_step": 8 * x.size,
                 "d2h_bytes_per_step": 8 * x.size + 8 * 11},
-        "gpu_launches": K * 6,
+        "gpu_launches": K * 8,  # chain, bonded, excluded-volume, fallback (forces); chain, bonded, excluded-volume, finish (energy)
         "clocks": clocks.summary(),
         "wall_s_timed_region": wall,
         "accuracy_vs_fp64": {"rel_force_err": rel_force_err, "rel_energy_err": rel_energy_err},
-        "breakdown_ms": {"forces": 1e3 * sum(t_force) / K, "energy": 1e3 * sum(t_energy) / K},
+        "breakdown_ms": {"forces": 1e3 * sum(t_force) / K, "energy": 1e3 * sum(t_energy) / K,
+                         "step_l2_warm": 1e3 * t_warm},
     }
     fb = abytes["forces"]
     t_f = sum(t_force) / K

@@ -63,8 +63,10 @@ enum {
 
 typedef enum medyan_precision {
     MEDYAN_PREC_FP64 = 0,   /* all arithmetic in double                                  */
-    MEDYAN_PREC_MIXED = 1   /* per-interaction math in float after FP64 coordinate
-                               differences; energy sums, dots, beta and the Armijo test in double */
+    MEDYAN_PREC_MIXED = 1   /* per-interaction force math in float after FP64 coordinate
+                               differences (excluded volume stays double); energies, force
+                               sums, dots, beta and the Armijo test in double, so the line
+                               search compares the same energies as the FP64 mode */
 } medyan_precision;
 
 /* ------------------------------------------------------------------------ */
@@ -171,8 +173,11 @@ medyan_status medyan_mech_get_coords(medyan_mech* h, double* coord);
 /* ForceFieldManager::computeEnergy / computeIndividualEnergies
    (ForceFieldManager.cpp:96-240): total and per-force-field energies at the
    uploaded coordinates. e_per_ff may be NULL, else double[MEDYAN_FF_COUNT].
-   A non-finite force-field energy sets *e_total = +inf and returns
-   MEDYAN_ERR_NONFINITE. */
+   A force field whose energy is the reference's error value (at or below -1:
+   the excluded-volume energy when its quadrature fallback also fails) sets
+   *e_total = +inf and returns MEDYAN_ERR_NONFINITE. A NaN term (e.g. a bend
+   over a zero-length cylinder) propagates into the total, as in the
+   reference, whose bonded energies carry no check. */
 medyan_status medyan_mech_energy(medyan_mech* h, double* e_total, double* e_per_ff);
 
 /* ForceFieldManager::computeForces (ForceFieldManager.cpp:242-290):
@@ -197,7 +202,11 @@ medyan_status medyan_mech_synchronize(medyan_mech* h);
 /* The handle's cudaStream_t, for event timing or stream ordering. */
 void* medyan_mech_stream(medyan_mech* h);
 /* Device pointers of the coordinate and force arrays (double[3*n_beads]) and
-   of the energy output (double[MEDYAN_FF_COUNT + 1]: per force field, then total). */
+   of the energy output (double[MEDYAN_FF_COUNT + 1]: per force field, then total).
+   The device arrays hold the beads in the library's internal order (filament
+   chains contiguous, fixed when the handle is created), which differs from
+   the caller's order unless each filament's beads are already consecutive;
+   medyan_mech_set_coords / get_coords / forces convert. */
 medyan_status medyan_mech_device_buffers(medyan_mech* h, double** coord, double** force, double** energy);
 
 /* ------------------------------------------------------------------------ */

@@ -97,22 +97,37 @@ medyan_status upload_system(medyan_mech* h, const medyan_system* s) {
         if (e != cudaSuccess) return cuda_status(e);                                  \
     } while (0)
 
+    // the internal bead order is fixed by the first vectorization
+    if ((int)h->order_host.size() != s->n_beads) {
+        chain_order(s, h->order_host);
+        h->pos_host.assign(s->n_beads, 0);
+        h->identity_order = true;
+        for (int p = 0; p < s->n_beads; ++p) {
+            h->pos_host[h->order_host[p]] = p;
+            if (h->order_host[p] != p) h->identity_order = false;
+        }
+        if (!h->identity_order) UPLOAD(h->order, h->order_host);
+        e = h->stage.reserve(3 * (size_t)s->n_beads);
+        if (e != cudaSuccess) return cuda_status(e);
+    }
+    const std::vector<int>& pos = h->pos_host;
+    auto R = [&](int32_t off) { return 3 * pos[off / 3]; };  // external offset -> internal offset
+
     // filament chains take every stretching link and bend that fits; the rest
     // stays on the generic path
     ChainHost chs;
-    build_chains(s, chs);
-    UPLOAD(h->chain_bead, chs.bead);
+    build_chains(s, pos, chs);
     UPLOAD(h->chain_flags, chs.flags);
     UPLOAD(h->chain_link_p, chs.link_p);
     UPLOAD(h->chain_bend_p, chs.bend_p);
-    h->chain.n_pos = (int)chs.bead.size();
+    h->chain.n_pos = s->n_beads;
 
     ff.n_stretch = (int)chs.left_stretch.size();
     i2.resize(ff.n_stretch);
     d2.resize(ff.n_stretch);
     for (int q = 0; q < ff.n_stretch; ++q) {
         const int i = chs.left_stretch[q];
-        i2[q] = make_int2(s->stretch_beads[2 * i], s->stretch_beads[2 * i + 1]);
+        i2[q] = make_int2(R(s->stretch_beads[2 * i]), R(s->stretch_beads[2 * i + 1]));
         d2[q] = make_double2(s->stretch_k[i], s->stretch_l0[i]);
     }
     UPLOAD(h->stretch_bs, i2);
@@ -123,7 +138,7 @@ medyan_status upload_system(medyan_mech* h, const medyan_system* s) {
     d2.resize(ff.n_bend);
     for (int q = 0; q < ff.n_bend; ++q) {
         const int i = chs.left_bend[q];
-        i4[q] = make_int4(s->bend_beads[3 * i], s->bend_beads[3 * i + 1], s->bend_beads[3 * i + 2], 0);
+        i4[q] = make_int4(R(s->bend_beads[3 * i]), R(s->bend_beads[3 * i + 1]), R(s->bend_beads[3 * i + 2]), 0);
         d2[q] = make_double2(s->bend_k[i], s->bend_theta0[i]);
     }
     UPLOAD(h->bend_bs, i4);
@@ -134,7 +149,7 @@ medyan_status upload_system(medyan_mech* h, const medyan_system* s) {
         i4.resize(n);
         d4.resize(n);
         for (int i = 0; i < n; ++i) {
-            i4[i] = make_int4(bs[4 * i], bs[4 * i + 1], bs[4 * i + 2], bs[4 * i + 3]);
+            i4[i] = make_int4(R(bs[4 * i]), R(bs[4 * i + 1]), R(bs[4 * i + 2]), R(bs[4 * i + 3]));
             d4[i] = make_double4(k[i], l0[i], p1[i], p2[i]);
         }
     };
@@ -155,7 +170,7 @@ medyan_status upload_system(medyan_mech* h, const medyan_system* s) {
     auto at = [](const double* p, int i) { return p ? p[i] : 0.0; };
     for (int i = 0; i < s->n_branch; ++i) {
         const int32_t* b = s->branch_beads + 4 * i;
-        i4[i] = make_int4(b[0], b[1], b[2], b[3]);
+        i4[i] = make_int4(R(b[0]), R(b[1]), R(b[2]), R(b[3]));
         d4[i] = make_double4(s->branch_pos[i], at(s->branch_stretch_k, i), at(s->branch_stretch_l0, i),
                              at(s->branch_bend_k, i));
         d4b[i] = make_double4(at(s->branch_bend_theta0, i), at(s->branch_dihedral_k, i),
@@ -170,7 +185,7 @@ medyan_status upload_system(medyan_mech* h, const medyan_system* s) {
     d1.resize(s->n_excl);
     for (int i = 0; i < s->n_excl; ++i) {
         const int32_t* b = s->excl_beads + 4 * i;
-        i4[i] = make_int4(b[0], b[1], b[2], b[3]);
+        i4[i] = make_int4(R(b[0]), R(b[1]), R(b[2]), R(b[3]));
         // kRepScaled = krep * eqLength_1 * eqLength_2, CylinderExclVolRepulsion.cpp:355
         d1[i] = s->excl_k[i] * s->excl_eqlen[2 * i] * s->excl_eqlen[2 * i + 1];
     }
@@ -179,8 +194,8 @@ medyan_status upload_system(medyan_mech* h, const medyan_system* s) {
 
     ff.n_boundary = s->n_boundary;
     ff.n_planes = s->n_planes;
-    ii.assign(s->boundary_beads ? s->boundary_beads : nullptr,
-              s->boundary_beads ? s->boundary_beads + s->n_boundary : nullptr);
+    ii.resize(s->n_boundary);
+    for (int i = 0; i < s->n_boundary; ++i) ii[i] = R(s->boundary_beads[i]);
     d2.resize(s->n_boundary);
     pl.resize(s->n_boundary);
     {
@@ -221,7 +236,6 @@ medyan_status refresh_device_ff(medyan_mech* h) {
     ff.boundary_p = h->boundary_p.ptr();
     ff.boundary_plane = h->boundary_plane.ptr();
     ff.planes = h->planes.ptr();
-    h->chain.bead = h->chain_bead.raw();
     h->chain.flags = h->chain_flags.raw();
     h->chain.link_p = h->chain_link_p.raw();
     h->chain.bend_p = h->chain_bend_p.raw();
@@ -248,11 +262,52 @@ medyan_status sync_status(medyan_mech* h) {
 // Energy at x (+ lam*d when d is set) for the lambda set in device memory;
 // results land in h->es.out.
 void enqueue_energy(medyan_mech* h, const double* x, const double* d, const LambdaSet* lam, cudaStream_t s) {
-    launch_energy(h->chain, h->ff, h->prec, x, d, lam, h->es, s);
+    launch_energy(h->chain, h->ff, h->prec, x, d, lam, h->es, s, &h->fork);
 }
 
 void enqueue_forces(medyan_mech* h, const double* x, double* f, cudaStream_t s) {
-    launch_forces(h->chain, h->ff, h->prec, x, ForceTarget{f, nullptr, nullptr, nullptr, nullptr, nullptr}, h->fs, s);
+    launch_forces(h->chain, h->ff, h->prec, x, ForceTarget{f, nullptr, nullptr, nullptr, nullptr, nullptr}, h->fs, s,
+                  &h->fork);
+}
+
+cudaError_t coords_to_device(medyan_mech* h, const double* host, double* dev, cudaStream_t s) {
+    const int n3 = 3 * h->n_beads;
+    if (n3 == 0) return cudaSuccess;
+    if (h->identity_order) return cudaMemcpyAsync(dev, host, sizeof(double) * n3, cudaMemcpyHostToDevice, s);
+    cudaError_t e = cudaMemcpyAsync(h->stage.raw(), host, sizeof(double) * n3, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) launch_to_internal(n3, h->order.raw(), h->stage.raw(), dev, s);
+    return e == cudaSuccess ? cudaGetLastError() : e;
+}
+
+cudaError_t coords_to_host(medyan_mech* h, const double* dev, double* host, cudaStream_t s) {
+    const int n3 = 3 * h->n_beads;
+    if (n3 == 0) return cudaSuccess;
+    if (h->identity_order) return cudaMemcpyAsync(host, dev, sizeof(double) * n3, cudaMemcpyDeviceToHost, s);
+    launch_to_external(n3, h->order.raw(), dev, h->stage.raw(), s);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(host, h->stage.raw(), sizeof(double) * n3, cudaMemcpyDeviceToHost, s);
+    return e;
+}
+
+cudaError_t launch_pass(medyan_mech* h, int which) {
+    if (!h->pass_graph[which] || h->pass_graph_gen[which] != h->ff_gen) {
+        if (h->pass_graph[which]) cudaGraphExecDestroy(h->pass_graph[which]);
+        h->pass_graph[which] = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return e;
+        if (which != kPassForces) enqueue_energy(h, h->x.raw(), nullptr, h->lam_zero.raw(), h->stream);
+        if (which != kPassEnergy) enqueue_forces(h, h->x.raw(), h->f.raw(), h->stream);
+        cudaGraph_t g = nullptr;
+        e = cudaStreamEndCapture(h->stream, &g);
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&h->pass_graph[which], g, 0);
+        if (g) cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            h->pass_graph[which] = nullptr;
+            return e;
+        }
+        h->pass_graph_gen[which] = h->ff_gen;
+    }
+    return cudaGraphLaunch(h->pass_graph[which], h->stream);
 }
 
 }  // namespace mb
@@ -260,6 +315,9 @@ void enqueue_forces(medyan_mech* h, const double* x, double* f, cudaStream_t s) 
 medyan_status medyan_mech::init() {
     cudaError_t e = cudaSetDevice(device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
+    for (int k = 0; k < 2 && e == cudaSuccess; ++k) e = cudaStreamCreateWithFlags(&fork.side[k], cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&fork.fork, cudaEventDisableTiming);
+    for (int k = 0; k < 2 && e == cudaSuccess; ++k) e = cudaEventCreateWithFlags(&fork.join[k], cudaEventDisableTiming);
     if (e == cudaSuccess) e = init_excl_kernels();
     const size_t n3 = 3 * (size_t)n_beads;
     if (e == cudaSuccess) e = x.reserve(n3);
@@ -296,7 +354,14 @@ medyan_mech::~medyan_mech() {
     cudaSetDevice(device);
     if (stream) cudaStreamSynchronize(stream);
     if (cg_graph) cudaGraphExecDestroy(cg_graph);
+    for (auto& g : pass_graph)
+        if (g) cudaGraphExecDestroy(g);
     destroy_nl(this);
+    for (auto& sd : fork.side)
+        if (sd) cudaStreamDestroy(sd);
+    if (fork.fork) cudaEventDestroy(fork.fork);
+    for (auto& ev : fork.join)
+        if (ev) cudaEventDestroy(ev);
     if (stream) cudaStreamDestroy(stream);
 }
 
@@ -363,25 +428,24 @@ medyan_status medyan_mech_destroy(medyan_mech* h) {
 
 medyan_status medyan_mech_set_coords(medyan_mech* h, const double* coord) {
     if (!h || (!coord && h->n_beads)) return MEDYAN_ERR_INVALID_ARG;
-    cudaError_t e = cudaMemcpyAsync(h->x.ptr(), coord, sizeof(double) * 3 * (size_t)h->n_beads,
-                                    cudaMemcpyHostToDevice, h->stream);
+    cudaError_t e = coords_to_device(h, coord, h->x.raw(), h->stream);
     if (e != cudaSuccess) return cuda_status(e);
     return sync_status(h);
 }
 
 medyan_status medyan_mech_get_coords(medyan_mech* h, double* coord) {
     if (!h || (!coord && h->n_beads)) return MEDYAN_ERR_INVALID_ARG;
-    cudaError_t e = cudaMemcpyAsync(coord, h->x.ptr(), sizeof(double) * 3 * (size_t)h->n_beads,
-                                    cudaMemcpyDeviceToHost, h->stream);
+    cudaError_t e = coords_to_host(h, h->x.raw(), coord, h->stream);
     if (e != cudaSuccess) return cuda_status(e);
     return sync_status(h);
 }
 
 medyan_status medyan_mech_energy(medyan_mech* h, double* e_total, double* e_per_ff) {
     if (!h || !e_total) return MEDYAN_ERR_INVALID_ARG;
-    enqueue_energy(h, h->x.ptr(), nullptr, h->lam_zero.ptr(), h->stream);
+    cudaError_t e = launch_pass(h, kPassEnergy);
+    if (e != cudaSuccess) return cuda_status(e);
     double out[MEDYAN_FF_COUNT + 1];
-    cudaError_t e = cudaMemcpyAsync(out, h->energy_out.ptr(), sizeof out, cudaMemcpyDeviceToHost, h->stream);
+    e = cudaMemcpyAsync(out, h->energy_out.ptr(), sizeof out, cudaMemcpyDeviceToHost, h->stream);
     if (e != cudaSuccess) return cuda_status(e);
     medyan_status st = sync_status(h);
     if (st != MEDYAN_OK) return st;
@@ -393,10 +457,10 @@ medyan_status medyan_mech_energy(medyan_mech* h, double* e_total, double* e_per_
 
 medyan_status medyan_mech_forces(medyan_mech* h, double* force_out) {
     if (!h || (!force_out && h->n_beads)) return MEDYAN_ERR_INVALID_ARG;
-    enqueue_forces(h, h->x.ptr(), h->f.ptr(), h->stream);
+    cudaError_t e = launch_pass(h, kPassForces);
+    if (e != cudaSuccess) return cuda_status(e);
     int status = 0;
-    cudaError_t e = cudaMemcpyAsync(force_out, h->f.ptr(), sizeof(double) * 3 * (size_t)h->n_beads,
-                                    cudaMemcpyDeviceToHost, h->stream);
+    e = coords_to_host(h, h->f.raw(), force_out, h->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(&status, h->force_status.ptr(), sizeof(int), cudaMemcpyDeviceToHost, h->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(h->force_status.ptr(), 0, sizeof(int), h->stream);
     if (e != cudaSuccess) return cuda_status(e);
@@ -407,14 +471,12 @@ medyan_status medyan_mech_forces(medyan_mech* h, double* force_out) {
 
 medyan_status medyan_mech_enqueue_energy(medyan_mech* h) {
     if (!h) return MEDYAN_ERR_INVALID_ARG;
-    enqueue_energy(h, h->x.ptr(), nullptr, h->lam_zero.ptr(), h->stream);
-    return cuda_status(cudaGetLastError());
+    return cuda_status(launch_pass(h, kPassEnergy));
 }
 
 medyan_status medyan_mech_enqueue_forces(medyan_mech* h) {
     if (!h) return MEDYAN_ERR_INVALID_ARG;
-    enqueue_forces(h, h->x.ptr(), h->f.ptr(), h->stream);
-    return cuda_status(cudaGetLastError());
+    return cuda_status(launch_pass(h, kPassForces));
 }
 
 medyan_status medyan_mech_synchronize(medyan_mech* h) {
@@ -441,15 +503,14 @@ medyan_status medyan_mech_device_buffers(medyan_mech* h, double** coord, double*
 medyan_status medyan_mech_evaluate(medyan_mech* h, const double* coord, double* e_total, double* e_per_ff,
                                    double* force_out) {
     if (!h || !coord || !e_total || !force_out) return MEDYAN_ERR_INVALID_ARG;
-    const size_t bytes = sizeof(double) * 3 * (size_t)h->n_beads;
-    cudaError_t e = cudaMemcpyAsync(h->x.ptr(), coord, bytes, cudaMemcpyHostToDevice, h->stream);
+    cudaError_t e = coords_to_device(h, coord, h->x.raw(), h->stream);
     if (e != cudaSuccess) return cuda_status(e);
-    enqueue_energy(h, h->x.ptr(), nullptr, h->lam_zero.ptr(), h->stream);
-    enqueue_forces(h, h->x.ptr(), h->f.ptr(), h->stream);
+    e = launch_pass(h, kPassBoth);
+    if (e != cudaSuccess) return cuda_status(e);
     double out[MEDYAN_FF_COUNT + 1];
     int status = 0;
     e = cudaMemcpyAsync(out, h->energy_out.ptr(), sizeof out, cudaMemcpyDeviceToHost, h->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(force_out, h->f.ptr(), bytes, cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = coords_to_host(h, h->f.raw(), force_out, h->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(&status, h->force_status.ptr(), sizeof(int), cudaMemcpyDeviceToHost, h->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(h->force_status.ptr(), 0, sizeof(int), h->stream);
     if (e != cudaSuccess) return cuda_status(e);

@@ -14,7 +14,7 @@
 //     call count are the reference's);
 //   force pass at x + lam*d into the force buffer that does not hold the
 //     current force;
-//   dots pass: commit x += lam*d, F.F, F.Fprev, max|F|, zero the old buffer;
+//   dots pass: commit x += lam*d, F.F, F.Fprev, max|F|;
 //     its last block computes beta (PR: max(0, (F.F - F.Fprev)/lastF.F));
 //   direction pass: d = F + beta*d (or F), d.F, max|d|; its last block checks
 //     d.F <= 0 (reset), convergence and call limits, and prepares the next
@@ -430,7 +430,7 @@ void enqueue_ls_pass(const CGLaunch& c, cudaStream_t s) {
 }
 
 void enqueue_step(const CGLaunch& c, cudaStream_t s) {
-    launch_forces(c.h->chain, c.h->ff, c.h->prec, c.x, c.tgt, c.h->fs, s);
+    launch_forces(c.h->chain, c.h->ff, c.h->prec, c.x, c.tgt, c.h->fs, s, &c.h->fork);
     k_cg_dots<<<c.vb, kVecThreads, 0, s>>>(c.n3, c.x, c.d, c.f0, c.f1, c.st, c.part);
     k_cg_dir<<<c.vb, kVecThreads, 0, s>>>(c.n3, c.x, c.d, c.f0, c.f1, c.st, c.part, c.minE, c.L);
     k_cg_reset_dir<<<c.vb, kVecThreads, 0, s>>>(c.n3, c.d, c.f0, c.f1, c.st);
@@ -547,7 +547,7 @@ extern "C" medyan_status medyan_cg_minimize(medyan_mech* h, const medyan_cg_para
     s0.skip_force = 0;
     s0.move_kind = 0;
     LambdaSet l0{};
-    e = cudaMemcpyAsync(c.x, coord_inout, bytes, cudaMemcpyHostToDevice, s);
+    e = coords_to_device(h, coord_inout, c.x, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(c.st, &s0, sizeof s0, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(c.L, &l0, sizeof l0, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(c.d, 0, bytes ? bytes : 8, s);
@@ -582,14 +582,14 @@ extern "C" medyan_status medyan_cg_minimize(medyan_mech* h, const medyan_cg_para
     if (e != cudaSuccess) return cuda_status(e);
     if (sf.status == MEDYAN_ERR_LINE_SEARCH) {
         // errorLineSearch: return at once, coordinates as they are
-        cudaMemcpyAsync(coord_inout, c.x, bytes, cudaMemcpyDeviceToHost, s);
-        if (force_out) cudaMemcpyAsync(force_out, sf.parity ? c.f1 : c.f0, bytes, cudaMemcpyDeviceToHost, s);
+        coords_to_host(h, c.x, coord_inout, s);
+        if (force_out) coords_to_host(h, sf.parity ? c.f1 : c.f0, force_out, s);
     } else {
         if (sf.call_limit && sf.have_min_e) cudaMemcpyAsync(c.x, c.minE, bytes, cudaMemcpyDeviceToDevice, s);
         enqueue_energy(h, c.x, nullptr, h->lam_zero.raw(), s);
         k_cg_record_energy<<<1, 1, 0, s>>>(c.st, h->energy_out.raw(), h->cg_eout.raw() + kOut, 0);
-        cudaMemcpyAsync(coord_inout, c.x, bytes, cudaMemcpyDeviceToHost, s);
-        if (force_out) cudaMemcpyAsync(force_out, sf.parity ? c.f1 : c.f0, bytes, cudaMemcpyDeviceToHost, s);
+        coords_to_host(h, c.x, coord_inout, s);
+        if (force_out) coords_to_host(h, sf.parity ? c.f1 : c.f0, force_out, s);
     }
     double eo[2 * kOut];
     e = cudaMemcpyAsync(eo, h->cg_eout.raw(), sizeof eo, cudaMemcpyDeviceToHost, s);

@@ -1,22 +1,30 @@
-// chain.cu — filament stretching and bending as one bead-centric pass.
+// chain.cu — filament stretching and bending as one bead-centric pass, and
+// the library's internal bead order.
 //
-// At upload the stretching links (b1 -> b2) and bending triplets
-// (b1, b2, b3) are arranged into chains: every bead gets one chain position,
-// beads of a filament consecutive, links between consecutive positions and
-// each bend centred on its middle bead (FilamentStretching::vectorize,
-// Filament/FilamentStretching.cpp:24-44, FilamentBending::vectorize,
-// Filament/FilamentBending.cpp:28-66, produce exactly this structure).
-// Interactions that do not fit (a bead with two outgoing links, a bend whose
-// beads are not consecutive on a chain, links closing a cycle) stay on the
-// generic per-interaction path.
+// Internal order. At create the beads are put in filament-chain order:
+// walking the stretching links (b1 -> b2) from every bead without a
+// predecessor, in bead-index order, gives each bead a position p, beads of a
+// filament consecutive (FilamentStretching::vectorize,
+// Filament/FilamentStretching.cpp:24-44, and FilamentBending::vectorize,
+// Filament/FilamentBending.cpp:28-66, produce exactly this structure). The
+// handle stores coordinates, forces and every bead offset in that order and
+// converts at the host boundary, so the chain kernels read and write the
+// coordinate array as contiguous tiles.
 //
-// The force kernel stages a tile of chain positions (+2 on each side) in
-// shared memory, evaluates each link and each bend once, and writes each
-// bead's force with a plain store: no atomics, no index loads beyond one
-// offset per bead, and every bead (including beads on no chain) is written,
-// so the pass also initializes the force array for the potentials that add
-// atomically afterwards. The energy kernel evaluates the link and bend owned
-// by each position at up to kMaxLambda step sizes from one read of x and d.
+// Chains. A link (b1 -> b2) with pos[b2] == pos[b1] + 1 and a bend
+// (b1, b2, b3) with pos[b1] + 1 == pos[b2] == pos[b3] - 1 are evaluated
+// here; anything else (a second link out of a bead, links closing a cycle,
+// bends across chain ends, interactions of a later update that no longer fit
+// the order) stays on the generic per-interaction path.
+//
+// Both kernels work on warp tiles of consecutive positions: each lane loads
+// one position (coalesced, no index loads) and gets its neighbours by warp
+// shuffles, so there is no shared memory and no block barrier. The force
+// kernel evaluates each link and bend once and writes each bead's force with
+// a plain store; every bead is written, so the pass also initializes the
+// force array for the potentials that add atomically afterwards. The energy
+// kernel evaluates the link and bend owned by each position at up to
+// kMaxLambda step sizes from one read of x and d.
 #include <algorithm>
 #include <vector>
 
@@ -27,157 +35,134 @@ namespace mb {
 
 namespace {
 
-constexpr int kTile = 256;
+constexpr int kThreads = 256;
+constexpr int kWarpOut = 30;  // forces written per warp: lanes 1..30 of 32 centres
 constexpr unsigned char kLink = 1, kBend = 2;
+constexpr unsigned kFull = 0xffffffffu;
 
+__device__ __forceinline__ V3 shfl_up3(const V3& v) {
+    return V3{__shfl_up_sync(kFull, v.x, 1), __shfl_up_sync(kFull, v.y, 1), __shfl_up_sync(kFull, v.z, 1)};
+}
+__device__ __forceinline__ V3 shfl_down3(const V3& v) {
+    return V3{__shfl_down_sync(kFull, v.x, 1), __shfl_down_sync(kFull, v.y, 1), __shfl_down_sync(kFull, v.z, 1)};
+}
 template <class R>
-struct ChainSmem {
-    double cx[kTile + 4], cy[kTile + 4], cz[kTile + 4];  // positions p0-2 .. p0+T+1
-    R fs[kTile + 1][3];                                  // link (q, q+1) force on q+1, q = p0-1 .. p0+T-1
-    R fr1[kTile + 2][3], fr2[kTile + 2][3];              // bend centred at q = p0-1 .. p0+T
-    unsigned char fl[kTile + 2];                         // flags of q = p0-1 .. p0+T
-};
+__device__ __forceinline__ T3<R> shfl_up3(const T3<R>& v) {
+    return T3<R>{__shfl_up_sync(kFull, v.x, 1), __shfl_up_sync(kFull, v.y, 1), __shfl_up_sync(kFull, v.z, 1)};
+}
+template <class R>
+__device__ __forceinline__ T3<R> shfl_down3(const T3<R>& v) {
+    return T3<R>{__shfl_down_sync(kFull, v.x, 1), __shfl_down_sync(kFull, v.y, 1), __shfl_down_sync(kFull, v.z, 1)};
+}
 
+// Coordinates of internal position q (zero outside [0, n)).
+__device__ __forceinline__ V3 pos_of(const double* __restrict__ x, int n, int q) {
+    return (q >= 0 && q < n) ? load3(x + 3 * q) : V3{0.0, 0.0, 0.0};
+}
+
+// Forces. Each warp owns 32 consecutive centres q = p0-1 .. p0+30 (one per
+// lane): the lane loads its position, flags and parameters (coalesced, all
+// independent), gets its neighbours' coordinates by shuffles (lanes 0 and 31
+// load the one outside the warp), evaluates the link (q, q+1) and the bend
+// centred at q once, and lanes 1..30 sum the five terms acting on their
+// position from their neighbours by shuffles. No shared memory, no block
+// barriers; every position is written exactly once.
 template <class R>
-__global__ void __launch_bounds__(kTile) k_chain_forces(const ChainDev ch, const double* __restrict__ x,
-                                                       const ForceTarget tgt) {
+__global__ void __launch_bounds__(kThreads) k_chain_forces(const ChainDev ch, const double* __restrict__ x,
+                                                           const ForceTarget tgt) {
     if (tgt.skip && *tgt.skip) return;
-    __shared__ ChainSmem<R> S;
     double* __restrict__ f = target_force(tgt);
     const double* __restrict__ d = tgt.d;
     const double lam = tgt.lam ? *tgt.lam : 0.0;
     const int n = ch.n_pos;
-    for (int p0 = blockIdx.x * kTile; p0 < n; p0 += gridDim.x * kTile) {
-        // stage positions p0-2 .. p0+T+1 and flags p0-1 .. p0+T
-        for (int t = threadIdx.x; t < kTile + 4; t += kTile) {
-            const int q = p0 - 2 + t;
-            double X = 0, Y = 0, Z = 0;
-            if (q >= 0 && q < n) {
-                const int o = ch.bead[q];
-                X = x[o];
-                Y = x[o + 1];
-                Z = x[o + 2];
-                if (d) {
-                    X = move1(X, lam, d[o]);
-                    Y = move1(Y, lam, d[o + 1]);
-                    Z = move1(Z, lam, d[o + 2]);
-                }
-            }
-            S.cx[t] = X;
-            S.cy[t] = Y;
-            S.cz[t] = Z;
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; (long long)w * kWarpOut < n; w += nw) {
+        const int q = w * kWarpOut - 1 + lane;
+        const bool in = q >= 0 && q < n;
+        const int qe = lane == 0 ? q - 1 : q + 1;  // the halo position of lanes 0 and 31
+        V3 c = pos_of(x, n, q), ce{0.0, 0.0, 0.0};
+        if (lane == 0 || lane == 31) ce = pos_of(x, n, qe);
+        if (d) {
+            c = move3(c, lam, pos_of(d, n, q));
+            if (lane == 0 || lane == 31) ce = move3(ce, lam, pos_of(d, n, qe));
         }
-        for (int t = threadIdx.x; t < kTile + 2; t += kTile) {
-            const int q = p0 - 1 + t;
-            S.fl[t] = (q >= 0 && q < n) ? ch.flags[q] : 0;
+        const unsigned char fl = in ? ch.flags[q] : 0;
+        const double2 lp = in ? ch.link_p[q] : double2{0.0, 0.0};
+        const double2 bp = in ? ch.bend_p[q] : double2{0.0, 0.0};
+        V3 cprev = shfl_up3(c), cnext = shfl_down3(c);
+        if (lane == 0) cprev = ce;
+        if (lane == 31) cnext = ce;
+        T3<R> F{0, 0, 0}, A{0, 0, 0}, B{0, 0, 0};
+        if (fl & kLink) F = stretch_force<R>(c, cnext, lp.x, lp.y);
+        if (fl & kBend) bend_force<R>(diff<R>(cprev, c), diff<R>(c, cnext), bp.x, bp.y, A, B);
+        const T3<R> Fp = shfl_up3(F), Bp = shfl_up3(B), An = shfl_down3(A);
+        if (lane >= 1 && lane <= kWarpOut && in) {
+            // link (q-1, q) acts on q; link (q, q+1) reacts on q; bends centred
+            // at q-1 (third bead), q (middle), q+1 (first bead); summed in double
+            f[3 * q] = double(Fp.x) - double(F.x) + double(Bp.x) + (double(A.x) - double(B.x)) - double(An.x);
+            f[3 * q + 1] = double(Fp.y) - double(F.y) + double(Bp.y) + (double(A.y) - double(B.y)) - double(An.y);
+            f[3 * q + 2] = double(Fp.z) - double(F.z) + double(Bp.z) + (double(A.z) - double(B.z)) - double(An.z);
         }
-        __syncthreads();
-        // terms of centres q = p0-1+t for t in [0, T+2)
-        for (int t = threadIdx.x; t < kTile + 2; t += kTile) {
-            const int q = p0 - 1 + t;
-            const unsigned char fl = S.fl[t];
-            const int c = t + 1;  // index of position q in the coordinate tile
-            if (t < kTile + 1) {
-                T3<R> F{0, 0, 0};
-                if (fl & kLink) {
-                    double2 lp = ch.link_p[q];
-                    F = stretch_force<R>(V3{S.cx[c], S.cy[c], S.cz[c]}, V3{S.cx[c + 1], S.cy[c + 1], S.cz[c + 1]},
-                                         lp.x, lp.y);
-                }
-                S.fs[t][0] = F.x;
-                S.fs[t][1] = F.y;
-                S.fs[t][2] = F.z;
-            }
-            T3<R> A{0, 0, 0}, B{0, 0, 0};
-            if (fl & kBend) {
-                double2 bp = ch.bend_p[q];
-                V3 c0{S.cx[c - 1], S.cy[c - 1], S.cz[c - 1]}, c1{S.cx[c], S.cy[c], S.cz[c]},
-                    c2{S.cx[c + 1], S.cy[c + 1], S.cz[c + 1]};
-                bend_force<R>(diff<R>(c0, c1), diff<R>(c1, c2), bp.x, bp.y, A, B);
-            }
-            S.fr1[t][0] = A.x;
-            S.fr1[t][1] = A.y;
-            S.fr1[t][2] = A.z;
-            S.fr2[t][0] = B.x;
-            S.fr2[t][1] = B.y;
-            S.fr2[t][2] = B.z;
-        }
-        __syncthreads();
-        const int p = p0 + threadIdx.x;
-        if (p < n) {
-            const int t = threadIdx.x + 1;  // centre p in the term arrays
-            double out[3];
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                // link (p-1, p) acts on p; link (p, p+1) reacts on p;
-                // bends centred at p-1 (third bead), p (middle), p+1 (first bead);
-                // summed in double
-                out[k] = double(S.fs[t - 1][k]) - double(S.fs[t][k]) + double(S.fr2[t - 1][k]) +
-                         (double(S.fr1[t][k]) - double(S.fr2[t][k])) - double(S.fr1[t + 1][k]);
-            }
-            const int o = ch.bead[p];
-            f[o] = out[0];
-            f[o + 1] = out[1];
-            f[o + 2] = out[2];
-        }
-        __syncthreads();
     }
 }
 
+// Energies. Each warp owns 32 consecutive positions and each lane the link
+// and bend of its own position, at up to kMaxLambda step sizes from one read
+// of x and d. A fixed grid (grid-stride over warp tiles) keeps the per-block
+// partial sums deterministic.
 template <class R>
-__global__ void __launch_bounds__(kTile) k_chain_energy(const ChainDev ch, const double* __restrict__ x,
-                                                       const double* __restrict__ d,
-                                                       const LambdaSet* __restrict__ lset,
-                                                       double* __restrict__ partial, int nblk_total, int blk_off) {
+__global__ void __launch_bounds__(kThreads) k_chain_energy(const ChainDev ch, const double* __restrict__ x,
+                                                           const double* __restrict__ d,
+                                                           const LambdaSet* __restrict__ lset,
+                                                           double* __restrict__ partial, int nblk_total, int blk_off) {
     __shared__ double sm[4 * 32];
-    __shared__ double cx[2][kTile + 2], cy[2][kTile + 2], cz[2][kTile + 2];  // x and d, positions p0-1 .. p0+T
     const int n = ch.n_pos;
     const int K = lset ? lset->K : 1;
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
     double acc[kMaxLambda][2];
 #pragma unroll
     for (int k = 0; k < kMaxLambda; ++k) acc[k][0] = acc[k][1] = 0.0;
-    for (int p0 = blockIdx.x * kTile; p0 < n; p0 += gridDim.x * kTile) {
-        for (int t = threadIdx.x; t < kTile + 2; t += kTile) {
-            const int q = p0 - 1 + t;
-            double X = 0, Y = 0, Z = 0, DX = 0, DY = 0, DZ = 0;
-            if (q >= 0 && q < n) {
-                const int o = ch.bead[q];
-                X = x[o];
-                Y = x[o + 1];
-                Z = x[o + 2];
-                if (d) {
-                    DX = d[o];
-                    DY = d[o + 1];
-                    DZ = d[o + 2];
-                }
-            }
-            cx[0][t] = X; cy[0][t] = Y; cz[0][t] = Z;
-            cx[1][t] = DX; cy[1][t] = DY; cz[1][t] = DZ;
+    for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; (long long)w * 32 < n; w += nw) {
+        const int q = w * 32 + lane;
+        const bool in = q < n;
+        const int qe = lane == 0 ? q - 1 : q + 1;
+        const V3 c = pos_of(x, n, q), dc = d ? pos_of(d, n, q) : V3{0.0, 0.0, 0.0};
+        V3 ce{0.0, 0.0, 0.0}, de{0.0, 0.0, 0.0};
+        if (lane == 0 || lane == 31) {
+            ce = pos_of(x, n, qe);
+            if (d) de = pos_of(d, n, qe);
         }
-        __syncthreads();
-        const int p = p0 + threadIdx.x;
-        if (p < n) {
-            const unsigned char fl = ch.flags[p];
-            const int c = threadIdx.x + 1;
-            double2 lp = {0, 0}, bp = {0, 0};
-            if (fl & kLink) lp = ch.link_p[p];
-            if (fl & kBend) bp = ch.bend_p[p];
-            if (fl) {
-                for (int k = 0; k < K; ++k) {
-                    const double lam = lset ? lset->lam[k] : 0.0;
-                    auto P = [&](int i) {
-                        V3 v{cx[0][i], cy[0][i], cz[0][i]};
-                        return d ? move3(v, lam, V3{cx[1][i], cy[1][i], cz[1][i]}) : v;
-                    };
-                    const V3 pc = P(c), pn = P(c + 1);
-                    if (fl & kLink) acc[k][0] += stretch_energy<R>(pc, pn, lp.x, lp.y);
-                    if (fl & kBend) acc[k][1] += bend_energy<R>(diff<R>(P(c - 1), pc), diff<R>(pc, pn), bp.x, bp.y);
+        const unsigned char fl = in ? ch.flags[q] : 0;
+        const double2 lp = in ? ch.link_p[q] : double2{0.0, 0.0};
+        const double2 bp = in ? ch.bend_p[q] : double2{0.0, 0.0};
+        V3 cp = shfl_up3(c), cn = shfl_down3(c), dp = shfl_up3(dc), dn = shfl_down3(dc);
+        if (lane == 0) {
+            cp = ce;
+            dp = de;
+        }
+        if (lane == 31) {
+            cn = ce;
+            dn = de;
+        }
+        if (fl) {
+#pragma unroll
+            for (int k = 0; k < kMaxLambda; ++k) {
+                if (k >= K) break;
+                const double lam = lset ? lset->lam[k] : 0.0;
+                const V3 Pc = d ? move3(c, lam, dc) : c, Pn = d ? move3(cn, lam, dn) : cn;
+                if (fl & kLink) acc[k][0] += stretch_energy<R>(Pc, Pn, lp.x, lp.y);
+                if (fl & kBend) {
+                    const V3 Pp = d ? move3(cp, lam, dp) : cp;
+                    acc[k][1] += bend_energy<R>(diff<R>(Pp, Pc), diff<R>(Pc, Pn), bp.x, bp.y);
                 }
             }
         }
-        __syncthreads();
     }
-    for (int k = 0; k < K; ++k) {
+#pragma unroll
+    for (int k = 0; k < kMaxLambda; ++k) {
+        if (k >= K) break;
         double e[2] = {acc[k][0], acc[k][1]};
         block_sum<2>(e, sm);
         if (threadIdx.x == 0) {
@@ -190,21 +175,47 @@ __global__ void __launch_bounds__(kTile) k_chain_energy(const ChainDev ch, const
     }
 }
 
+// Reordering between the caller's bead order and the internal one:
+// internal position p holds external bead order[p].
+__global__ void k_to_internal(int n3, const int* __restrict__ order, const double* __restrict__ ext,
+                              double* __restrict__ in) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x) {
+        const int p = i / 3, k = i - 3 * p;
+        in[i] = ext[3 * order[p] + k];
+    }
+}
+
+__global__ void k_to_external(int n3, const int* __restrict__ order, const double* __restrict__ in,
+                              double* __restrict__ ext) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x) {
+        const int p = i / 3, k = i - 3 * p;
+        ext[3 * order[p] + k] = in[i];
+    }
+}
+
+int reorder_blocks(int n3) {
+    const int b = (n3 + kThreads - 1) / kThreads;
+    return b < 1 ? 1 : (b > 148 * 8 ? 148 * 8 : b);
+}
+
 }  // namespace
 
 int chain_blocks(const ChainDev& ch) {
-    int tiles = (ch.n_pos + kTile - 1) / kTile;
-    int cap = 148 * 4;
-    return tiles < cap ? (tiles < 1 ? 1 : tiles) : cap;
+    // energy: one 32-position tile per warp, at most 4 blocks per SM
+    const int per_block = 32 * (kThreads / 32);
+    const int b = (ch.n_pos + per_block - 1) / per_block;
+    const int cap = 148 * 4;
+    return b < 1 ? 1 : (b < cap ? b : cap);
 }
 
 void launch_chain_forces(const ChainDev& ch, int prec, const double* x, const ForceTarget& t, cudaStream_t s) {
     if (ch.n_pos <= 0) return;
-    const int g = (ch.n_pos + kTile - 1) / kTile;
+    const int per_block = kWarpOut * (kThreads / 32);
+    const int g = (ch.n_pos + per_block - 1) / per_block;
     if (prec == MEDYAN_PREC_MIXED)
-        k_chain_forces<float><<<g, kTile, 0, s>>>(ch, x, t);
+        k_chain_forces<float><<<g, kThreads, 0, s>>>(ch, x, t);
     else
-        k_chain_forces<double><<<g, kTile, 0, s>>>(ch, x, t);
+        k_chain_forces<double><<<g, kThreads, 0, s>>>(ch, x, t);
 }
 
 void launch_chain_energy(const ChainDev& ch, int prec, const double* x, const double* d, const LambdaSet* lam,
@@ -212,70 +223,69 @@ void launch_chain_energy(const ChainDev& ch, int prec, const double* x, const do
     if (ch.n_pos <= 0) return;
     const int g = chain_blocks(ch);
     if (prec == MEDYAN_PREC_MIXED)
-        k_chain_energy<float><<<g, kTile, 0, s>>>(ch, x, d, lam, partial, nblk_total, blk_off);
+        k_chain_energy<float><<<g, kThreads, 0, s>>>(ch, x, d, lam, partial, nblk_total, blk_off);
     else
-        k_chain_energy<double><<<g, kTile, 0, s>>>(ch, x, d, lam, partial, nblk_total, blk_off);
+        k_chain_energy<double><<<g, kThreads, 0, s>>>(ch, x, d, lam, partial, nblk_total, blk_off);
 }
 
-// Host: arrange stretching links and bends into chains. Returns the leftover
-// (non-chain) stretching and bending interaction indices.
-void build_chains(const medyan_system* s, ChainHost& out) {
+void launch_to_internal(int n3, const int* order, const double* ext, double* in, cudaStream_t s) {
+    if (n3 > 0) k_to_internal<<<reorder_blocks(n3), kThreads, 0, s>>>(n3, order, ext, in);
+}
+
+void launch_to_external(int n3, const int* order, const double* in, double* ext, cudaStream_t s) {
+    if (n3 > 0) k_to_external<<<reorder_blocks(n3), kThreads, 0, s>>>(n3, order, in, ext);
+}
+
+// Internal order: walk the stretching links from every bead without a
+// predecessor, in bead-index order; beads left unvisited lie on link cycles,
+// which are entered at their smallest bead. order[p] = external bead.
+void chain_order(const medyan_system* s, std::vector<int>& order) {
     const int nb = s->n_beads;
-    std::vector<int> next(nb, -1), prev(nb, -1), link_id(nb, -1);
-    out.left_stretch.clear();
-    out.left_bend.clear();
+    std::vector<int> next(nb, -1), prev(nb, -1);
     for (int i = 0; i < s->n_stretch; ++i) {
         const int a = s->stretch_beads[2 * i] / 3, c = s->stretch_beads[2 * i + 1] / 3;
         if (a != c && next[a] < 0 && prev[c] < 0) {
             next[a] = c;
             prev[c] = a;
-            link_id[a] = i;
-        } else {
-            out.left_stretch.push_back(i);
         }
     }
-    // break cycles: walk from every bead without a predecessor; beads left
-    // unvisited lie on cycles, whose link into the smallest bead is dropped
-    std::vector<int> pos(nb, -1);
-    std::vector<int> order;
+    std::vector<char> seen(nb, 0);
+    order.clear();
     order.reserve(nb);
     auto walk = [&](int h) {
-        for (int b = h; b >= 0 && pos[b] < 0; b = next[b]) {
-            pos[b] = (int)order.size();
+        for (int b = h; b >= 0 && !seen[b]; b = next[b]) {
+            seen[b] = 1;
             order.push_back(b);
         }
     };
     for (int b = 0; b < nb; ++b)
         if (prev[b] < 0) walk(b);
-    for (int b = 0; b < nb; ++b) {
-        if (pos[b] >= 0) continue;
-        // b is on an unvisited cycle; cut the link entering b
-        const int a = prev[b];
-        out.left_stretch.push_back(link_id[a]);
-        next[a] = -1;
-        link_id[a] = -1;
-        prev[b] = -1;
-        walk(b);
-    }
-    std::sort(out.left_stretch.begin(), out.left_stretch.end());
-    const int n = (int)order.size();
-    out.bead.assign(n, 0);
+    for (int b = 0; b < nb; ++b)
+        if (!seen[b]) walk(b);
+}
+
+// Chains over a fixed internal order (pos = inverse of order). Bead offsets in
+// s are external; the leftover lists index s's interactions.
+void build_chains(const medyan_system* s, const std::vector<int>& pos, ChainHost& out) {
+    const int n = s->n_beads;
+    out.left_stretch.clear();
+    out.left_bend.clear();
     out.flags.assign(n, 0);
     out.link_p.assign(n, make_double2(0, 0));
     out.bend_p.assign(n, make_double2(0, 0));
-    for (int p = 0; p < n; ++p) {
-        const int b = order[p];
-        out.bead[p] = 3 * b;
-        if (next[b] >= 0) {
+    for (int i = 0; i < s->n_stretch; ++i) {
+        const int p = pos[s->stretch_beads[2 * i] / 3], q = pos[s->stretch_beads[2 * i + 1] / 3];
+        if (q == p + 1 && !(out.flags[p] & kLink)) {
             out.flags[p] |= kLink;
-            const int i = link_id[b];
             out.link_p[p] = make_double2(s->stretch_k[i], s->stretch_l0[i]);
+        } else {
+            out.left_stretch.push_back(i);
         }
     }
     for (int i = 0; i < s->n_bend; ++i) {
-        const int b1 = s->bend_beads[3 * i] / 3, b2 = s->bend_beads[3 * i + 1] / 3, b3 = s->bend_beads[3 * i + 2] / 3;
-        const int p = pos[b2];
-        if (next[b1] == b2 && next[b2] == b3 && !(out.flags[p] & kBend)) {
+        const int p1 = pos[s->bend_beads[3 * i] / 3], p = pos[s->bend_beads[3 * i + 1] / 3],
+                  p3 = pos[s->bend_beads[3 * i + 2] / 3];
+        if (p1 == p - 1 && p3 == p + 1 && !(out.flags[p] & kBend)) {
             out.flags[p] |= kBend;
             out.bend_p[p] = make_double2(s->bend_k[i], s->bend_theta0[i]);
         } else {

@@ -10,6 +10,8 @@
 // reference's composite Simpson quadrature for them
 // (CylinderExclVolRepulsion::energyN/forceN, CylinderExclVolRepulsion.cpp:884-1256)
 // with all threads of the block splitting the grid.
+#include <mutex>
+
 #include "internal.h"
 #include "excl.cuh"
 
@@ -21,11 +23,11 @@ __device__ __forceinline__ V3 at(const V3& x, const V3& d, double lam, bool move
 
 template <class R>
 __global__ void __launch_bounds__(kExclBlock) k_excl_energy(const DeviceFF ff, const double* __restrict__ x,
-                                                        const double* __restrict__ d,
-                                                        const LambdaSet* __restrict__ lset,
-                                                        double* __restrict__ partial, int nblk_total, int blk_off,
-                                                        int* __restrict__ fb_count, int2* __restrict__ fb_list,
-                                                        int* __restrict__ bad) {
+                                                            const double* __restrict__ d,
+                                                            const LambdaSet* __restrict__ lset,
+                                                            double* __restrict__ partial, int nblk_total,
+                                                            int blk_off, int* __restrict__ fb_count,
+                                                            int2* __restrict__ fb_list, int* __restrict__ bad) {
     __shared__ double smem[4 * 32];
     const int i = blockIdx.x * kExclBlock + threadIdx.x;
     const bool move = d != nullptr;
@@ -39,7 +41,9 @@ __global__ void __launch_bounds__(kExclBlock) k_excl_energy(const DeviceFF ff, c
         if (move) { D[0] = load3(d + q.x); D[1] = load3(d + q.y); D[2] = load3(d + q.z); D[3] = load3(d + q.w); }
     }
     const int K = lset ? lset->K : 1;
-    for (int k = 0; k < K; ++k) {
+#pragma unroll
+    for (int k = 0; k < kMaxLambda; ++k) {
+        if (k >= K) break;
         const double lam = lset ? lset->lam[k] : 0.0;
         double e[1] = {0.0};
         if (valid) {
@@ -109,24 +113,30 @@ __device__ __forceinline__ Six six_of(const V3& c1, const V3& c2, const V3& c3, 
 }
 
 // Grid abscissae advance by repeated addition, as the reference's loops do
-// (s += deltas): grid[i] = value of s in iteration i.
-__device__ void fill_grid(double* grid, int n, double delta) {
-    if (threadIdx.x == 0) {
-        double s = 0.0;
-        for (int i = 0; i <= n; ++i) {
-            s += delta;
-            grid[i] = s;
-        }
+// (s += deltas): grid[i] = value of s in iteration i. Both grids are filled
+// once per device (init_excl_kernels) and read from global memory.
+__device__ double g_grid_energyN[400 + 1];
+__device__ double g_grid_forceN[10000 + 1];
+
+__global__ void k_fill_grids() {
+    double s = 0.0;
+    for (int i = 0; i <= 400; ++i) {
+        s += 1.0 / 400.0;
+        g_grid_energyN[i] = s;
     }
-    __syncthreads();
+    s = 0.0;
+    for (int i = 0; i <= 10000; ++i) {
+        s += 1.0 / 10000.0;
+        g_grid_forceN[i] = s;
+    }
 }
 
 // energyN: 400 x 400 composite Simpson sum (:884-999). Block-parallel over
 // the interior grid; T1..T4 are reduced separately and combined as written.
-__device__ double energyN_block(const Six& q, double kRS, double* grid, double* red) {
+__device__ double energyN_block(const Six& q, double kRS, double* red) {
     const int N = 400;
     const double ds = 1.0 / double(N), dt = 1.0 / double(N);
-    fill_grid(grid, N, ds);
+    const double* __restrict__ grid = g_grid_energyN;
     auto g = [&](double s, double t) {
         double r_2 = r2_of(q.a, q.b, q.c, q.d, q.e, q.F, s, t);
         return (1.0 / (r_2 * r_2));
@@ -153,7 +163,7 @@ __device__ double energyN_block(const Six& q, double kRS, double* grid, double* 
 
 // forceN: 10^4 x 10^4 composite Simpson sums of the six force integrands,
 // then the bead forces of :1133-1148. Returns true when finite.
-__device__ bool forceN_block(V3 c1, V3 c2, const V3& c3, const V3& c4, double kRS, bool movebeads, double* grid,
+__device__ bool forceN_block(V3 c1, V3 c2, const V3& c3, const V3& c4, double kRS, bool movebeads,
                              double* red, double (&out)[4][3]) {
     if (movebeads && in_plane(c1, c2, c3, c4)) {
         // movePointOutOfPlane for beads 2 and 1, both along the normal of the
@@ -171,7 +181,7 @@ __device__ bool forceN_block(V3 c1, V3 c2, const V3& c3, const V3& c4, double kR
     const Six q = six_of(c1, c2, c3, c4);
     const int N = 10000;
     const double ds = 1.0 / double(N), dt = 1.0 / double(N);
-    fill_grid(grid, N, ds);
+    const double* __restrict__ grid = g_grid_forceN;
     double T[6] = {0, 0, 0, 0, 0, 0};
     auto acc = [&](double s, double t, double w) {
         double r_2 = r2_of(q.a, q.b, q.c, q.d, q.e, q.F, s, t);
@@ -221,7 +231,6 @@ __global__ void __launch_bounds__(kBlock) k_excl_force_fallback(const DeviceFF f
                                                                 const ForceTarget tgt, int* __restrict__ fb_count,
                                                                 const int* __restrict__ fb_list,
                                                                 int* __restrict__ status) {
-    extern __shared__ double grid[];  // 10001 abscissae
     __shared__ double red[6 * 32];
     const int n = min(*fb_count, kFallbackCap);
     if (n == 0) return;
@@ -233,8 +242,8 @@ __global__ void __launch_bounds__(kBlock) k_excl_force_fallback(const DeviceFF f
         const V3 c1 = pos_at(x, tgt, lam, q.x), c2 = pos_at(x, tgt, lam, q.y), c3 = pos_at(x, tgt, lam, q.z),
                  c4 = pos_at(x, tgt, lam, q.w);
         double out[4][3];
-        bool ok = forceN_block(c1, c2, c3, c4, ff.excl_krs[i], false, grid, red, out);
-        if (!ok) ok = forceN_block(c1, c2, c3, c4, ff.excl_krs[i], true, grid, red, out);
+        bool ok = forceN_block(c1, c2, c3, c4, ff.excl_krs[i], false, red, out);
+        if (!ok) ok = forceN_block(c1, c2, c3, c4, ff.excl_krs[i], true, red, out);
         if (threadIdx.x == 0) {
             if (ok) {
                 add_force(f, q.x, out[0][0], out[0][1], out[0][2]);
@@ -251,20 +260,23 @@ __global__ void __launch_bounds__(kBlock) k_excl_force_fallback(const DeviceFF f
     if (threadIdx.x == 0) *fb_count = 0;
 }
 
-// Sums the per-block energy partials of each force field (one warp per
-// (lambda, slot), fixed order), evaluates the energyN fallback for queued
-// pairs in (slot, pair) order, and applies ForceFieldManager::computeEnergy's
-// rule (ForceFieldManager.cpp:137-176): a force field at or below -1 makes the
+constexpr int kFinishThreads = 512;
+
+// Sums the per-block energy partials of each force field (each thread takes
+// rows threadIdx.x, +512, ... and adds every row's values into its force-field
+// slots; then one block reduction: a fixed order, so the result is
+// deterministic), evaluates the energyN fallback for queued pairs in (slot,
+// pair) order, and applies ForceFieldManager::computeEnergy's rule
+// (ForceFieldManager.cpp:137-176): a force field at or below -1 makes the
 // total +inf.
-__global__ void __launch_bounds__(kBlock) k_energy_finish(const DeviceFF ff, const double* __restrict__ x,
-                                                          const double* __restrict__ d,
-                                                          const LambdaSet* __restrict__ lset,
-                                                          const double* __restrict__ partial, int nch, int nbb,
-                                                          int nbe, int* __restrict__ fb_count,
-                                                          int2* __restrict__ fb_list, int* __restrict__ bad,
-                                                          double* __restrict__ out) {
-    __shared__ double grid[401];
-    __shared__ double red[4 * 32];
+__global__ void __launch_bounds__(kFinishThreads) k_energy_finish(const DeviceFF ff, const double* __restrict__ x,
+                                                                  const double* __restrict__ d,
+                                                                  const LambdaSet* __restrict__ lset,
+                                                                  const double* __restrict__ partial, int nch,
+                                                                  int nbb, int nbe, int* __restrict__ fb_count,
+                                                                  int2* __restrict__ fb_list, int* __restrict__ bad,
+                                                                  double* __restrict__ out) {
+    __shared__ double red[kMaxLambda * MEDYAN_FF_COUNT * 32];
     __shared__ double sums[kMaxLambda][MEDYAN_FF_COUNT];
     __shared__ double fbE[kMaxLambda];
     __shared__ int nfb;
@@ -296,36 +308,57 @@ __global__ void __launch_bounds__(kBlock) k_energy_finish(const DeviceFF ff, con
             V3 X = load3(x + offs[j]);
             P[j] = d ? move3(X, lam, load3(d + offs[j])) : X;
         }
-        double U = energyN_block(six_of(P[0], P[1], P[2], P[3]), ff.excl_krs[q.x], grid, red);
+        double U = energyN_block(six_of(P[0], P[1], P[2], P[3]), ff.excl_krs[q.x], red);
         if (threadIdx.x == 0) {
             if (excl_energy_bad(U)) atomicOr(bad + q.y, 1);
             else fbE[q.y] += U;
         }
         __syncthreads();
     }
-    // per-slot sums: warp w handles combos w, w + nwarps, ...
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-    for (int combo = warp; combo < K * MEDYAN_FF_COUNT; combo += nwarp) {
-        const int k = combo / MEDYAN_FF_COUNT, slot = combo % MEDYAN_FF_COUNT;
-        // row ranges: chain rows [0, nch), bonded rows nch + seg[], excluded-volume rows after
-        int b0 = 0, b1 = 0, j = 0, c0 = 0, c1 = 0, cj = 0;
-        switch (slot) {
-            case 0: c0 = 0; c1 = nch; cj = 0; b0 = nch + ff.seg[0]; b1 = nch + ff.seg[1]; break;
-            case 1: c0 = 0; c1 = nch; cj = 1; b0 = nch + ff.seg[1]; b1 = nch + ff.seg[2]; break;
-            case 2: b0 = nch + ff.seg[2]; b1 = nch + ff.seg[3]; break;
-            case 3: b0 = nch + ff.seg[3]; b1 = nch + ff.seg[4]; break;
-            case 4: case 5: case 6: case 7: b0 = nch + ff.seg[4]; b1 = nch + ff.seg[5]; j = slot - 4; break;
-            case 8: b0 = nch + nbb; b1 = nch + nbb + nbe; break;
-            default: b0 = nch + ff.seg[5]; b1 = nch + ff.seg[6]; break;
-        }
-        const double* base = partial + (size_t)k * total_blocks * 4;
-        double s = 0.0, s2 = 0.0;
-        for (int b = c0 + lane; b < c1; b += 32) s2 += base[(size_t)b * 4 + cj];
-        for (int b = b0 + lane; b < b1; b += 32) s += base[(size_t)b * 4 + j];
-        s += s2;
+    // per-slot sums. Row r's four values go to slots (sx, sy, sz, sw), -1 = none:
+    // chain rows (stretch, bend), bonded segments (one slot; the branch segment
+    // four), excluded-volume rows.
+    double acc[kMaxLambda * MEDYAN_FF_COUNT];
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-        if (lane == 0) sums[k][slot] = s;
+    for (int j = 0; j < kMaxLambda * MEDYAN_FF_COUNT; ++j) acc[j] = 0.0;
+#pragma unroll 2
+    for (int r = threadIdx.x; r < total_blocks; r += blockDim.x) {
+        int sx = 8, sy = -1, sz = -1, sw = -1;
+        if (r < nch) {
+            sx = 0;
+            sy = 1;
+        } else if (r < nch + nbb) {
+            const int b = r - nch;
+            int sg = 0;
+            while (sg < 5 && b >= ff.seg[sg + 1]) ++sg;
+            sx = sg < 4 ? sg : (sg == 4 ? 4 : MEDYAN_FF_BOUNDARY);
+            if (sg == 4) {
+                sy = 5;
+                sz = 6;
+                sw = 7;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kMaxLambda; ++k) {
+            if (k < K) {
+                const double* p = partial + ((size_t)k * total_blocks + r) * 4;
+                const double vx = __ldcg(p), vy = __ldcg(p + 1), vz = __ldcg(p + 2), vw = __ldcg(p + 3);
+#pragma unroll
+                for (int j = 0; j < MEDYAN_FF_COUNT; ++j) {
+                    double a = acc[k * MEDYAN_FF_COUNT + j];
+                    if (sx == j) a += vx;
+                    if (sy == j) a += vy;
+                    if (sz == j) a += vz;
+                    if (sw == j) a += vw;
+                    acc[k * MEDYAN_FF_COUNT + j] = a;
+                }
+            }
+        }
+    }
+    block_sum<kMaxLambda * MEDYAN_FF_COUNT>(acc, red);
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < kMaxLambda; ++k)
+            for (int j = 0; j < MEDYAN_FF_COUNT; ++j) sums[k][j] = acc[k * MEDYAN_FF_COUNT + j];
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -367,7 +400,7 @@ void launch_excl_energy(const DeviceFF& ff, int prec, const double* x, const dou
 
 void launch_excl_energy_fallback_and_finish(const DeviceFF& ff, const double* x, const double* d,
                                             const LambdaSet* lam, const EnergyScratch& es, cudaStream_t s) {
-    k_energy_finish<<<1, kBlock, 0, s>>>(ff, x, d, lam, es.partial, es.n_blocks_chain, es.n_blocks_bonded,
+    k_energy_finish<<<1, kFinishThreads, 0, s>>>(ff, x, d, lam, es.partial, es.n_blocks_chain, es.n_blocks_bonded,
                                          es.n_blocks_excl, es.fb_count, es.fb_list, es.bad, es.out);
 }
 
@@ -377,11 +410,27 @@ void launch_excl_forces(const DeviceFF& ff, int prec, const double* x, const For
     if (nbe <= 0) return;
     (void)prec;  // FP64 in both modes, as for the energy
     k_excl_forces<double><<<nbe, kExclBlock, 0, s>>>(ff, x, t, fs.fb_count, fs.fb_list, fs.status);
-    k_excl_force_fallback<<<1, kBlock, kForceNGridBytes, s>>>(ff, x, t, fs.fb_count, fs.fb_list, fs.status);
+    k_excl_force_fallback<<<1, kBlock, 0, s>>>(ff, x, t, fs.fb_count, fs.fb_list, fs.status);
 }
 
 cudaError_t init_excl_kernels() {
-    return cudaFuncSetAttribute(k_excl_force_fallback, cudaFuncAttributeMaxDynamicSharedMemorySize, kForceNGridBytes);
+    static std::mutex mu;
+    static bool filled[64];
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(mu);
+    if (filled[dev]) return cudaSuccess;
+    cudaStream_t s = nullptr;
+    e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return e;
+    k_fill_grids<<<1, 1, 0, s>>>();
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+    if (e == cudaSuccess) filled[dev] = true;
+    return e;
 }
 
 }  // namespace mb

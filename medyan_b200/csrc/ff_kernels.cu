@@ -16,23 +16,29 @@ namespace mb {
 
 namespace {
 
+// Segment of global bonded block b, among segments [S0, S1).
+template <int S0, int S1>
 __device__ __forceinline__ int segment_of(const DeviceFF& ff, int b) {
-    int s = 0;
+    int s = S0;
 #pragma unroll
-    for (int q = 1; q < 6; ++q) s += (b >= ff.seg[q]) ? 1 : 0;
+    for (int q = S0 + 1; q < S1; ++q) s += (b >= ff.seg[q]) ? 1 : 0;
     return s;
 }
 
+// Segment c is compiled into the instantiation for [S0, S1).
+template <int S0, int S1>
+__device__ constexpr bool has_seg(int c) { return S0 <= c && c < S1; }
+
 __device__ __forceinline__ V3 at(const V3& x, const V3& d, double lam, bool move) { return move ? move3(x, lam, d) : x; }
 
-template <class R>
+template <class R, int S0, int S1>
 __global__ void __launch_bounds__(kBlock) k_bonded_energy(const DeviceFF ff, const double* __restrict__ x,
                                                           const double* __restrict__ d,
                                                           const LambdaSet* __restrict__ lset,
                                                           double* __restrict__ partial, int nblk_total, int blk_off) {
     __shared__ double smem[4 * 32];
-    const int b = blockIdx.x;
-    const int s = segment_of(ff, b);
+    const int b = blockIdx.x + ff.seg[S0];
+    const int s = segment_of<S0, S1>(ff, b);
     const int i = (b - ff.seg[s]) * kBlock + threadIdx.x;
     const bool move = d != nullptr;
     V3 X[4] = {}, D[4] = {};
@@ -42,7 +48,7 @@ __global__ void __launch_bounds__(kBlock) k_bonded_energy(const DeviceFF ff, con
     int plane = 0;
     switch (s) {
         case 0:
-            if (i < ff.n_stretch) {
+            if (has_seg<S0, S1>(0) && i < ff.n_stretch) {
                 int2 q = ff.stretch_bs[i];
                 double2 p = ff.stretch_p[i];
                 pa = double4{p.x, p.y, 0, 0};
@@ -53,7 +59,7 @@ __global__ void __launch_bounds__(kBlock) k_bonded_energy(const DeviceFF ff, con
             }
             break;
         case 1:
-            if (i < ff.n_bend) {
+            if (has_seg<S0, S1>(1) && i < ff.n_bend) {
                 int4 q = ff.bend_bs[i];
                 double2 p = ff.bend_p[i];
                 pa = double4{p.x, p.y, 0, 0};
@@ -67,7 +73,7 @@ __global__ void __launch_bounds__(kBlock) k_bonded_energy(const DeviceFF ff, con
         case 2:
         case 3: {
             const int n = s == 2 ? ff.n_linker : ff.n_motor;
-            if (i < n) {
+            if ((has_seg<S0, S1>(2) || has_seg<S0, S1>(3)) && i < n) {
                 int4 q = s == 2 ? ff.linker_bs[i] : ff.motor_bs[i];
                 pa = s == 2 ? ff.linker_p[i] : ff.motor_p[i];
                 X[0] = load3(x + q.x);
@@ -82,7 +88,7 @@ __global__ void __launch_bounds__(kBlock) k_bonded_energy(const DeviceFF ff, con
             break;
         }
         case 4:
-            if (i < ff.n_branch) {
+            if (has_seg<S0, S1>(4) && i < ff.n_branch) {
                 int4 q = ff.branch_bs[i];
                 pa = ff.branch_pa[i];
                 pb = ff.branch_pb[i];
@@ -97,7 +103,7 @@ __global__ void __launch_bounds__(kBlock) k_bonded_energy(const DeviceFF ff, con
             }
             break;
         default:
-            if (i < ff.n_boundary) {
+            if (has_seg<S0, S1>(5) && i < ff.n_boundary) {
                 int o = ff.boundary_bs[i];
                 double2 p = ff.boundary_p[i];
                 plane = ff.boundary_plane[i];
@@ -110,24 +116,38 @@ __global__ void __launch_bounds__(kBlock) k_bonded_energy(const DeviceFF ff, con
     }
     (void)nb;
     const int K = lset ? lset->K : 1;
-    for (int k = 0; k < K; ++k) {
+#pragma unroll
+    for (int k = 0; k < kMaxLambda; ++k) {
+        if (k >= K) break;
         const double lam = lset ? lset->lam[k] : 0.0;
         double e[4] = {0.0, 0.0, 0.0, 0.0};
         if (valid) {
             V3 P0 = at(X[0], D[0], lam, move), P1 = at(X[1], D[1], lam, move);
             V3 P2 = at(X[2], D[2], lam, move), P3 = at(X[3], D[3], lam, move);
             switch (s) {
-                case 0: e[0] = stretch_energy<R>(P0, P1, pa.x, pa.y); break;
-                case 1: e[0] = bend_energy<R>(diff<R>(P0, P1), diff<R>(P1, P2), pa.x, pa.y); break;
-                case 2:
-                case 3: e[0] = spring_energy<R>(P0, P1, P2, P3, pa.x, pa.y, pa.z, pa.w); break;
-                case 4:
-                    if (ff.branch_mask & 1) e[0] = branch_stretch_energy<R>(P0, P1, P2, pa.y, pa.z, pa.x);
-                    if (ff.branch_mask & 2) e[1] = bend_energy<R>(diff<R>(P0, P1), diff<R>(P2, P3), pa.w, pb.x);
-                    if (ff.branch_mask & 4) e[2] = branch_dihedral_energy<R>(P0, P1, P2, P3, pb.y, pa.x);
-                    if (ff.branch_mask & 8) e[3] = branch_position_energy<R>(P0, P1, P2, pb.z, pa.x);
+                case 0:
+                    if constexpr (has_seg<S0, S1>(0)) e[0] = stretch_energy<R>(P0, P1, pa.x, pa.y);
                     break;
-                default: e[0] = boundary_energy<R>(ff.planes[plane], P0, pa.x, pa.y); break;
+                case 1:
+                    if constexpr (has_seg<S0, S1>(1))
+                        e[0] = bend_energy<R>(diff<R>(P0, P1), diff<R>(P1, P2), pa.x, pa.y);
+                    break;
+                case 2:
+                case 3:
+                    if constexpr (has_seg<S0, S1>(2) || has_seg<S0, S1>(3))
+                        e[0] = spring_energy<R>(P0, P1, P2, P3, pa.x, pa.y, pa.z, pa.w);
+                    break;
+                case 4:
+                    if constexpr (has_seg<S0, S1>(4)) {
+                        if (ff.branch_mask & 1) e[0] = branch_stretch_energy<R>(P0, P1, P2, pa.y, pa.z, pa.x);
+                        if (ff.branch_mask & 2) e[1] = bend_energy<R>(diff<R>(P0, P1), diff<R>(P2, P3), pa.w, pb.x);
+                        if (ff.branch_mask & 4) e[2] = branch_dihedral_energy<R>(P0, P1, P2, P3, pb.y, pa.x);
+                        if (ff.branch_mask & 8) e[3] = branch_position_energy<R>(P0, P1, P2, pb.z, pa.x);
+                    }
+                    break;
+                default:
+                    if constexpr (has_seg<S0, S1>(5)) e[0] = boundary_energy<R>(ff.planes[plane], P0, pa.x, pa.y);
+                    break;
             }
         }
         block_sum<4>(e, smem);
@@ -152,18 +172,18 @@ struct PosLoader {
     }
 };
 
-template <class R>
+template <class R, int S0, int S1>
 __global__ void __launch_bounds__(kBlock) k_bonded_forces(const DeviceFF ff, const double* __restrict__ x,
                                                           const ForceTarget tgt) {
     if (tgt.skip && *tgt.skip) return;
     double* __restrict__ f = target_force(tgt);
     const PosLoader P{x, tgt.d, tgt.lam ? *tgt.lam : 0.0};
-    const int b = blockIdx.x;
-    const int s = segment_of(ff, b);
+    const int b = blockIdx.x + ff.seg[S0];
+    const int s = segment_of<S0, S1>(ff, b);
     const int i = (b - ff.seg[s]) * kBlock + threadIdx.x;
     switch (s) {
         case 0:
-            if (i < ff.n_stretch) {
+            if (has_seg<S0, S1>(0) && i < ff.n_stretch) {
                 int2 q = ff.stretch_bs[i];
                 double2 p = ff.stretch_p[i];
                 T3<R> F = stretch_force<R>(P(q.x), P(q.y), p.x, p.y);
@@ -172,7 +192,7 @@ __global__ void __launch_bounds__(kBlock) k_bonded_forces(const DeviceFF ff, con
             }
             break;
         case 1:
-            if (i < ff.n_bend) {
+            if (has_seg<S0, S1>(1) && i < ff.n_bend) {
                 int4 q = ff.bend_bs[i];
                 double2 p = ff.bend_p[i];
                 V3 c1 = P(q.x), c2 = P(q.y), c3 = P(q.z);
@@ -186,7 +206,7 @@ __global__ void __launch_bounds__(kBlock) k_bonded_forces(const DeviceFF ff, con
         case 2:
         case 3: {
             const int n = s == 2 ? ff.n_linker : ff.n_motor;
-            if (i < n) {
+            if ((has_seg<S0, S1>(2) || has_seg<S0, S1>(3)) && i < n) {
                 int4 q = s == 2 ? ff.linker_bs[i] : ff.motor_bs[i];
                 double4 p = s == 2 ? ff.linker_p[i] : ff.motor_p[i];
                 T3<R> Fl = spring_force<R>(P(q.x), P(q.y), P(q.z), P(q.w), p.x, p.y, p.z, p.w);
@@ -199,7 +219,7 @@ __global__ void __launch_bounds__(kBlock) k_bonded_forces(const DeviceFF ff, con
             break;
         }
         case 4:
-            if (i < ff.n_branch) {
+            if (has_seg<S0, S1>(4) && i < ff.n_branch) {
                 int4 q = ff.branch_bs[i];
                 double4 pa = ff.branch_pa[i], pb = ff.branch_pb[i];
                 V3 c1 = P(q.x), c2 = P(q.y), c3 = P(q.z), c4 = P(q.w);
@@ -241,7 +261,7 @@ __global__ void __launch_bounds__(kBlock) k_bonded_forces(const DeviceFF ff, con
             }
             break;
         default:
-            if (i < ff.n_boundary) {
+            if (has_seg<S0, S1>(5) && i < ff.n_boundary) {
                 int o = ff.boundary_bs[i];
                 double2 p = ff.boundary_p[i];
                 double4 pl = ff.planes[ff.boundary_plane[i]];
@@ -256,33 +276,84 @@ __global__ void __launch_bounds__(kBlock) k_bonded_forces(const DeviceFF ff, con
 
 int bonded_blocks(const DeviceFF& ff) { return ff.seg[6]; }
 
-void launch_energy(const ChainDev& ch, const DeviceFF& ff, int prec, const double* x, const double* d,
-                   const LambdaSet* lam, const EnergyScratch& es, cudaStream_t s) {
-    const int nbb = es.n_blocks_bonded;
-    const int total = es.total();
-    launch_chain_energy(ch, prec, x, d, lam, es.partial, total, 0, s);
-    if (nbb > 0) {
-        if (prec == MEDYAN_PREC_MIXED)
-            k_bonded_energy<float><<<nbb, kBlock, 0, s>>>(ff, x, d, lam, es.partial, total, es.n_blocks_chain);
-        else
-            k_bonded_energy<double><<<nbb, kBlock, 0, s>>>(ff, x, d, lam, es.partial, total, es.n_blocks_chain);
+namespace {
+
+// Bonded kernels are launched per group of segments, so each group gets the
+// registers its own potentials need: filament leftovers [0, 2), linker and
+// motor [2, 4), branching [4, 5), boundary [5, 6).
+template <int S0, int S1>
+void bonded_energy_group(const DeviceFF& ff, const double* x, const double* d, const LambdaSet* lam,
+                         const EnergyScratch& es, cudaStream_t s) {
+    const int nb = ff.seg[S1] - ff.seg[S0];
+    if (nb > 0)
+        k_bonded_energy<double, S0, S1><<<nb, kBlock, 0, s>>>(ff, x, d, lam, es.partial, es.total(),
+                                                               es.n_blocks_chain);
+}
+
+template <int S0, int S1>
+void bonded_forces_group(const DeviceFF& ff, int prec, const double* x, const ForceTarget& t, cudaStream_t s) {
+    const int nb = ff.seg[S1] - ff.seg[S0];
+    if (nb <= 0) return;
+    if (prec == MEDYAN_PREC_MIXED)
+        k_bonded_forces<float, S0, S1><<<nb, kBlock, 0, s>>>(ff, x, t);
+    else
+        k_bonded_forces<double, S0, S1><<<nb, kBlock, 0, s>>>(ff, x, t);
+}
+
+void fork_to(const Fork* fk, cudaStream_t s, int n) {
+    cudaEventRecord(fk->fork, s);
+    for (int k = 0; k < n; ++k) cudaStreamWaitEvent(fk->side[k], fk->fork, 0);
+}
+
+void join_from(const Fork* fk, cudaStream_t s, int n) {
+    for (int k = 0; k < n; ++k) {
+        cudaEventRecord(fk->join[k], fk->side[k]);
+        cudaStreamWaitEvent(s, fk->join[k], 0);
     }
-    launch_excl_energy(ff, prec, x, d, lam, es, s);
+}
+
+}  // namespace
+
+void launch_energy(const ChainDev& ch, const DeviceFF& ff, int prec, const double* x, const double* d,
+                   const LambdaSet* lam, const EnergyScratch& es, cudaStream_t s, const Fork* fk) {
+    // Energies are evaluated in double in both precision modes: the backtracking
+    // line search compares totals whose differences are ~1e-9 of the total,
+    // below float resolution per term. Only the force pass runs in float.
+    (void)prec;
+    // three branches: chain + boundary + filament leftovers | linker, motor,
+    // branching | excluded volume; then the finish kernel
+    cudaStream_t s1 = s, s2 = s;
+    if (fk) {
+        fork_to(fk, s, 2);
+        s1 = fk->side[0];
+        s2 = fk->side[1];
+    }
+    launch_excl_energy(ff, prec, x, d, lam, es, s2);
+    bonded_energy_group<2, 4>(ff, x, d, lam, es, s1);
+    bonded_energy_group<4, 5>(ff, x, d, lam, es, s1);
+    launch_chain_energy(ch, MEDYAN_PREC_FP64, x, d, lam, es.partial, es.total(), 0, s);
+    bonded_energy_group<5, 6>(ff, x, d, lam, es, s);
+    bonded_energy_group<0, 2>(ff, x, d, lam, es, s);
+    if (fk) join_from(fk, s, 2);
     launch_excl_energy_fallback_and_finish(ff, x, d, lam, es, s);
 }
 
 void launch_forces(const ChainDev& ch, const DeviceFF& ff, int prec, const double* x, const ForceTarget& t,
-                   const ForceScratch& fs, cudaStream_t s) {
-    // the chain pass stores every bead's force; everything after adds
+                   const ForceScratch& fs, cudaStream_t s, const Fork* fk) {
+    // the chain pass stores every bead's force; everything after adds, in two
+    // branches: excluded volume | bonded groups
     launch_chain_forces(ch, prec, x, t, s);
-    const int nbb = bonded_blocks(ff);
-    if (nbb > 0) {
-        if (prec == MEDYAN_PREC_MIXED)
-            k_bonded_forces<float><<<nbb, kBlock, 0, s>>>(ff, x, t);
-        else
-            k_bonded_forces<double><<<nbb, kBlock, 0, s>>>(ff, x, t);
+    cudaStream_t s1 = s;
+    if (fk) {
+        fork_to(fk, s, 1);
+        s1 = fk->side[0];
     }
+    bonded_forces_group<2, 4>(ff, prec, x, t, s1);
+    bonded_forces_group<4, 5>(ff, prec, x, t, s1);
+    bonded_forces_group<5, 6>(ff, prec, x, t, s1);
+    bonded_forces_group<0, 2>(ff, prec, x, t, s1);
     launch_excl_forces(ff, prec, x, t, fs, s);
+    if (fk) join_from(fk, s, 1);
 }
 
 }  // namespace mb

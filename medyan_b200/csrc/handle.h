@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstddef>
 #include <cstdint>
+#include <vector>
 
 #include "internal.h"
 
@@ -104,14 +105,27 @@ struct medyan_mech {
     int prec = 0;
     int n_beads = 0;
     cudaStream_t stream = nullptr;
+    mb::Fork fork{};                      // side streams of the passes
+
+    // standalone passes at the handle's coordinates as instantiated graphs:
+    // [0] energy, [1] forces, [2] energy then forces
+    cudaGraphExec_t pass_graph[3] = {nullptr, nullptr, nullptr};
+    long long pass_graph_gen[3] = {-1, -1, -1};
 
     mb::DeviceFF ff{};
     mb::EnergyScratch es{};
     mb::ForceScratch fs{};
 
+    // internal bead order (chain.cu), fixed at create: internal position p
+    // holds the caller's bead order_host[p]; pos_host is the inverse.
+    // Coordinates, forces and all bead offsets on the device are internal.
+    std::vector<int> order_host, pos_host;
+    bool identity_order = true;
+    mb::DevBuf<int> order;       // device copy of order_host (empty when identity)
+    mb::DevBuf<double> stage;    // 3*n_beads staging for reordered transfers
+
     // filament chains (chain.cu)
     mb::ChainDev chain{};
-    mb::DevBuf<int> chain_bead;
     mb::DevBuf<unsigned char> chain_flags;
     mb::DevBuf<double2> chain_link_p, chain_bend_p;
 
@@ -157,5 +171,14 @@ medyan_status refresh_device_ff(medyan_mech* h);
 medyan_status sync_status(medyan_mech* h);
 void enqueue_energy(medyan_mech* h, const double* x, const double* d, const LambdaSet* lam, cudaStream_t s);
 void enqueue_forces(medyan_mech* h, const double* x, double* f, cudaStream_t s);
+// Energy (kPassEnergy), forces (kPassForces) or both at h->x into h->es.out /
+// h->f, launched as the handle's graph for that pass (rebuilt when the force
+// fields change).
+constexpr int kPassEnergy = 0, kPassForces = 1, kPassBoth = 2;
+cudaError_t launch_pass(medyan_mech* h, int which);
+// Host coordinates/forces (caller's bead order) to and from internal device
+// arrays; stream-ordered on s (the host buffer must stay valid until s syncs).
+cudaError_t coords_to_device(medyan_mech* h, const double* host, double* dev, cudaStream_t s);
+cudaError_t coords_to_host(medyan_mech* h, const double* dev, double* host, cudaStream_t s);
 void destroy_nl(medyan_mech* h);
 }  // namespace mb

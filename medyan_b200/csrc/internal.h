@@ -35,18 +35,16 @@ struct DeviceFF {
     int seg[7];
 };
 
-// Filament chains (chain.cu): one position per bead, links between
-// consecutive positions, bends centred on positions.
+// Filament chains (chain.cu) over the internal bead order: chain position p
+// is internal bead p (coordinate offset 3p).
 struct ChainDev {
-    int n_pos;
-    const int* bead;             // coordinate offset of each position
+    int n_pos;                   // = n_beads
     const unsigned char* flags;  // bit 0: link (p, p+1); bit 1: bend centred at p
     const double2* link_p;       // (k, l0) of link (p, p+1)
     const double2* bend_p;       // (k, theta0) of the bend centred at p
 };
 
 struct ChainHost {
-    std::vector<int> bead;
     std::vector<unsigned char> flags;
     std::vector<double2> link_p, bend_p;
     std::vector<int> left_stretch, left_bend;  // interactions kept on the generic path
@@ -95,17 +93,31 @@ struct ForceScratch {
     int* status;          // bit 0: fallback failed, bit 1: queue overflow
 };
 
+// Two side streams and their events. A pass launched with a Fork runs its
+// independent kernels on separate streams joined back into the caller's
+// stream; under stream capture the fork and join become graph edges, so the
+// kernels are parallel branches of the graph.
+struct Fork {
+    cudaStream_t side[2];
+    cudaEvent_t fork, join[2];
+};
+
 // Launchers (ff_kernels.cu / excl_kernels.cu / chain.cu). prec: MEDYAN_PREC_*.
 // The chain pass writes every bead's force first; the other passes add.
+// fk may be null (everything on s, in order).
 void launch_energy(const ChainDev& ch, const DeviceFF& ff, int prec, const double* x, const double* d,
-                   const LambdaSet* lam, const EnergyScratch& es, cudaStream_t s);
+                   const LambdaSet* lam, const EnergyScratch& es, cudaStream_t s, const Fork* fk = nullptr);
 void launch_forces(const ChainDev& ch, const DeviceFF& ff, int prec, const double* x, const ForceTarget& t,
-                   const ForceScratch& fs, cudaStream_t s);
+                   const ForceScratch& fs, cudaStream_t s, const Fork* fk = nullptr);
 void launch_chain_forces(const ChainDev& ch, int prec, const double* x, const ForceTarget& t, cudaStream_t s);
 void launch_chain_energy(const ChainDev& ch, int prec, const double* x, const double* d, const LambdaSet* lam,
                          double* partial, int nblk_total, int blk_off, cudaStream_t s);
 int chain_blocks(const ChainDev& ch);
-void build_chains(const medyan_system* s, ChainHost& out);
+void chain_order(const medyan_system* s, std::vector<int>& order);
+void build_chains(const medyan_system* s, const std::vector<int>& pos, ChainHost& out);
+// coordinate-layout conversion: internal position p <-> external bead order[p]
+void launch_to_internal(int n3, const int* order, const double* ext, double* in, cudaStream_t s);
+void launch_to_external(int n3, const int* order, const double* in, double* ext, cudaStream_t s);
 
 void launch_excl_energy(const DeviceFF& ff, int prec, const double* x, const double* d, const LambdaSet* lam,
                         const EnergyScratch& es, cudaStream_t s);
@@ -115,7 +127,8 @@ void launch_excl_energy_fallback_and_finish(const DeviceFF& ff, const double* x,
                                             const LambdaSet* lam, const EnergyScratch& es, cudaStream_t s);
 
 // One-time per-device kernel attributes (forceN's 80 KB abscissa table).
-constexpr int kForceNGridBytes = (10000 + 1) * (int)sizeof(double);
+// Fills the quadrature grids of the excluded-volume fallbacks, once per
+// device (the current one); call before any stream capture.
 cudaError_t init_excl_kernels();
 
 int bonded_blocks(const DeviceFF& ff);

@@ -503,7 +503,16 @@ medyan_status medyan_mech_set_cylinders(medyan_mech* h, const medyan_cylinders* 
         cudaError_t e = b->planes.assign(b->planes_host4().data(), boundary->n_planes, h->stream);
         if (e != cudaSuccess) return cuda_status(e);
     }
-    cudaError_t e = b->set(cyl, h->stream);
+    // bead indices into the handle's internal order
+    std::vector<int32_t> b1(cyl->n_cyl), b2(cyl->n_cyl);
+    for (int i = 0; i < cyl->n_cyl; ++i) {
+        b1[i] = h->pos_host.empty() ? cyl->bead1[i] : h->pos_host[cyl->bead1[i]];
+        b2[i] = h->pos_host.empty() ? cyl->bead2[i] : h->pos_host[cyl->bead2[i]];
+    }
+    medyan_cylinders ci = *cyl;
+    ci.bead1 = b1.data();
+    ci.bead2 = b2.data();
+    cudaError_t e = b->set(&ci, h->stream);
     return cuda_status(e);
 }
 
@@ -544,11 +553,13 @@ medyan_status medyan_mech_get_excl_volume(medyan_mech* h, int32_t* beads_out, do
         e = cudaMemcpyAsync(krs.data(), h->excl_krs.raw(), sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) return cuda_status(e);
+    // internal offsets back to the caller's bead order
+    auto ext = [&](int off) { return h->order_host.empty() ? off : 3 * h->order_host[off / 3]; };
     for (int64_t i = 0; i < n; ++i) {
-        beads_out[4 * i] = bs[i].x;
-        beads_out[4 * i + 1] = bs[i].y;
-        beads_out[4 * i + 2] = bs[i].z;
-        beads_out[4 * i + 3] = bs[i].w;
+        beads_out[4 * i] = ext(bs[i].x);
+        beads_out[4 * i + 1] = ext(bs[i].y);
+        beads_out[4 * i + 2] = ext(bs[i].z);
+        beads_out[4 * i + 3] = ext(bs[i].w);
         // the device keeps krep*L1*L2; report it with unit lengths
         if (k_out) k_out[i] = krs[i];
         if (eqlen_out) {
