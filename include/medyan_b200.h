@@ -320,6 +320,43 @@ medyan_status medyan_mech_get_excl_volume(medyan_mech* h, int32_t* beads_out, do
                                           double* eqlen_out, int64_t capacity, int64_t* n_out);
 
 /* ------------------------------------------------------------------------ */
+/* Excluded-volume energy without device allocation                          */
+/* ------------------------------------------------------------------------ */
+/* No counterpart in the reference. The reference's CylinderExclVolume energy
+   (src/Mechanics/ForceField/Volume/CylinderExclVolRepulsion.cpp) runs inside
+   ForceFieldManager, which this library covers through a handle. Handles
+   allocate device scratch with cudaMalloc. This entry point allocates
+   nothing, for callers that cannot let a library allocate device memory when
+   they need an energy. Examples: an application whose own pool allocator owns
+   the device, or a step loop whose device footprint must stay fixed.
+
+   Computes the excluded-volume energy of n_pairs cylinder pairs. All array
+   pointers are DEVICE pointers on the current device, owned by the caller:
+     d_coords      double[3*n_beads]   AoS coordinates
+     d_excl_beads  int32[4*n_pairs]    coordinate offsets 3*bead, 16-byte aligned
+     d_excl_krs    double[n_pairs]     krep * eqLength1 * eqLength2 per pair
+   The kernels and the fallback for degenerate pairs are those of
+   medyan_mech_energy's excluded-volume slot, in FP64. The call enqueues on
+   `stream` (a cudaStream_t; NULL = legacy default stream), waits for it and
+   stores the energy in *e_out (host).
+
+   Scratch lives in a fixed static device array of the library, sized for
+   MEDYAN_NOALLOC_MAX_EXCL_PAIRS pairs. Larger n_pairs returns
+   MEDYAN_ERR_CAPACITY. Bead offsets outside [0, 3*n_beads) or not multiples
+   of 3 return MEDYAN_ERR_INDEX_RANGE before any energy kernel runs. A
+   non-finite pair energy returns MEDYAN_ERR_NONFINITE.
+
+   The first call on each device sets up: it looks up the scratch array's
+   address (cudaGetSymbolAddress) with that device current. Make that first
+   call before any stream capture begins. All calls on one device share the
+   scratch: calls that overlap in time (other host threads, other streams)
+   race and give wrong results, so serialize them. */
+#define MEDYAN_NOALLOC_MAX_EXCL_PAIRS 262144
+medyan_status medyan_excl_energy_noalloc(const double* d_coords, int32_t n_beads,
+                                         const int32_t* d_excl_beads, const double* d_excl_krs,
+                                         int32_t n_pairs, double* e_out, void* stream);
+
+/* ------------------------------------------------------------------------ */
 /* Library info                                                              */
 /* ------------------------------------------------------------------------ */
 const char* medyan_status_string(int32_t status);

@@ -42,6 +42,7 @@ PROTOTYPES = {
     "medyan_mech_set_cylinders": (C.c_int32, [_vp, _vp, _vp, _vp]),
     "medyan_mech_rebuild_neighbors": (C.c_int32, [_vp, _pi64, _pi64]),
     "medyan_mech_get_excl_volume": (C.c_int32, [_vp, _pi, _pd, _pd, C.c_int64, _pi64]),
+    "medyan_excl_energy_noalloc": (C.c_int32, [_vp, C.c_int32, _vp, _vp, C.c_int32, _pd, _vp]),
 }
 
 _lib = None
