@@ -254,6 +254,7 @@ def run_ours(args, rank: int, world: int) -> dict:
 
     if not args.no_minimize and rank == 0:
         result["minimization"] = minimize_extras(net, make)
+        result["batched_ensemble"] = batch_extras()
     for f in {id(ff): ff, id(ff64): ff64}.values():
         f.close()
     return result
@@ -298,6 +299,53 @@ def minimize_extras(net, make) -> dict:
     if "fp64" in out and "mixed" in out:
         e64, em = out["fp64"]["energy_after"], out["mixed"]["energy_after"]
         out["final_energy_rel_diff_mixed_vs_fp64"] = abs(em - e64) / abs(e64)
+    return out
+
+
+def batch_extras(n_replicas: int = 256) -> dict:
+    """The batched ensemble (256 networks of the medium network's composition,
+    200-4,000 cylinders each): one batched minimization per precision, gradTol
+    1 pN, and the same replicas minimized one at a time for comparison (first
+    16 replicas). Neighbor lists are built on the device per replica."""
+    import numpy as np
+    import torch
+
+    from medyan_b200.forcefield import BatchMinimizer, ForceFieldManager, conjugate_gradient_params
+    from medyan_b200.network import make_batch
+    nets = make_batch(n_replicas, 2)
+    p = conjugate_gradient_params(grad_tol=1.0, max_dist=1.0, lambda_max=0.01, energy_rel_tol=1e-9)
+    warm = conjugate_gradient_params(grad_tol=1.0, energy_call_limit=3)
+    xs = [net.flat_coords() for net in nets]
+    out = {"replicas": n_replicas, "beads": int(sum(n.n_beads for n in nets))}
+    for prec in ("fp64", "mixed"):
+        svs = [net.system_view() for net in nets]
+        with BatchMinimizer(svs, prec) as b:
+            for r, net in enumerate(nets):
+                bp, _ = net.boundary_params()
+                b.rebuild_neighbor_lists(r, xs[r], net.cylinders_view(), net.nl_params(), bp)
+            b.minimize(xs, warm)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            st, xo, fo, rs = b.minimize(xs, p)
+            dt = time.perf_counter() - t0
+        m = 16
+        seq = 0.0
+        for r in range(m):
+            with ForceFieldManager(prec) as ff:
+                ff.vectorize_all_force_fields(svs[r])
+                bp, _ = nets[r].boundary_params()
+                ff.set_coords(xs[r])
+                ff.set_cylinders(nets[r].cylinders_view(), nets[r].nl_params(), bp)
+                ff.rebuild_neighbor_lists()
+                ff.minimize(xs[r], warm)
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                ff.minimize(xs[r], p)
+                seq += time.perf_counter() - t0
+        its = [r.num_iter for r in rs]
+        out[prec] = {"seconds": dt, "minimizations_per_s": n_replicas / dt,
+                     "one_at_a_time_minimizations_per_s": m / seq, "iterations_mean": float(np.mean(its)),
+                     "iterations_max": int(max(its)), "statuses": sorted(set(int(v) for v in st))}
     return out
 
 

@@ -320,6 +320,66 @@ medyan_status medyan_mech_get_excl_volume(medyan_mech* h, int32_t* beads_out, do
                                           double* eqlen_out, int64_t capacity, int64_t* n_out);
 
 /* ------------------------------------------------------------------------ */
+/* Derivatives (sensitivity analysis)                                        */
+/* ------------------------------------------------------------------------ */
+/* No counterpart in the reference. Gradient of the total energy with respect
+   to every interaction's parameters, at the handle's coordinates, analytic
+   and in FP64. With v != NULL (double[3*n_beads], caller's bead order) the
+   outputs are instead the derivatives of those gradients along v,
+   d/de [dE/dtheta](x + e v) = v . d2E/(dx dtheta), by a centred difference
+   (step 1e-5 nm in the max-norm of v) — the mixed term an implicit adjoint
+   needs. Outputs are double[n] in the force field's interaction order (the
+   order given at vectorization; for excluded volume and boundary rebuilt on
+   the device, the order of medyan_mech_get_excl_volume); either may be NULL.
+     MEDYAN_FF_FILAMENT_STRETCHING, _LINKER_STRETCHING, _MOTOR_STRETCHING:
+         d_k = dE/dk,      d_p = dE/dl0
+     MEDYAN_FF_FILAMENT_BENDING:     d_k = dE/dk,   d_p = dE/dtheta0
+     MEDYAN_FF_EXCLUDED_VOLUME:      d_k = dE/dkRS with kRS = krep*L1*L2
+                                     (multiply by L1*L2 for dE/dkrep); d_p = 0
+     MEDYAN_FF_BOUNDARY:             d_k = dE/dk,   d_p = dE/dscreen_length
+   n must equal the force field's interaction count (else
+   MEDYAN_ERR_CAPACITY); the branching slots return MEDYAN_ERR_UNSUPPORTED. */
+medyan_status medyan_mech_param_grad(medyan_mech* h, int32_t ff, const double* v, double* d_k, double* d_p,
+                                     int64_t n);
+
+/* Hessian-vector product hv = (d2E/dx2) v at the handle's coordinates
+   (double[3*n_beads], caller's bead order): a centred difference of the
+   analytic forces along v, -(F(x + e v) - F(x - e v)) / (2 e) with e = 1e-5 nm
+   in the max-norm of v; both sides run through the force kernels with the
+   move applied on the fly. Use an FP64 handle (a mixed handle differences
+   float forces). */
+medyan_status medyan_mech_hvp(medyan_mech* h, const double* v, double* hv);
+
+/* ------------------------------------------------------------------------ */
+/* Batched minimization of independent networks                              */
+/* ------------------------------------------------------------------------ */
+/* No counterpart in the reference (which minimizes one system at a time).
+   A batch holds one handle per replica network. medyan_batch_minimize
+   enqueues every replica's whole minimization (one graph launch each, loops
+   on the device) before waiting for any, so the replicas run concurrently and
+   each stops at its own convergence test; every replica gets exactly the
+   CGMethod::minimize semantics of medyan_cg_minimize. */
+typedef struct medyan_batch medyan_batch;
+
+medyan_status medyan_batch_create(const medyan_system* systems, int32_t n_replicas, int32_t precision,
+                                  medyan_batch** out);
+medyan_status medyan_batch_destroy(medyan_batch* b);
+int32_t medyan_batch_size(const medyan_batch* b);
+/* The handle of replica r (owned by the batch), e.g. for
+   medyan_mech_set_cylinders / medyan_mech_rebuild_neighbors; NULL if out of range. */
+medyan_mech* medyan_batch_replica(medyan_batch* b, int32_t r);
+/* coords_inout[r]: double[3*n_beads(r)]; forces_out may be NULL, else
+   forces_out[r] likewise; results may be NULL, else medyan_min_result[n];
+   statuses[n] receives each replica's status (MEDYAN_ERR_LINE_SEARCH is a
+   per-replica outcome). Returns the first status that is neither OK nor
+   MEDYAN_ERR_LINE_SEARCH, else MEDYAN_OK. */
+medyan_status medyan_batch_minimize(medyan_batch* b, const medyan_cg_params* p, double* const* coords_inout,
+                                    double* const* forces_out, medyan_min_result* results, int32_t* statuses);
+/* Energy and forces of every replica (e_totals: double[n]). */
+medyan_status medyan_batch_evaluate(medyan_batch* b, const double* const* coords, double* e_totals,
+                                    double* const* forces_out);
+
+/* ------------------------------------------------------------------------ */
 /* Excluded-volume energy without device allocation                          */
 /* ------------------------------------------------------------------------ */
 /* No counterpart in the reference. The reference's CylinderExclVolume energy

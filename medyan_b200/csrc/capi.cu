@@ -122,6 +122,19 @@ medyan_status upload_system(medyan_mech* h, const medyan_system* s) {
     UPLOAD(h->chain_bend_p, chs.bend_p);
     h->chain.n_pos = s->n_beads;
 
+    // caller's interaction -> chain position or leftover record
+    {
+        std::vector<int> sm(s->n_stretch), bm(s->n_bend);
+        for (int i = 0; i < s->n_stretch; ++i) sm[i] = pos[s->stretch_beads[2 * i] / 3];
+        for (int q = 0; q < (int)chs.left_stretch.size(); ++q) sm[chs.left_stretch[q]] = -1 - q;
+        for (int i = 0; i < s->n_bend; ++i) bm[i] = pos[s->bend_beads[3 * i + 1] / 3];
+        for (int q = 0; q < (int)chs.left_bend.size(); ++q) bm[chs.left_bend[q]] = -1 - q;
+        UPLOAD(h->stretch_map, sm);
+        UPLOAD(h->bend_map, bm);
+        h->n_stretch_in = s->n_stretch;
+        h->n_bend_in = s->n_bend;
+    }
+
     ff.n_stretch = (int)chs.left_stretch.size();
     i2.resize(ff.n_stretch);
     d2.resize(ff.n_stretch);
@@ -315,9 +328,11 @@ cudaError_t launch_pass(medyan_mech* h, int which) {
 medyan_status medyan_mech::init() {
     cudaError_t e = cudaSetDevice(device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
-    for (int k = 0; k < 2 && e == cudaSuccess; ++k) e = cudaStreamCreateWithFlags(&fork.side[k], cudaStreamNonBlocking);
+    for (int k = 0; k < kForkWays && e == cudaSuccess; ++k)
+        e = cudaStreamCreateWithFlags(&fork.side[k], cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&fork.fork, cudaEventDisableTiming);
-    for (int k = 0; k < 2 && e == cudaSuccess; ++k) e = cudaEventCreateWithFlags(&fork.join[k], cudaEventDisableTiming);
+    for (int k = 0; k < kForkWays && e == cudaSuccess; ++k)
+        e = cudaEventCreateWithFlags(&fork.join[k], cudaEventDisableTiming);
     if (e == cudaSuccess) e = init_excl_kernels();
     const size_t n3 = 3 * (size_t)n_beads;
     if (e == cudaSuccess) e = x.reserve(n3);
@@ -354,6 +369,7 @@ medyan_mech::~medyan_mech() {
     cudaSetDevice(device);
     if (stream) cudaStreamSynchronize(stream);
     if (cg_graph) cudaGraphExecDestroy(cg_graph);
+    if (cg_pinned) cudaFreeHost(cg_pinned);
     for (auto& g : pass_graph)
         if (g) cudaGraphExecDestroy(g);
     destroy_nl(this);

@@ -382,6 +382,35 @@ __global__ void k_cg_record_energy(CGState* __restrict__ st, const double* __res
     }
 }
 
+// After the loop (MController / CGMethod epilogue): unless the line search
+// failed, restore the lowest-energy coordinates when a call limit ended the
+// run (copycoordsifminimumE); copy the current force into f0.
+__global__ void __launch_bounds__(kVecThreads) k_cg_finalize(int n3, double* __restrict__ x,
+                                                             const double* __restrict__ minE,
+                                                             double* __restrict__ f0, const double* __restrict__ f1,
+                                                             const CGState* __restrict__ st) {
+    const bool restore = st->status != MEDYAN_ERR_LINE_SEARCH && st->call_limit && st->have_min_e;
+    const bool copy_f = st->parity != 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x) {
+        if (restore) x[i] = minE[i];
+        if (copy_f) f0[i] = f1[i];
+    }
+}
+
+// energiesAfter, recorded unless the line search failed (the reference
+// returns at once then).
+__global__ void k_cg_record_final(CGState* __restrict__ st, const double* __restrict__ out, double* __restrict__ dst) {
+    if (st->status == MEDYAN_ERR_LINE_SEARCH) return;
+    CGState& s = *st;
+    double tot = 0.0;
+    for (int i = 0; i < MEDYAN_FF_COUNT; ++i) {
+        dst[i] = out[i];
+        tot += out[i];
+    }
+    dst[MEDYAN_FF_COUNT] = tot;
+    s.num_energy_call++;
+}
+
 // Condition kernels for the graph's WHILE nodes.
 __global__ void k_cond_ls(const CGState* __restrict__ st, cudaGraphConditionalHandle h) {
     cudaGraphSetConditional(h, (!st->done && st->ls_active) ? 1u : 0u);
@@ -512,9 +541,13 @@ cudaError_t build_graph(const CGLaunch& c, cudaGraphExec_t* exec) {
 
 using namespace mb;
 
-extern "C" medyan_status medyan_cg_minimize(medyan_mech* h, const medyan_cg_params* p, double* coord_inout,
-                                            double* force_out, medyan_min_result* out) {
-    if (!h || !p || !coord_inout) return MEDYAN_ERR_INVALID_ARG;
+namespace mb {
+
+// Enqueues a whole minimization on the handle's stream: setup, the first
+// energy and force, the loop graph, the epilogue and the final energy. No
+// host synchronization; cg_collect reads the results.
+medyan_status cg_enqueue(medyan_mech* h, const medyan_cg_params* p, const double* coord_in) {
+    if (!h || !p || !coord_in) return MEDYAN_ERR_INVALID_ARG;
     if (p->method < 0 || p->method > 2 || !(p->max_dist > 0) || !(p->lambda_max > 0)) return MEDYAN_ERR_INVALID_ARG;
     const int n3 = 3 * h->n_beads;
     cudaStream_t s = h->stream;
@@ -527,6 +560,19 @@ extern "C" medyan_status medyan_cg_minimize(medyan_mech* h, const medyan_cg_para
     if (e == cudaSuccess) e = h->cg_lam.reserve(1);
     if (e != cudaSuccess) return cuda_status(e);
     const size_t bytes = sizeof(double) * (size_t)n3;
+    // pinned staging: coordinates in, coordinates and forces out, state, lambda set
+    const size_t need = 2 * bytes + sizeof(CGState) + sizeof(LambdaSet) + 64;
+    if (h->cg_pinned_bytes < need) {
+        if (h->cg_pinned) cudaFreeHost(h->cg_pinned);
+        h->cg_pinned = nullptr;
+        h->cg_pinned_bytes = 0;
+        e = cudaMallocHost(reinterpret_cast<void**>(&h->cg_pinned), need);
+        if (e != cudaSuccess) return cuda_status(e);
+        h->cg_pinned_bytes = need;
+    }
+    double* px = reinterpret_cast<double*>(h->cg_pinned);
+    CGState* ps = reinterpret_cast<CGState*>(h->cg_pinned + 2 * bytes);
+    LambdaSet* pl = reinterpret_cast<LambdaSet*>(h->cg_pinned + 2 * bytes + sizeof(CGState));
     CGLaunch c = make_launch(h);
 
     CGState s0{};
@@ -547,9 +593,12 @@ extern "C" medyan_status medyan_cg_minimize(medyan_mech* h, const medyan_cg_para
     s0.skip_force = 0;
     s0.move_kind = 0;
     LambdaSet l0{};
-    e = coords_to_device(h, coord_inout, c.x, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(c.st, &s0, sizeof s0, cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(c.L, &l0, sizeof l0, cudaMemcpyHostToDevice, s);
+    if (n3) std::memcpy(px, coord_in, bytes);
+    *ps = s0;
+    *pl = l0;
+    e = coords_to_device(h, px, c.x, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(c.st, ps, sizeof s0, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(c.L, pl, sizeof l0, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(c.d, 0, bytes ? bytes : 8, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(c.f0, 0, bytes ? bytes : 8, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(c.f1, 0, bytes ? bytes : 8, s);
@@ -576,26 +625,32 @@ extern "C" medyan_status medyan_cg_minimize(medyan_mech* h, const medyan_cg_para
     e = cudaGraphLaunch(h->cg_graph, s);
     if (e != cudaSuccess) return cuda_status(e);
 
-    CGState sf{};
-    e = cudaMemcpyAsync(&sf, c.st, sizeof sf, cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    // epilogue and energiesAfter, on the device
+    k_cg_finalize<<<c.vb, kVecThreads, 0, s>>>(n3, c.x, c.minE, c.f0, c.f1, c.st);
+    enqueue_energy(h, c.x, nullptr, h->lam_zero.raw(), s);
+    k_cg_record_final<<<1, 1, 0, s>>>(c.st, h->energy_out.raw(), h->cg_eout.raw() + kOut);
+    return cuda_status(cudaGetLastError());
+}
+
+// Waits for the handle's minimization and copies its results out.
+medyan_status cg_collect(medyan_mech* h, double* coord_out, double* force_out, medyan_min_result* out) {
+    cudaStream_t s = h->stream;
+    const size_t bytes = sizeof(double) * 3 * (size_t)h->n_beads;
+    double* px = reinterpret_cast<double*>(h->cg_pinned);
+    double* pf = reinterpret_cast<double*>(h->cg_pinned + bytes);
+    CGState* ps = reinterpret_cast<CGState*>(h->cg_pinned + 2 * bytes);
+    cudaError_t e = coords_to_host(h, h->x.raw(), px, s);
+    if (e == cudaSuccess && force_out) e = coords_to_host(h, h->f.raw(), pf, s);
     if (e != cudaSuccess) return cuda_status(e);
-    if (sf.status == MEDYAN_ERR_LINE_SEARCH) {
-        // errorLineSearch: return at once, coordinates as they are
-        coords_to_host(h, c.x, coord_inout, s);
-        if (force_out) coords_to_host(h, sf.parity ? c.f1 : c.f0, force_out, s);
-    } else {
-        if (sf.call_limit && sf.have_min_e) cudaMemcpyAsync(c.x, c.minE, bytes, cudaMemcpyDeviceToDevice, s);
-        enqueue_energy(h, c.x, nullptr, h->lam_zero.raw(), s);
-        k_cg_record_energy<<<1, 1, 0, s>>>(c.st, h->energy_out.raw(), h->cg_eout.raw() + kOut, 0);
-        coords_to_host(h, c.x, coord_inout, s);
-        if (force_out) coords_to_host(h, sf.parity ? c.f1 : c.f0, force_out, s);
-    }
     double eo[2 * kOut];
-    e = cudaMemcpyAsync(eo, h->cg_eout.raw(), sizeof eo, cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&sf, c.st, sizeof sf, cudaMemcpyDeviceToHost, s);
+    e = cudaMemcpyAsync(ps, h->cg_state.raw(), sizeof(CGState), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_status(e);
+    const CGState sf = *ps;
+    e = cudaMemcpy(eo, h->cg_eout.raw(), sizeof eo, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_status(e);
+    if (bytes) std::memcpy(coord_out, px, bytes);
+    if (force_out && bytes) std::memcpy(force_out, pf, bytes);
     if (out) {
         std::memset(out, 0, sizeof *out);
         for (int i = 0; i < MEDYAN_FF_COUNT; ++i) {
@@ -616,4 +671,13 @@ extern "C" medyan_status medyan_cg_minimize(medyan_mech* h, const medyan_cg_para
         out->energy_rel_tol = sf.energy_rel_tol;
     }
     return (medyan_status)sf.status;
+}
+
+}  // namespace mb
+
+extern "C" medyan_status medyan_cg_minimize(medyan_mech* h, const medyan_cg_params* p, double* coord_inout,
+                                            double* force_out, medyan_min_result* out) {
+    medyan_status st = cg_enqueue(h, p, coord_inout);
+    if (st != MEDYAN_OK) return st;
+    return cg_collect(h, coord_inout, force_out, out);
 }

@@ -260,13 +260,12 @@ __global__ void __launch_bounds__(kBlock) k_excl_force_fallback(const DeviceFF f
     if (threadIdx.x == 0) *fb_count = 0;
 }
 
-constexpr int kFinishThreads = 512;
+constexpr int kFinishThreads = 1024;
 
-// Sums the per-block energy partials of each force field (each thread takes
-// rows threadIdx.x, +512, ... and adds every row's values into its force-field
-// slots; then one block reduction: a fixed order, so the result is
-// deterministic), evaluates the energyN fallback for queued pairs in (slot,
-// pair) order, and applies ForceFieldManager::computeEnergy's rule
+// Sums the per-block energy partials of each force field (one warp per
+// (lambda, slot) pair, rows in a fixed order, so the result is deterministic),
+// evaluates the energyN fallback for queued pairs in (slot, pair) order, and
+// applies ForceFieldManager::computeEnergy's rule
 // (ForceFieldManager.cpp:137-176): a force field at or below -1 makes the
 // total +inf.
 __global__ void __launch_bounds__(kFinishThreads) k_energy_finish(const DeviceFF ff, const double* __restrict__ x,
@@ -276,7 +275,7 @@ __global__ void __launch_bounds__(kFinishThreads) k_energy_finish(const DeviceFF
                                                                   int nbb, int nbe, int* __restrict__ fb_count,
                                                                   int2* __restrict__ fb_list, int* __restrict__ bad,
                                                                   double* __restrict__ out) {
-    __shared__ double red[kMaxLambda * MEDYAN_FF_COUNT * 32];
+    __shared__ double red[4 * 32];
     __shared__ double sums[kMaxLambda][MEDYAN_FF_COUNT];
     __shared__ double fbE[kMaxLambda];
     __shared__ int nfb;
@@ -315,50 +314,41 @@ __global__ void __launch_bounds__(kFinishThreads) k_energy_finish(const DeviceFF
         }
         __syncthreads();
     }
-    // per-slot sums. Row r's four values go to slots (sx, sy, sz, sw), -1 = none:
-    // chain rows (stretch, bend), bonded segments (one slot; the branch segment
-    // four), excluded-volume rows.
-    double acc[kMaxLambda * MEDYAN_FF_COUNT];
+    // per-slot sums: warp w takes (lambda, slot) combos w, w + nwarps, ...;
+    // each lane sums rows lane, lane + 32, ... of the slot's row ranges, eight
+    // loads in flight at a time, then the warp reduces (fixed order)
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    auto range_sum = [&](const double* base, int b0, int b1, int j) {
+        double acc = 0.0;
+        int b = b0 + lane;
+        for (; b + 32 * 7 < b1; b += 32 * 8) {
+            double v[8];
 #pragma unroll
-    for (int j = 0; j < kMaxLambda * MEDYAN_FF_COUNT; ++j) acc[j] = 0.0;
-#pragma unroll 2
-    for (int r = threadIdx.x; r < total_blocks; r += blockDim.x) {
-        int sx = 8, sy = -1, sz = -1, sw = -1;
-        if (r < nch) {
-            sx = 0;
-            sy = 1;
-        } else if (r < nch + nbb) {
-            const int b = r - nch;
-            int sg = 0;
-            while (sg < 5 && b >= ff.seg[sg + 1]) ++sg;
-            sx = sg < 4 ? sg : (sg == 4 ? 4 : MEDYAN_FF_BOUNDARY);
-            if (sg == 4) {
-                sy = 5;
-                sz = 6;
-                sw = 7;
-            }
+            for (int u = 0; u < 8; ++u) v[u] = __ldcg(base + (size_t)(b + 32 * u) * 4 + j);
+#pragma unroll
+            for (int u = 0; u < 8; ++u) acc += v[u];
         }
-#pragma unroll
-        for (int k = 0; k < kMaxLambda; ++k) {
-            if (k < K) {
-                const double* p = partial + ((size_t)k * total_blocks + r) * 4;
-                const double vx = __ldcg(p), vy = __ldcg(p + 1), vz = __ldcg(p + 2), vw = __ldcg(p + 3);
-#pragma unroll
-                for (int j = 0; j < MEDYAN_FF_COUNT; ++j) {
-                    double a = acc[k * MEDYAN_FF_COUNT + j];
-                    if (sx == j) a += vx;
-                    if (sy == j) a += vy;
-                    if (sz == j) a += vz;
-                    if (sw == j) a += vw;
-                    acc[k * MEDYAN_FF_COUNT + j] = a;
-                }
-            }
+        for (; b < b1; b += 32) acc += __ldcg(base + (size_t)b * 4 + j);
+        return acc;
+    };
+    for (int combo = warp; combo < K * MEDYAN_FF_COUNT; combo += nwarp) {
+        const int k = combo / MEDYAN_FF_COUNT, slot = combo % MEDYAN_FF_COUNT;
+        // row ranges: chain rows [0, nch), bonded rows nch + seg[], excluded-volume rows after
+        int b0 = 0, b1 = 0, j = 0, c1 = 0, cj = 0;
+        switch (slot) {
+            case 0: c1 = nch; cj = 0; b0 = nch + ff.seg[0]; b1 = nch + ff.seg[1]; break;
+            case 1: c1 = nch; cj = 1; b0 = nch + ff.seg[1]; b1 = nch + ff.seg[2]; break;
+            case 2: b0 = nch + ff.seg[2]; b1 = nch + ff.seg[3]; break;
+            case 3: b0 = nch + ff.seg[3]; b1 = nch + ff.seg[4]; break;
+            case 4: case 5: case 6: case 7: b0 = nch + ff.seg[4]; b1 = nch + ff.seg[5]; j = slot - 4; break;
+            case 8: b0 = nch + nbb; b1 = nch + nbb + nbe; break;
+            default: b0 = nch + ff.seg[5]; b1 = nch + ff.seg[6]; break;
         }
-    }
-    block_sum<kMaxLambda * MEDYAN_FF_COUNT>(acc, red);
-    if (threadIdx.x == 0) {
-        for (int k = 0; k < kMaxLambda; ++k)
-            for (int j = 0; j < MEDYAN_FF_COUNT; ++j) sums[k][j] = acc[k * MEDYAN_FF_COUNT + j];
+        const double* base = partial + (size_t)k * total_blocks * 4;
+        double sv = range_sum(base, b0, b1, j) + range_sum(base, 0, c1, cj);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) sv += __shfl_down_sync(0xffffffffu, sv, o);
+        if (lane == 0) sums[k][slot] = sv;
     }
     __syncthreads();
     if (threadIdx.x == 0) {

@@ -320,40 +320,40 @@ void launch_energy(const ChainDev& ch, const DeviceFF& ff, int prec, const doubl
     // line search compares totals whose differences are ~1e-9 of the total,
     // below float resolution per term. Only the force pass runs in float.
     (void)prec;
-    // three branches: chain + boundary + filament leftovers | linker, motor,
-    // branching | excluded volume; then the finish kernel
-    cudaStream_t s1 = s, s2 = s;
+    // five branches: chain | excluded volume | linker, motor | branching |
+    // boundary, filament leftovers; then the finish kernel
+    cudaStream_t b[kForkWays] = {s, s, s, s};
     if (fk) {
-        fork_to(fk, s, 2);
-        s1 = fk->side[0];
-        s2 = fk->side[1];
+        fork_to(fk, s, kForkWays);
+        for (int k = 0; k < kForkWays; ++k) b[k] = fk->side[k];
     }
-    launch_excl_energy(ff, prec, x, d, lam, es, s2);
-    bonded_energy_group<2, 4>(ff, x, d, lam, es, s1);
-    bonded_energy_group<4, 5>(ff, x, d, lam, es, s1);
+    launch_excl_energy(ff, prec, x, d, lam, es, b[0]);
+    bonded_energy_group<2, 4>(ff, x, d, lam, es, b[1]);
+    bonded_energy_group<4, 5>(ff, x, d, lam, es, b[2]);
+    bonded_energy_group<5, 6>(ff, x, d, lam, es, b[3]);
+    bonded_energy_group<0, 2>(ff, x, d, lam, es, b[3]);
     launch_chain_energy(ch, MEDYAN_PREC_FP64, x, d, lam, es.partial, es.total(), 0, s);
-    bonded_energy_group<5, 6>(ff, x, d, lam, es, s);
-    bonded_energy_group<0, 2>(ff, x, d, lam, es, s);
-    if (fk) join_from(fk, s, 2);
+    if (fk) join_from(fk, s, kForkWays);
     launch_excl_energy_fallback_and_finish(ff, x, d, lam, es, s);
 }
 
 void launch_forces(const ChainDev& ch, const DeviceFF& ff, int prec, const double* x, const ForceTarget& t,
                    const ForceScratch& fs, cudaStream_t s, const Fork* fk) {
-    // the chain pass stores every bead's force; everything after adds, in two
-    // branches: excluded volume | bonded groups
+    // the chain pass stores every bead's force; everything after adds, in four
+    // branches: excluded volume | linker, motor | branching | boundary,
+    // filament leftovers
     launch_chain_forces(ch, prec, x, t, s);
-    cudaStream_t s1 = s;
+    cudaStream_t b[kForkWays] = {s, s, s, s};
     if (fk) {
-        fork_to(fk, s, 1);
-        s1 = fk->side[0];
+        fork_to(fk, s, 3);
+        for (int k = 0; k < 3; ++k) b[k + 1] = fk->side[k];
     }
-    bonded_forces_group<2, 4>(ff, prec, x, t, s1);
-    bonded_forces_group<4, 5>(ff, prec, x, t, s1);
-    bonded_forces_group<5, 6>(ff, prec, x, t, s1);
-    bonded_forces_group<0, 2>(ff, prec, x, t, s1);
+    bonded_forces_group<2, 4>(ff, prec, x, t, b[1]);
+    bonded_forces_group<4, 5>(ff, prec, x, t, b[2]);
+    bonded_forces_group<5, 6>(ff, prec, x, t, b[3]);
+    bonded_forces_group<0, 2>(ff, prec, x, t, b[3]);
     launch_excl_forces(ff, prec, x, t, fs, s);
-    if (fk) join_from(fk, s, 1);
+    if (fk) join_from(fk, s, 3);
 }
 
 }  // namespace mb

@@ -129,6 +129,14 @@ struct medyan_mech {
     mb::DevBuf<unsigned char> chain_flags;
     mb::DevBuf<double2> chain_link_p, chain_bend_p;
 
+    // interaction i of the caller's stretching / bending arrays -> chain
+    // position p (>= 0) or leftover record q (encoded -1 - q); used by the
+    // parameter gradients (diff.cu), which report in the caller's order
+    int n_stretch_in = 0, n_bend_in = 0;
+    mb::DevBuf<int> stretch_map, bend_map;
+    // Hessian-vector product scratch (diff.cu)
+    mb::DevBuf<double> hv_v, hv_a, hv_b, hv_lam, pg_k, pg_p;
+
     // force-field records
     mb::DevBuf<int2> stretch_bs;
     mb::DevBuf<double2> stretch_p;
@@ -151,6 +159,10 @@ struct medyan_mech {
     mb::DevBuf<mb::CGState> cg_state;
     mb::DevBuf<mb::LambdaSet> cg_lam;
     cudaGraphExec_t cg_graph = nullptr;   // instantiated minimization graph
+    // pinned host staging of a minimization's inputs and results, so that
+    // enqueueing it never waits on the device (batched minimization)
+    unsigned char* cg_pinned = nullptr;
+    size_t cg_pinned_bytes = 0;
     int cg_graph_prec = -1;
     long long cg_graph_gen = -1;          // ff_gen the graph was captured with
     long long ff_gen = 0;                 // bumped whenever DeviceFF changes
@@ -179,6 +191,10 @@ cudaError_t launch_pass(medyan_mech* h, int which);
 // Host coordinates/forces (caller's bead order) to and from internal device
 // arrays; stream-ordered on s (the host buffer must stay valid until s syncs).
 cudaError_t coords_to_device(medyan_mech* h, const double* host, double* dev, cudaStream_t s);
+// A minimization in two halves (cg.cu): enqueue everything on the handle's
+// stream without waiting, then wait and copy the results out.
+medyan_status cg_enqueue(medyan_mech* h, const medyan_cg_params* p, const double* coord_in);
+medyan_status cg_collect(medyan_mech* h, double* coord_out, double* force_out, medyan_min_result* out);
 cudaError_t coords_to_host(medyan_mech* h, const double* dev, double* host, cudaStream_t s);
 void destroy_nl(medyan_mech* h);
 }  // namespace mb

@@ -97,9 +97,10 @@ struct ForceScratch {
 // independent kernels on separate streams joined back into the caller's
 // stream; under stream capture the fork and join become graph edges, so the
 // kernels are parallel branches of the graph.
+constexpr int kForkWays = 4;
 struct Fork {
-    cudaStream_t side[2];
-    cudaEvent_t fork, join[2];
+    cudaStream_t side[kForkWays];
+    cudaEvent_t fork, join[kForkWays];
 };
 
 // Launchers (ff_kernels.cu / excl_kernels.cu / chain.cu). prec: MEDYAN_PREC_*.

@@ -133,6 +133,26 @@ class ForceFieldManager:
             L.check(st, "medyan_cg_minimize")
         return st, x, f, r
 
+    # -- derivatives -------------------------------------------------------
+    def param_grad(self, ff_slot: int, n: int, v=None):
+        """(dE/dk, dE/dp) per interaction of force field ff_slot at the
+        current coordinates; with v, their derivative along v."""
+        dk = np.zeros(max(n, 1))
+        dp = np.zeros(max(n, 1))
+        vv = f64(v) if v is not None else None
+        L.check(self.lib.medyan_mech_param_grad(self.handle, ff_slot, _dp(vv) if vv is not None else None, _dp(dk),
+                                                _dp(dp), n), "medyan_mech_param_grad")
+        return dk[:n], dp[:n]
+
+    def hvp(self, v) -> np.ndarray:
+        """Hessian of the total energy at the current coordinates times v."""
+        vv = f64(v)
+        hv = np.zeros_like(vv)
+        st = self.lib.medyan_mech_hvp(self.handle, _dp(vv), _dp(hv))
+        if st not in (0, 3):
+            L.check(st, "medyan_mech_hvp")
+        return hv
+
     # -- neighbor lists ----------------------------------------------------
     def set_cylinders(self, cylinders, nl_params, boundary_params) -> None:
         self._cyl = (cylinders, nl_params, boundary_params)
@@ -163,6 +183,80 @@ class ForceFieldManager:
     def close(self) -> None:
         if self.handle:
             self.lib.medyan_mech_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+class BatchMinimizer:
+    """Independent networks minimized together (medyan_batch_*): every
+    replica's minimization is enqueued before any is awaited, so they run
+    concurrently on the device, each to its own convergence."""
+
+    def __init__(self, systems: list, precision: str = "fp64"):
+        self.lib = L.load()
+        self.precision = {"fp64": PREC_FP64, "mixed": PREC_MIXED}[precision]
+        self._systems = list(systems)
+        arr = (type(self._systems[0].struct) * len(self._systems))(*[sv.struct for sv in self._systems]) \
+            if self._systems else None
+        self.handle = C.c_void_p()
+        L.check(self.lib.medyan_batch_create(arr, len(self._systems), self.precision, C.byref(self.handle)),
+                "medyan_batch_create")
+        self.n = len(self._systems)
+
+    def replica(self, r: int) -> C.c_void_p:
+        """The handle of replica r (for set_cylinders / rebuild_neighbors)."""
+        return C.c_void_p(self.lib.medyan_batch_replica(self.handle, r))
+
+    def rebuild_neighbor_lists(self, r: int, coord, cylinders, nl_params, boundary_params) -> tuple[int, int]:
+        h = self.replica(r)
+        x = f64(coord)
+        L.check(self.lib.medyan_mech_set_coords(h, _dp(x)), "medyan_mech_set_coords")
+        L.check(self.lib.medyan_mech_set_cylinders(h, cylinders.ref(), C.byref(nl_params),
+                                                   C.byref(boundary_params) if boundary_params is not None else None),
+                "medyan_mech_set_cylinders")
+        ne, nb = C.c_int64(0), C.c_int64(0)
+        L.check(self.lib.medyan_mech_rebuild_neighbors(h, C.byref(ne), C.byref(nb)), "medyan_mech_rebuild_neighbors")
+        return ne.value, nb.value
+
+    def minimize(self, coords: list, params: CGParams):
+        """Returns (statuses, coords, forces, results) per replica."""
+        xs = [f64(x).copy() for x in coords]
+        fs = [np.zeros_like(x) for x in xs]
+        xp = (_pd * self.n)(*[_dp(x) for x in xs])
+        fp = (_pd * self.n)(*[_dp(f) for f in fs])
+        res = (MinResult * self.n)()
+        st = (C.c_int32 * self.n)()
+        top = self.lib.medyan_batch_minimize(self.handle, C.byref(params), xp, fp, res, st)
+        if top != 0:
+            L.check(top, "medyan_batch_minimize")
+        return list(st), xs, fs, list(res)
+
+    def evaluate(self, coords: list):
+        """Total energies and forces of every replica."""
+        xs = [f64(x) for x in coords]
+        fs = [np.zeros_like(x) for x in xs]
+        xp = (_pd * self.n)(*[_dp(x) for x in xs])
+        fp = (_pd * self.n)(*[_dp(f) for f in fs])
+        e = np.zeros(self.n)
+        st = self.lib.medyan_batch_evaluate(self.handle, xp, _dp(e), fp)
+        if st not in (0, 3):
+            L.check(st, "medyan_batch_evaluate")
+        return e, fs
+
+    def close(self) -> None:
+        if self.handle:
+            self.lib.medyan_batch_destroy(self.handle)
             self.handle = C.c_void_p()
 
     def __del__(self):

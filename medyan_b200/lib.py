@@ -43,6 +43,14 @@ PROTOTYPES = {
     "medyan_mech_rebuild_neighbors": (C.c_int32, [_vp, _pi64, _pi64]),
     "medyan_mech_get_excl_volume": (C.c_int32, [_vp, _pi, _pd, _pd, C.c_int64, _pi64]),
     "medyan_excl_energy_noalloc": (C.c_int32, [_vp, C.c_int32, _vp, _vp, C.c_int32, _pd, _vp]),
+    "medyan_mech_param_grad": (C.c_int32, [_vp, C.c_int32, _pd, _pd, _pd, C.c_int64]),
+    "medyan_mech_hvp": (C.c_int32, [_vp, _pd, _pd]),
+    "medyan_batch_create": (C.c_int32, [_vp, C.c_int32, C.c_int32, C.POINTER(_vp)]),
+    "medyan_batch_destroy": (C.c_int32, [_vp]),
+    "medyan_batch_size": (C.c_int32, [_vp]),
+    "medyan_batch_replica": (_vp, [_vp, C.c_int32]),
+    "medyan_batch_minimize": (C.c_int32, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    "medyan_batch_evaluate": (C.c_int32, [_vp, _vp, _pd, _vp]),
 }
 
 _lib = None

@@ -422,3 +422,26 @@ def make_network(spec: NetworkSpec) -> Network:
 
 def make_workload(index: int, seed: int | None = None, **over) -> Network:
     return make_network(workload_spec(index, seed, **over))
+
+
+def batch_specs(n_replicas: int = 256, seed: int = 2, cyl_range=(200, 4000)) -> list[NetworkSpec]:
+    """The batched ensemble: replicas of the medium network's composition
+    (linkers 10 %, motors 1 %, branch points 1 % of the cylinders) whose
+    cylinder counts are log-uniform in cyl_range, rounded to whole filaments.
+    Filaments have 10 cylinders (1.08 um) so that the smallest replicas fit
+    their box; the box keeps the medium network's cylinder density
+    (40,000 cylinders in a 5 um cube) but is at least 1.5 um wide."""
+    rng = np.random.default_rng(seed)
+    lo, hi = np.log(cyl_range[0]), np.log(cyl_range[1])
+    out = []
+    for r in range(n_replicas):
+        ncyl = int(round(float(np.exp(rng.uniform(lo, hi))) / 10.0)) * 10
+        ncyl = max(ncyl, 10)
+        box = max(5000.0 * (ncyl / 40000.0) ** (1.0 / 3.0), 1500.0)
+        out.append(NetworkSpec(f"cfg2_replica{r}_{ncyl}cyl", ncyl // 10, 10, box, n_linker=ncyl // 10,
+                               n_motor=ncyl // 100, n_branch=ncyl // 100, seed=seed * 100000 + r))
+    return out
+
+
+def make_batch(n_replicas: int = 256, seed: int = 2, cyl_range=(200, 4000)) -> list[Network]:
+    return [make_network(s) for s in batch_specs(n_replicas, seed, cyl_range)]

@@ -1,0 +1,85 @@
+"""Batched minimization of independent networks (medyan_batch_*): every
+replica must behave exactly as it does alone (same call counts and
+coordinates as the oracle's CGMethod on that replica), with replicas of
+uneven size and different outcomes in one batch."""
+import numpy as np
+import pytest
+
+from medyan_b200._abi import SystemView
+from medyan_b200.forcefield import BatchMinimizer, ForceFieldManager, conjugate_gradient_params as cgp
+from medyan_b200.network import make_batch
+
+pytestmark = pytest.mark.gpu
+
+
+def replicas(oracle, n=6, seed=5, cyl_range=(200, 800)):
+    nets = make_batch(n, seed, cyl_range)
+    out = []
+    for net in nets:
+        st, extra = oracle.complete(net)
+        assert st == 0
+        out.append((net.system_view(**extra), net.flat_coords()))
+    return out
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batch_matches_single(gpu_lib, oracle, precision):
+    reps = replicas(oracle)
+    p = cgp(grad_tol=1e-4, energy_rel_tol=1e-14, energy_call_limit=40)
+    with BatchMinimizer([sv for sv, _ in reps], precision) as b:
+        st, xs, fs, rs = b.minimize([x for _, x in reps], p)
+    for r, (sv, x) in enumerate(reps):
+        with ForceFieldManager(precision) as ff:
+            ff.vectorize_all_force_fields(sv)
+            s1, x1, f1, r1 = ff.minimize(x, p)
+        assert st[r] == s1 == 0
+        # a replica in a batch is the same computation as alone (forces
+        # accumulate with atomics, so equal to rounding, not bit for bit)
+        assert (rs[r].num_energy_call, rs[r].num_force_call, rs[r].num_iter) == \
+            (r1.num_energy_call, r1.num_force_call, r1.num_iter)
+        assert np.abs(xs[r] - x1).max() <= 1e-7
+        assert np.abs(fs[r] - f1).max() <= 1e-7 * np.abs(f1).max()
+        if precision == "fp64":
+            so, xo, fo, ro = oracle.minimize(sv, x, p)
+            assert (rs[r].num_energy_call, rs[r].num_iter) == (ro.num_energy_call, ro.num_iter)
+            assert np.abs(xs[r] - xo).max() <= 1e-7
+
+
+def test_batch_converges_each_replica(gpu_lib, oracle):
+    reps = replicas(oracle, n=5, seed=7)
+    p = cgp(grad_tol=1.0)
+    with BatchMinimizer([sv for sv, _ in reps], "fp64") as b:
+        st, xs, fs, rs = b.minimize([x for _, x in reps], p)
+    iters = [r.num_iter for r in rs]
+    for r in range(len(reps)):
+        assert st[r] == 0
+        # converged, or stopped by the force-call limit (MinimizationResult::callLimitExceeded)
+        assert (rs[r].grad_inf_norm < 1.0 or rs[r].energy_rel_change < 1e-9
+                or rs[r].num_force_call >= rs[r].force_call_limit), (rs[r].grad_inf_norm, rs[r].num_force_call)
+        assert np.abs(fs[r]).max() == pytest.approx(rs[r].grad_inf_norm)
+    assert len(set(iters)) > 1  # replicas stop at their own iteration counts
+
+
+def test_batch_line_search_failure_is_per_replica(gpu_lib, oracle):
+    # a degenerate replica (NaN bend energy, recovery off) next to a healthy one
+    bad_x = np.array([0, 0, 0, 0, 0, 0, 10, 0, 0, 30, 5, 0, 60, 5, 0], float)
+    bad = SystemView(5, bend_beads=[0, 3, 6], bend_k=[10.0], bend_theta0=[0.0], stretch_beads=[9, 12],
+                     stretch_k=[5.0], stretch_l0=[20.0])
+    (good, good_x), = replicas(oracle, n=1, seed=9)
+    p = cgp(grad_tol=1e-3, try_to_recover=False, energy_call_limit=40)
+    with BatchMinimizer([bad, good], "fp64") as b:
+        st, xs, fs, rs = b.minimize([bad_x, good_x], p)
+    so, xo, fo, ro = oracle.minimize(bad, bad_x, p)
+    assert st[0] == so == 7 and rs[0].error_flags == ro.error_flags == 1
+    assert st[1] == 0
+
+
+def test_batch_evaluate(gpu_lib, oracle):
+    reps = replicas(oracle, n=4, seed=11)
+    with BatchMinimizer([sv for sv, _ in reps], "fp64") as b:
+        e, fs = b.evaluate([x for _, x in reps])
+    for r, (sv, x) in enumerate(reps):
+        eo, _ = oracle.energy(sv, x)
+        fo = oracle.forces(sv, x)
+        assert abs(e[r] - eo) <= 1e-12 * abs(eo)
+        assert np.abs(fs[r] - fo).max() <= 1e-12 * np.abs(fo).max()
