@@ -117,8 +117,8 @@ __device__ void line_search_failed(CGState& s) {
 
 // After an energy pass: the reference's backtracking loop over the evaluated
 // trial lambdas (CGMethod.hpp:264-362).
-__global__ void k_ls_decide(CGState* __restrict__ st, LambdaSet* __restrict__ L, const double* __restrict__ out) {
-    CGState& s = *st;
+__device__ void ls_decide(CGState& s, LambdaSet& Lr, const double* __restrict__ out) {
+    LambdaSet* L = &Lr;
     s.reset_after_dir = 0;
     if (s.done || !s.ls_active) {
         L->K = 0;
@@ -181,6 +181,10 @@ __global__ void k_ls_decide(CGState* __restrict__ st, LambdaSet* __restrict__ L,
     fill_pass(s, *L);  // undecided: evaluate the next halvings
 }
 
+__global__ void k_ls_decide(CGState* __restrict__ st, LambdaSet* __restrict__ L, const double* __restrict__ out) {
+    ls_decide(*st, *L, out);
+}
+
 // ----------------------------------------------------------- vector passes
 __device__ __forceinline__ void block_reduce3(double& a, double& b, double& m, double* sm) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -234,35 +238,8 @@ __device__ void reduce_partials(const double* __restrict__ part, int nblk, doubl
     block_reduce3(a, b, m, sm);
 }
 
-// dots pass: commit the move, F.F, F.Fprev, max|F|.
-__global__ void __launch_bounds__(kVecThreads) k_cg_dots(int n3, double* __restrict__ x, const double* __restrict__ d,
-                                                         double* __restrict__ f0, double* __restrict__ f1,
-                                                         CGState* __restrict__ st, double* __restrict__ part) {
-    __shared__ double sm[96];
-    if (st->done || st->skip_force) return;
-    const int parity = st->parity;
-    const double* __restrict__ Fn = parity ? f0 : f1;  // new force (written by the force pass)
-    const double* __restrict__ Fo = parity ? f1 : f0;  // force at the previous point
-    const double lam = st->lam_move;
-    double a = 0.0, b = 0.0, m = 0.0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x) {
-        x[i] = move1(x[i], lam, d[i]);
-        const double fn = Fn[i], fo = Fo[i];
-        a += fn * fn;
-        b += fn * fo;
-        m = dmax_ref(m, fabs(fn));
-    }
-    block_reduce3(a, b, m, sm);
-    if (threadIdx.x == 0) {
-        part[4 * blockIdx.x] = a;
-        part[4 * blockIdx.x + 1] = b;
-        part[4 * blockIdx.x + 2] = m;
-    }
-    if (!last_block(&st->ticket_dots)) return;
-    reduce_partials(part, gridDim.x, a, b, m, sm);
-    if (threadIdx.x != 0) return;
-    CGState& s = *st;
-    s.ticket_dots = 0;
+// Scalar part of the dots pass (one thread): F.F = a, F.Fprev = b, max|F| = m.
+__device__ void dots_tail(CGState& s, double a, double b, double m) {
     s.num_force_call++;
     s.grad_inf_norm = m;  // maxF (CGMethod.hpp:202-212)
     if (isinf(m)) {
@@ -300,6 +277,64 @@ __global__ void __launch_bounds__(kVecThreads) k_cg_dots(int n3, double* __restr
     s.skip_force = 1;
 }
 
+// dots pass: commit the move, F.F, F.Fprev, max|F|.
+__global__ void __launch_bounds__(kVecThreads) k_cg_dots(int n3, double* __restrict__ x, const double* __restrict__ d,
+                                                         double* __restrict__ f0, double* __restrict__ f1,
+                                                         CGState* __restrict__ st, double* __restrict__ part) {
+    __shared__ double sm[96];
+    if (st->done || st->skip_force) return;
+    const int parity = st->parity;
+    const double* __restrict__ Fn = parity ? f0 : f1;  // new force (written by the force pass)
+    const double* __restrict__ Fo = parity ? f1 : f0;  // force at the previous point
+    const double lam = st->lam_move;
+    double a = 0.0, b = 0.0, m = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x) {
+        x[i] = move1(x[i], lam, d[i]);
+        const double fn = Fn[i], fo = Fo[i];
+        a += fn * fn;
+        b += fn * fo;
+        m = dmax_ref(m, fabs(fn));
+    }
+    block_reduce3(a, b, m, sm);
+    if (threadIdx.x == 0) {
+        part[4 * blockIdx.x] = a;
+        part[4 * blockIdx.x + 1] = b;
+        part[4 * blockIdx.x + 2] = m;
+    }
+    if (!last_block(&st->ticket_dots)) return;
+    reduce_partials(part, gridDim.x, a, b, m, sm);
+    if (threadIdx.x != 0) return;
+    st->ticket_dots = 0;
+    dots_tail(*st, a, b, m);
+}
+
+// Scalar part of the direction pass (one thread): d.F = a, max|d| = m.
+__device__ void dir_tail(CGState& s, LambdaSet& L, double a, double m) {
+    s.copy_min_e = 0;
+    s.dmax = m;
+    if (s.dir_mode == 0 && a <= 0) {
+        // conjugacy lost: resetCGParams (d = F; its d.F is F.F)
+        s.reset_after_dir = 1;
+        s.slope = s.new_grad;
+        s.dmax = s.grad_inf_norm;
+    } else {
+        s.slope = a;
+    }
+    if (s.method != MEDYAN_CG_STEEPEST) s.last_fdotf = s.new_grad;
+    s.dir_mode = 0;
+    // loop condition (CGMethod.hpp:1279-1282)
+    const bool limit = (s.energy_call_limit != 0 && s.num_energy_call > s.energy_call_limit) ||
+                       (s.force_call_limit != 0 && s.num_force_call > s.force_call_limit);
+    const bool conv = s.grad_inf_norm < s.grad_tol || s.energy_rel_change < s.energy_rel_tol;
+    if (limit || conv) {
+        s.done = 1;
+        s.call_limit = limit;
+        L.K = 0;
+    } else {
+        begin_line_search(s, L);
+    }
+}
+
 // direction pass: d = F + beta*d (dir_mode 0) or d = F + 0*d (1), d.F, max|d|.
 __global__ void __launch_bounds__(kVecThreads) k_cg_dir(int n3, const double* __restrict__ x, double* __restrict__ d,
                                                         const double* __restrict__ f0, const double* __restrict__ f1,
@@ -328,31 +363,8 @@ __global__ void __launch_bounds__(kVecThreads) k_cg_dir(int n3, const double* __
     if (!last_block(&st->ticket_dir)) return;
     reduce_partials(part, gridDim.x, a, b, m, sm);
     if (threadIdx.x != 0) return;
-    CGState& s = *st;
-    s.ticket_dir = 0;
-    s.copy_min_e = 0;
-    s.dmax = m;
-    if (s.dir_mode == 0 && a <= 0) {
-        // conjugacy lost: resetCGParams (d = F; its d.F is F.F)
-        s.reset_after_dir = 1;
-        s.slope = s.new_grad;
-        s.dmax = s.grad_inf_norm;
-    } else {
-        s.slope = a;
-    }
-    if (s.method != MEDYAN_CG_STEEPEST) s.last_fdotf = s.new_grad;
-    s.dir_mode = 0;
-    // loop condition (CGMethod.hpp:1279-1282)
-    const bool limit = (s.energy_call_limit != 0 && s.num_energy_call > s.energy_call_limit) ||
-                       (s.force_call_limit != 0 && s.num_force_call > s.force_call_limit);
-    const bool conv = s.grad_inf_norm < s.grad_tol || s.energy_rel_change < s.energy_rel_tol;
-    if (limit || conv) {
-        s.done = 1;
-        s.call_limit = limit;
-        L->K = 0;
-    } else {
-        begin_line_search(s, *L);
-    }
+    st->ticket_dir = 0;
+    dir_tail(*st, *L, a, m);
 }
 
 __global__ void __launch_bounds__(kVecThreads) k_cg_reset_dir(int n3, double* __restrict__ d,

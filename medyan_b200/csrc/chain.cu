@@ -115,18 +115,28 @@ template <class R>
 __global__ void __launch_bounds__(kThreads) k_chain_energy(const ChainDev ch, const double* __restrict__ x,
                                                            const double* __restrict__ d,
                                                            const LambdaSet* __restrict__ lset,
-                                                           double* __restrict__ partial, int nblk_total, int blk_off) {
+                                                           double* __restrict__ partial, int nblk_total, int blk_off,
+                                                           const int4* __restrict__ table) {
     __shared__ double sm[4 * 32];
     const int n = ch.n_pos;
     const int K = lset ? lset->K : 1;
     const int lane = threadIdx.x & 31;
-    const int nw = (gridDim.x * blockDim.x) >> 5;
+    // grid-stride over all positions, or (table) this block's chunk
+    // [table.y, table.z) of one replica's positions
+    int lo = 0, hi = n, w0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, ws = (gridDim.x * blockDim.x) >> 5;
+    if (table) {
+        const int4 t = table[blockIdx.x];
+        lo = t.y;
+        hi = t.z;
+        w0 = threadIdx.x >> 5;
+        ws = blockDim.x >> 5;
+    }
     double acc[kMaxLambda][2];
 #pragma unroll
     for (int k = 0; k < kMaxLambda; ++k) acc[k][0] = acc[k][1] = 0.0;
-    for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; (long long)w * 32 < n; w += nw) {
-        const int q = w * 32 + lane;
-        const bool in = q < n;
+    for (int w = w0; lo + (long long)w * 32 < hi; w += ws) {
+        const int q = lo + w * 32 + lane;
+        const bool in = q < hi;
         const int qe = lane == 0 ? q - 1 : q + 1;
         const V3 c = pos_of(x, n, q), dc = d ? pos_of(d, n, q) : V3{0.0, 0.0, 0.0};
         V3 ce{0.0, 0.0, 0.0}, de{0.0, 0.0, 0.0};
@@ -219,13 +229,15 @@ void launch_chain_forces(const ChainDev& ch, int prec, const double* x, const Fo
 }
 
 void launch_chain_energy(const ChainDev& ch, int prec, const double* x, const double* d, const LambdaSet* lam,
-                         double* partial, int nblk_total, int blk_off, cudaStream_t s) {
+                         double* partial, int nblk_total, int blk_off, cudaStream_t s, const int4* table,
+                         int table_blocks) {
     if (ch.n_pos <= 0) return;
-    const int g = chain_blocks(ch);
+    const int g = table ? table_blocks : chain_blocks(ch);
+    if (g <= 0) return;
     if (prec == MEDYAN_PREC_MIXED)
-        k_chain_energy<float><<<g, kThreads, 0, s>>>(ch, x, d, lam, partial, nblk_total, blk_off);
+        k_chain_energy<float><<<g, kThreads, 0, s>>>(ch, x, d, lam, partial, nblk_total, blk_off, table);
     else
-        k_chain_energy<double><<<g, kThreads, 0, s>>>(ch, x, d, lam, partial, nblk_total, blk_off);
+        k_chain_energy<double><<<g, kThreads, 0, s>>>(ch, x, d, lam, partial, nblk_total, blk_off, table);
 }
 
 void launch_to_internal(int n3, const int* order, const double* ext, double* in, cudaStream_t s) {

@@ -8,7 +8,9 @@
 // potentials. Energy passes evaluate up to kMaxLambda positions x + lam*d per
 // interaction from one read of the interaction record and of x and d; the
 // per-block sums are reduced deterministically by the finish kernel. Forces
-// are accumulated into the FP64 force array with atomic adds.
+// are accumulated into the FP64 force array with atomic adds. A record whose
+// first bead offset is -1 is padding (batched layouts align each replica's
+// records to whole blocks) and contributes nothing.
 #include "internal.h"
 #include "potentials.cuh"
 
@@ -50,6 +52,7 @@ __global__ void __launch_bounds__(kBlock) k_bonded_energy(const DeviceFF ff, con
         case 0:
             if (has_seg<S0, S1>(0) && i < ff.n_stretch) {
                 int2 q = ff.stretch_bs[i];
+                if (q.x < 0) break;  // padding record
                 double2 p = ff.stretch_p[i];
                 pa = double4{p.x, p.y, 0, 0};
                 X[0] = load3(x + q.x);
@@ -61,6 +64,7 @@ __global__ void __launch_bounds__(kBlock) k_bonded_energy(const DeviceFF ff, con
         case 1:
             if (has_seg<S0, S1>(1) && i < ff.n_bend) {
                 int4 q = ff.bend_bs[i];
+                if (q.x < 0) break;
                 double2 p = ff.bend_p[i];
                 pa = double4{p.x, p.y, 0, 0};
                 X[0] = load3(x + q.x);
@@ -75,6 +79,7 @@ __global__ void __launch_bounds__(kBlock) k_bonded_energy(const DeviceFF ff, con
             const int n = s == 2 ? ff.n_linker : ff.n_motor;
             if ((has_seg<S0, S1>(2) || has_seg<S0, S1>(3)) && i < n) {
                 int4 q = s == 2 ? ff.linker_bs[i] : ff.motor_bs[i];
+                if (q.x < 0) break;
                 pa = s == 2 ? ff.linker_p[i] : ff.motor_p[i];
                 X[0] = load3(x + q.x);
                 X[1] = load3(x + q.y);
@@ -90,6 +95,7 @@ __global__ void __launch_bounds__(kBlock) k_bonded_energy(const DeviceFF ff, con
         case 4:
             if (has_seg<S0, S1>(4) && i < ff.n_branch) {
                 int4 q = ff.branch_bs[i];
+                if (q.x < 0) break;
                 pa = ff.branch_pa[i];
                 pb = ff.branch_pb[i];
                 X[0] = load3(x + q.x);
@@ -105,6 +111,7 @@ __global__ void __launch_bounds__(kBlock) k_bonded_energy(const DeviceFF ff, con
         default:
             if (has_seg<S0, S1>(5) && i < ff.n_boundary) {
                 int o = ff.boundary_bs[i];
+                if (o < 0) break;
                 double2 p = ff.boundary_p[i];
                 plane = ff.boundary_plane[i];
                 pa = double4{p.x, p.y, 0, 0};
@@ -185,6 +192,7 @@ __global__ void __launch_bounds__(kBlock) k_bonded_forces(const DeviceFF ff, con
         case 0:
             if (has_seg<S0, S1>(0) && i < ff.n_stretch) {
                 int2 q = ff.stretch_bs[i];
+                if (q.x < 0) break;  // padding record
                 double2 p = ff.stretch_p[i];
                 T3<R> F = stretch_force<R>(P(q.x), P(q.y), p.x, p.y);
                 add_force(f, q.y, F.x, F.y, F.z);
@@ -194,6 +202,7 @@ __global__ void __launch_bounds__(kBlock) k_bonded_forces(const DeviceFF ff, con
         case 1:
             if (has_seg<S0, S1>(1) && i < ff.n_bend) {
                 int4 q = ff.bend_bs[i];
+                if (q.x < 0) break;
                 double2 p = ff.bend_p[i];
                 V3 c1 = P(q.x), c2 = P(q.y), c3 = P(q.z);
                 T3<R> Fr1, Fr2;
@@ -208,6 +217,7 @@ __global__ void __launch_bounds__(kBlock) k_bonded_forces(const DeviceFF ff, con
             const int n = s == 2 ? ff.n_linker : ff.n_motor;
             if ((has_seg<S0, S1>(2) || has_seg<S0, S1>(3)) && i < n) {
                 int4 q = s == 2 ? ff.linker_bs[i] : ff.motor_bs[i];
+                if (q.x < 0) break;
                 double4 p = s == 2 ? ff.linker_p[i] : ff.motor_p[i];
                 T3<R> Fl = spring_force<R>(P(q.x), P(q.y), P(q.z), P(q.w), p.x, p.y, p.z, p.w);
                 const R a1 = R(1) - R(p.z), a2 = R(p.z), b1 = R(1) - R(p.w), b2 = R(p.w);
@@ -221,6 +231,7 @@ __global__ void __launch_bounds__(kBlock) k_bonded_forces(const DeviceFF ff, con
         case 4:
             if (has_seg<S0, S1>(4) && i < ff.n_branch) {
                 int4 q = ff.branch_bs[i];
+                if (q.x < 0) break;
                 double4 pa = ff.branch_pa[i], pb = ff.branch_pb[i];
                 V3 c1 = P(q.x), c2 = P(q.y), c3 = P(q.z), c4 = P(q.w);
                 T3<R> F1{0, 0, 0}, F2{0, 0, 0}, F3{0, 0, 0}, F4{0, 0, 0};
@@ -263,6 +274,7 @@ __global__ void __launch_bounds__(kBlock) k_bonded_forces(const DeviceFF ff, con
         default:
             if (has_seg<S0, S1>(5) && i < ff.n_boundary) {
                 int o = ff.boundary_bs[i];
+                if (o < 0) break;
                 double2 p = ff.boundary_p[i];
                 double4 pl = ff.planes[ff.boundary_plane[i]];
                 R f0 = boundary_force_mag<R>(pl, P(o), p.x, p.y);
@@ -314,26 +326,33 @@ void join_from(const Fork* fk, cudaStream_t s, int n) {
 
 }  // namespace
 
+void launch_energy_producers(const ChainDev& ch, const DeviceFF& ff, const double* x, const double* d,
+                             const LambdaSet* lam, const EnergyScratch& es, cudaStream_t s, const Fork* fk,
+                             const int4* chain_table, int chain_table_blocks) {
+    // five branches: chain | excluded volume | linker, motor | branching |
+    // boundary, filament leftovers
+    cudaStream_t b[kForkWays] = {s, s, s, s};
+    if (fk) {
+        fork_to(fk, s, kForkWays);
+        for (int k = 0; k < kForkWays; ++k) b[k] = fk->side[k];
+    }
+    launch_excl_energy(ff, MEDYAN_PREC_FP64, x, d, lam, es, b[0]);
+    bonded_energy_group<2, 4>(ff, x, d, lam, es, b[1]);
+    bonded_energy_group<4, 5>(ff, x, d, lam, es, b[2]);
+    bonded_energy_group<5, 6>(ff, x, d, lam, es, b[3]);
+    bonded_energy_group<0, 2>(ff, x, d, lam, es, b[3]);
+    launch_chain_energy(ch, MEDYAN_PREC_FP64, x, d, lam, es.partial, es.total(), 0, s, chain_table,
+                        chain_table_blocks);
+    if (fk) join_from(fk, s, kForkWays);
+}
+
 void launch_energy(const ChainDev& ch, const DeviceFF& ff, int prec, const double* x, const double* d,
                    const LambdaSet* lam, const EnergyScratch& es, cudaStream_t s, const Fork* fk) {
     // Energies are evaluated in double in both precision modes: the backtracking
     // line search compares totals whose differences are ~1e-9 of the total,
     // below float resolution per term. Only the force pass runs in float.
     (void)prec;
-    // five branches: chain | excluded volume | linker, motor | branching |
-    // boundary, filament leftovers; then the finish kernel
-    cudaStream_t b[kForkWays] = {s, s, s, s};
-    if (fk) {
-        fork_to(fk, s, kForkWays);
-        for (int k = 0; k < kForkWays; ++k) b[k] = fk->side[k];
-    }
-    launch_excl_energy(ff, prec, x, d, lam, es, b[0]);
-    bonded_energy_group<2, 4>(ff, x, d, lam, es, b[1]);
-    bonded_energy_group<4, 5>(ff, x, d, lam, es, b[2]);
-    bonded_energy_group<5, 6>(ff, x, d, lam, es, b[3]);
-    bonded_energy_group<0, 2>(ff, x, d, lam, es, b[3]);
-    launch_chain_energy(ch, MEDYAN_PREC_FP64, x, d, lam, es.partial, es.total(), 0, s);
-    if (fk) join_from(fk, s, kForkWays);
+    launch_energy_producers(ch, ff, x, d, lam, es, s, fk, nullptr, 0);
     launch_excl_energy_fallback_and_finish(ff, x, d, lam, es, s);
 }
 

@@ -111,8 +111,11 @@ void launch_energy(const ChainDev& ch, const DeviceFF& ff, int prec, const doubl
 void launch_forces(const ChainDev& ch, const DeviceFF& ff, int prec, const double* x, const ForceTarget& t,
                    const ForceScratch& fs, cudaStream_t s, const Fork* fk = nullptr);
 void launch_chain_forces(const ChainDev& ch, int prec, const double* x, const ForceTarget& t, cudaStream_t s);
+// table (optional): block b evaluates positions [table[b].y, table[b].z) of one
+// replica (batched layouts), table_blocks blocks; else a grid-stride pass.
 void launch_chain_energy(const ChainDev& ch, int prec, const double* x, const double* d, const LambdaSet* lam,
-                         double* partial, int nblk_total, int blk_off, cudaStream_t s);
+                         double* partial, int nblk_total, int blk_off, cudaStream_t s,
+                         const int4* table = nullptr, int table_blocks = 0);
 int chain_blocks(const ChainDev& ch);
 void chain_order(const medyan_system* s, std::vector<int>& order);
 void build_chains(const medyan_system* s, const std::vector<int>& pos, ChainHost& out);
@@ -128,6 +131,15 @@ void launch_excl_energy_fallback_and_finish(const DeviceFF& ff, const double* x,
                                             const LambdaSet* lam, const EnergyScratch& es, cudaStream_t s);
 
 // One-time per-device kernel attributes (forceN's 80 KB abscissa table).
+// Batched energy finish (one block per replica); see excl_kernels.cu.
+void launch_energy_finish_batched(const DeviceFF& ff, const double* x, const double* d, const LambdaSet* lam,
+                                  const EnergyScratch& es, const int* rows_chain, const int* rows_seg,
+                                  const int* rows_excl, const int* excl_pairs, int R, double* out, cudaStream_t s);
+// Energy producers only (chain, bonded groups, excluded volume), no finish.
+void launch_energy_producers(const ChainDev& ch, const DeviceFF& ff, const double* x, const double* d,
+                             const LambdaSet* lam, const EnergyScratch& es, cudaStream_t s, const Fork* fk,
+                             const int4* chain_table, int chain_table_blocks);
+
 // Fills the quadrature grids of the excluded-volume fallbacks, once per
 // device (the current one); call before any stream capture.
 cudaError_t init_excl_kernels();
