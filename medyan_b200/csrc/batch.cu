@@ -1,19 +1,22 @@
 // batch.cu — many independent networks minimized together.
 //
-// Each replica gets its own handle (device buffers, internal bead order,
-// stream, pass graphs and minimization graph). A batch minimization enqueues
-// every replica's whole minimization (one graph launch each, with its
-// conditional loops running on the device) on its own stream before waiting
-// for any, so the replicas run concurrently and each finishes as soon as its
-// own convergence test passes: the per-replica convergence mask is the
-// replica's own loop condition. Results are identical to minimizing each
-// replica alone (CGMethod::minimize semantics per replica).
+// Each replica keeps its own handle (vectorization, internal bead order,
+// device neighbor list, single-network passes). A batched minimization packs
+// the replicas' device arrays into one set (pbatch.h) and runs one
+// conjugate-gradient loop for all of them: every force and energy kernel
+// launches once per pass for the whole batch, while the CG state, the
+// line-search step sizes and the reductions stay per replica, so each replica
+// follows CGMethod::minimize exactly and stops at its own convergence test
+// (a done replica is masked out of the remaining iterations).
+#include <cstring>
 #include <vector>
 
 #include "handle.h"
+#include "pbatch.h"
 
 struct medyan_batch {
     std::vector<medyan_mech*> h;
+    mb::PackedBatch pb;
     ~medyan_batch() {
         for (auto* p : h) medyan_mech_destroy(p);
     }
@@ -58,21 +61,60 @@ medyan_status medyan_batch_minimize(medyan_batch* b, const medyan_cg_params* p, 
                                     double* const* forces_out, medyan_min_result* results, int32_t* statuses) {
     if (!b || !p || (!b->h.empty() && (!coords_inout || !statuses))) return MEDYAN_ERR_INVALID_ARG;
     const int n = (int)b->h.size();
+    if (n == 0) return MEDYAN_OK;
     for (int r = 0; r < n; ++r)
-        if (!coords_inout[r]) return MEDYAN_ERR_INVALID_ARG;
-    // enqueue every replica first, then collect in order; a replica that
-    // could not be enqueued reports its own status and is not collected
-    std::vector<medyan_status> enq(n);
-    for (int r = 0; r < n; ++r) enq[r] = cg_enqueue(b->h[r], p, coords_inout[r]);
+        if (!coords_inout[r] && b->h[r]->n_beads) return MEDYAN_ERR_INVALID_ARG;
+    PackedBatch& pb = b->pb;
+    medyan_status st = pack_batch(pb, b->h);
+    if (st != MEDYAN_OK) return st;
+    cudaStream_t s = pb.stream;
+    for (int r = 0; r < n; ++r) {
+        cudaError_t e = coords_to_device(b->h[r], coords_inout[r], pb.x.raw() + 3 * (size_t)pb.base[r], s);
+        if (e != cudaSuccess) return cuda_status(e);
+    }
+    st = cg_batch_run(pb, b->h[0]->prec, p);
+    if (st != MEDYAN_OK) return st;
+    std::vector<CGState> sf(n);
+    std::vector<double> eo((size_t)n * 2 * (MEDYAN_FF_COUNT + 1));
+    cudaError_t e = cudaMemcpyAsync(sf.data(), pb.st.raw(), sizeof(CGState) * n, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(eo.data(), pb.eout.raw(), sizeof(double) * eo.size(), cudaMemcpyDeviceToHost, s);
+    for (int r = 0; r < n && e == cudaSuccess; ++r) {
+        const size_t o = 3 * (size_t)pb.base[r];
+        e = coords_to_host(b->h[r], pb.x.raw() + o, coords_inout[r], s);
+        if (e == cudaSuccess && forces_out && forces_out[r]) e = coords_to_host(b->h[r], pb.fcur.raw() + o, forces_out[r], s);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_status(e);
+    const int kOut = MEDYAN_FF_COUNT + 1;
     medyan_status worst = MEDYAN_OK;
     for (int r = 0; r < n; ++r) {
-        medyan_status st = enq[r];
-        if (st == MEDYAN_OK)
-            st = cg_collect(b->h[r], coords_inout[r], forces_out ? forces_out[r] : nullptr,
-                            results ? &results[r] : nullptr);
-        statuses[r] = st;
-        // a failed line search is a per-replica result; anything else is an error
-        if (st != MEDYAN_OK && st != MEDYAN_ERR_LINE_SEARCH && worst == MEDYAN_OK) worst = st;
+        const CGState& c = sf[r];
+        statuses[r] = c.status;
+        if (c.status != MEDYAN_OK && c.status != MEDYAN_ERR_LINE_SEARCH && worst == MEDYAN_OK)
+            worst = (medyan_status)c.status;
+        if (!results) continue;
+        medyan_min_result& out = results[r];
+        std::memset(&out, 0, sizeof out);
+        const double* before = eo.data() + (size_t)r * 2 * kOut;
+        const double* after = before + kOut;
+        const bool ls = c.status == MEDYAN_ERR_LINE_SEARCH;
+        for (int i = 0; i < MEDYAN_FF_COUNT; ++i) {
+            out.energy_before[i] = before[i];
+            out.energy_after[i] = ls ? 0.0 : after[i];
+        }
+        out.energy_before_total = before[MEDYAN_FF_COUNT];
+        out.energy_after_total = ls ? 0.0 : after[MEDYAN_FF_COUNT];
+        out.error_flags = (uint32_t)c.error_flags;
+        out.num_energy_call = c.num_energy_call;
+        out.energy_call_limit = c.energy_call_limit;
+        out.num_force_call = c.num_force_call;
+        out.force_call_limit = c.force_call_limit;
+        out.num_iter = c.num_iter;
+        out.grad_inf_norm = c.grad_inf_norm;
+        out.grad_tol = c.grad_tol;
+        out.energy_rel_change = c.energy_rel_change;
+        out.energy_rel_tol = c.energy_rel_tol;
     }
     return worst;
 }

@@ -32,6 +32,7 @@
 
 #include "device_math.cuh"
 #include "handle.h"
+#include "pbatch.h"
 
 namespace mb {
 
@@ -434,6 +435,190 @@ __global__ void k_cond_iter(const CGState* __restrict__ st, cudaGraphConditional
     cudaGraphSetConditional(h, st->done ? 0u : 1u);
 }
 
+// ------------------------------------------------------------ batched form
+// One block per replica for the vector passes (bead range [base[r],
+// base[r+1])); one thread per replica for the scalar steps. The per-replica
+// scalar logic is the single-network code above (dots_tail, dir_tail,
+// ls_decide, fill_pass).
+//
+// Step sizes: every replica's trials in a line-search pass are lam0_r * 2^-j
+// (fill_pass halves), so the energy kernels evaluate x + Lg.lam[k] * dS with
+// dS = lam0_r * d per replica and Lg.lam = {1, 1/2, 1/4, 1/8} (preceded by 0
+// when some replica needs E(x)): scaling by a power of two is exact, so each
+// position is bitwise the reference's x + lam * d. The force pass uses
+// dS = lam_move_r * d with step 1.
+
+// Global pass plan from the replicas' lambda sets (one block).
+__global__ void k_b_plan(int R, CGState* __restrict__ st, LambdaSet* __restrict__ Lr, LambdaSet* __restrict__ Lg,
+                         double* __restrict__ lam0, int* __restrict__ off) {
+    __shared__ int e0s, maxt;
+    if (threadIdx.x == 0) {
+        e0s = 0;
+        maxt = 0;
+    }
+    __syncthreads();
+    for (int r = threadIdx.x; r < R; r += blockDim.x) {
+        const CGState& s = st[r];
+        if (!s.done && s.ls_active && Lr[r].K > 0 && s.need_e0) atomicOr(&e0s, 1);
+    }
+    __syncthreads();
+    const int e0 = e0s;
+    for (int r = threadIdx.x; r < R; r += blockDim.x) {
+        const CGState& s = st[r];
+        LambdaSet& L = Lr[r];
+        if (s.done || !s.ls_active || L.K <= 0) {
+            lam0[r] = 0.0;
+            off[r] = 0;
+            continue;
+        }
+        const int ne = s.need_e0 ? 1 : 0;
+        int t = L.K - ne;
+        const int cap = kMaxLambda - e0;  // trial slots this pass can hold
+        if (t > cap) t = cap;             // the rest follow in the next pass
+        L.K = ne + t;
+        lam0[r] = t > 0 ? L.lam[ne] : 0.0;
+        off[r] = (e0 && !ne) ? 1 : 0;
+        atomicMax(&maxt, t);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        LambdaSet g{};
+        int k = 0;
+        if (e0) g.lam[k++] = 0.0;
+        double l = 1.0;
+        for (int j = 0; j < maxt && k < kMaxLambda; ++j, l *= 0.5) g.lam[k++] = l;
+        g.K = (e0 || maxt) ? k : 0;
+        *Lg = g;
+    }
+}
+
+// dS = lam0_r * d (line search) or lam_move_r * d (force pass), per replica.
+__global__ void __launch_bounds__(kVecThreads) k_b_scale(const int* __restrict__ base, const double* __restrict__ d,
+                                                         double* __restrict__ dS, const CGState* __restrict__ st,
+                                                         const double* __restrict__ lam0, int force_pass) {
+    const int r = blockIdx.x;
+    const CGState& s = st[r];
+    double lam;
+    if (force_pass) lam = (s.done || s.skip_force) ? 0.0 : s.lam_move;
+    else lam = lam0[r];
+    const int i0 = 3 * base[r], i1 = 3 * base[r + 1];
+    for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x) dS[i] = __dmul_rn(lam, d[i]);
+}
+
+__global__ void k_b_decide(int R, CGState* __restrict__ st, LambdaSet* __restrict__ Lr,
+                           const double* __restrict__ out, const int* __restrict__ off, int* __restrict__ fb_count,
+                           int* __restrict__ bad) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r == 0) {
+        *fb_count = 0;  // every replica's finish block has read the queue
+        for (int k = 0; k < kMaxLambda; ++k) bad[k] = 0;
+    }
+    if (r >= R) return;
+    ls_decide(st[r], Lr[r], out + ((size_t)r * kMaxLambda + off[r]) * kOut);
+}
+
+// dots pass per replica: commit the move, F.F, F.Fprev, max|F|; the new
+// force becomes the current one.
+__global__ void __launch_bounds__(kVecThreads) k_b_dots(const int* __restrict__ base, double* __restrict__ x,
+                                                        const double* __restrict__ d, double* __restrict__ fcur,
+                                                        const double* __restrict__ fnew, CGState* __restrict__ st) {
+    __shared__ double sm[96];
+    const int r = blockIdx.x;
+    CGState& s = st[r];
+    if (s.done || s.skip_force) return;
+    const double lam = s.lam_move;
+    double a = 0.0, b = 0.0, m = 0.0;
+    const int i0 = 3 * base[r], i1 = 3 * base[r + 1];
+    for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+        x[i] = move1(x[i], lam, d[i]);
+        const double fn = fnew[i], fo = fcur[i];
+        a += fn * fn;
+        b += fn * fo;
+        m = dmax_ref(m, fabs(fn));
+        fcur[i] = fn;
+    }
+    block_reduce3(a, b, m, sm);
+    if (threadIdx.x == 0) dots_tail(s, a, b, m);
+}
+
+__global__ void __launch_bounds__(kVecThreads) k_b_dir(const int* __restrict__ base, const double* __restrict__ x,
+                                                       double* __restrict__ d, const double* __restrict__ fcur,
+                                                       CGState* __restrict__ st, double* __restrict__ min_e,
+                                                       LambdaSet* __restrict__ Lr) {
+    __shared__ double sm[96];
+    const int r = blockIdx.x;
+    CGState& s = st[r];
+    if (s.done || s.ls_active) return;
+    const double beta = s.dir_mode ? 0.0 : s.beta;
+    const bool copy = s.copy_min_e;
+    double a = 0.0, b = 0.0, m = 0.0;
+    const int i0 = 3 * base[r], i1 = 3 * base[r + 1];
+    for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+        const double fi = fcur[i];
+        const double dn = fi + beta * d[i];
+        d[i] = dn;
+        a += dn * fi;
+        m = dmax_ref(m, fabs(dn));
+        if (copy) min_e[i] = x[i];
+    }
+    block_reduce3(a, b, m, sm);
+    if (threadIdx.x == 0) dir_tail(s, Lr[r], a, m);
+}
+
+__global__ void __launch_bounds__(kVecThreads) k_b_reset(const int* __restrict__ base, double* __restrict__ d,
+                                                         const double* __restrict__ fcur,
+                                                         const CGState* __restrict__ st) {
+    const int r = blockIdx.x;
+    if (!st[r].reset_after_dir) return;
+    const int i0 = 3 * base[r], i1 = 3 * base[r + 1];
+    for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x) d[i] = fcur[i] + 0.0 * d[i];
+}
+
+// energiesBefore (before = 1) or energiesAfter, per replica, from slot 0.
+__global__ void k_b_record(int R, CGState* __restrict__ st, const double* __restrict__ out,
+                           double* __restrict__ eout, int before) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= R) return;
+    CGState& s = st[r];
+    if (!before && s.status == MEDYAN_ERR_LINE_SEARCH) return;
+    const double* o = out + (size_t)r * kMaxLambda * kOut;
+    double* dst = eout + ((size_t)r * 2 + (before ? 0 : 1)) * kOut;
+    double tot = 0.0;
+    for (int i = 0; i < MEDYAN_FF_COUNT; ++i) {
+        dst[i] = o[i];
+        tot += o[i];
+    }
+    dst[MEDYAN_FF_COUNT] = tot;
+    s.num_energy_call++;
+    if (before) {
+        s.prev_energy = tot;
+        s.need_e0 = 1;
+    }
+}
+
+__global__ void __launch_bounds__(kVecThreads) k_b_finalize(const int* __restrict__ base, double* __restrict__ x,
+                                                            const double* __restrict__ minE,
+                                                            const CGState* __restrict__ st) {
+    const int r = blockIdx.x;
+    const CGState& s = st[r];
+    if (!(s.status != MEDYAN_ERR_LINE_SEARCH && s.call_limit && s.have_min_e)) return;
+    const int i0 = 3 * base[r], i1 = 3 * base[r + 1];
+    for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x) x[i] = minE[i];
+}
+
+// Loop conditions: any replica still iterating / still in a line search.
+__global__ void k_b_cond(int R, const CGState* __restrict__ st, cudaGraphConditionalHandle h, int ls) {
+    __shared__ int any;
+    if (threadIdx.x == 0) any = 0;
+    __syncthreads();
+    for (int r = threadIdx.x; r < R; r += blockDim.x) {
+        const CGState& s = st[r];
+        if (!s.done && (!ls || s.ls_active)) any = 1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) cudaGraphSetConditional(h, any ? 1u : 0u);
+}
+
 }  // namespace
 
 // ----------------------------------------------------------------- host side
@@ -683,6 +868,188 @@ medyan_status cg_collect(medyan_mech* h, double* coord_out, double* force_out, m
         out->energy_rel_tol = sf.energy_rel_tol;
     }
     return (medyan_status)sf.status;
+}
+
+namespace {
+
+void b_energy_pass(PackedBatch& pb, const double* dS, const LambdaSet* L, cudaStream_t s) {
+    launch_energy_producers(pb.ch, pb.ff, pb.x.raw(), dS, L, pb.es, s, &pb.fork, pb.chain_table.raw(),
+                            pb.n_chain_blocks);
+    launch_energy_finish_batched(pb.ff, pb.x.raw(), dS, L, pb.es, pb.rows_chain(), pb.rows_seg(), pb.rows_excl(),
+                                 pb.excl_pairs(), pb.R, pb.out.raw(), s);
+}
+
+void b_step(PackedBatch& pb, int prec, cudaStream_t s) {
+    const int R = pb.R;
+    k_b_scale<<<R, kVecThreads, 0, s>>>(pb.base_dev.raw(), pb.d.raw(), pb.dS.raw(), pb.st.raw(), pb.lam0.raw(), 1);
+    const ForceTarget t{pb.fnew.raw(), nullptr, nullptr, nullptr, pb.dS.raw(), pb.one.raw()};
+    launch_forces(pb.ch, pb.ff, prec, pb.x.raw(), t, pb.fs, s, &pb.fork);
+    k_b_dots<<<R, kVecThreads, 0, s>>>(pb.base_dev.raw(), pb.x.raw(), pb.d.raw(), pb.fcur.raw(), pb.fnew.raw(),
+                                       pb.st.raw());
+    k_b_dir<<<R, kVecThreads, 0, s>>>(pb.base_dev.raw(), pb.x.raw(), pb.d.raw(), pb.fcur.raw(), pb.st.raw(),
+                                      pb.minE.raw(), pb.Lr.raw());
+    k_b_reset<<<R, kVecThreads, 0, s>>>(pb.base_dev.raw(), pb.d.raw(), pb.fcur.raw(), pb.st.raw());
+}
+
+void b_ls_pass(PackedBatch& pb, cudaStream_t s) {
+    const int R = pb.R;
+    k_b_plan<<<1, 256, 0, s>>>(R, pb.st.raw(), pb.Lr.raw(), pb.Lg.raw(), pb.lam0.raw(), pb.off.raw());
+    k_b_scale<<<R, kVecThreads, 0, s>>>(pb.base_dev.raw(), pb.d.raw(), pb.dS.raw(), pb.st.raw(), pb.lam0.raw(), 0);
+    b_energy_pass(pb, pb.dS.raw(), pb.Lg.raw(), s);
+    k_b_decide<<<(R + 127) / 128, 128, 0, s>>>(R, pb.st.raw(), pb.Lr.raw(), pb.out.raw(), pb.off.raw(),
+                                               pb.es.fb_count, pb.es.bad);
+}
+
+// WHILE(any replica iterating) { WHILE(any replica in a line search) { pass }; step }
+cudaError_t b_build_graph(PackedBatch& pb, int prec, cudaGraphExec_t* exec) {
+    const int R = pb.R;
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaGraphCreate(&g, 0);
+    if (e != cudaSuccess) return e;
+    cudaGraphConditionalHandle h_iter, h_ls;
+    e = cudaGraphConditionalHandleCreate(&h_iter, g, 1, cudaGraphCondAssignDefault);
+    cudaGraphNode_t n_iter;
+    cudaGraphNodeParams p_iter = {};
+    if (e == cudaSuccess) {
+        p_iter.type = cudaGraphNodeTypeConditional;
+        p_iter.conditional.handle = h_iter;
+        p_iter.conditional.type = cudaGraphCondTypeWhile;
+        p_iter.conditional.size = 1;
+        e = cudaGraphAddNode(&n_iter, g, nullptr, 0, &p_iter);
+    }
+    cudaGraph_t body = e == cudaSuccess ? p_iter.conditional.phGraph_out[0] : nullptr;
+    cudaStream_t s = nullptr;
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&h_ls, body, 0, 0);
+    cudaGraphNode_t n_arm = nullptr;
+    if (e == cudaSuccess) {
+        e = cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed);
+        if (e == cudaSuccess) {
+            k_b_cond<<<1, 256, 0, s>>>(R, pb.st.raw(), h_ls, 1);
+            cudaGraph_t tmp;
+            e = cudaStreamEndCapture(s, &tmp);
+        }
+        size_t nn = 0;
+        if (e == cudaSuccess) e = cudaGraphGetNodes(body, nullptr, &nn);
+        if (e == cudaSuccess && nn == 1) e = cudaGraphGetNodes(body, &n_arm, &nn);
+        if (e == cudaSuccess && !n_arm) e = cudaErrorUnknown;
+    }
+    cudaGraphNode_t n_ls;
+    cudaGraphNodeParams p_ls = {};
+    if (e == cudaSuccess) {
+        p_ls.type = cudaGraphNodeTypeConditional;
+        p_ls.conditional.handle = h_ls;
+        p_ls.conditional.type = cudaGraphCondTypeWhile;
+        p_ls.conditional.size = 1;
+        e = cudaGraphAddNode(&n_ls, body, &n_arm, 1, &p_ls);
+    }
+    if (e == cudaSuccess) {
+        cudaGraph_t ls_body = p_ls.conditional.phGraph_out[0];
+        e = cudaStreamBeginCaptureToGraph(s, ls_body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed);
+        if (e == cudaSuccess) {
+            b_ls_pass(pb, s);
+            k_b_cond<<<1, 256, 0, s>>>(R, pb.st.raw(), h_ls, 1);
+            cudaGraph_t tmp;
+            e = cudaStreamEndCapture(s, &tmp);
+        }
+    }
+    if (e == cudaSuccess) {
+        const cudaGraphNode_t deps[1] = {n_ls};
+        e = cudaStreamBeginCaptureToGraph(s, body, deps, nullptr, 1, cudaStreamCaptureModeRelaxed);
+        if (e == cudaSuccess) {
+            b_step(pb, prec, s);
+            k_b_cond<<<1, 256, 0, s>>>(R, pb.st.raw(), h_iter, 0);
+            cudaGraph_t tmp;
+            e = cudaStreamEndCapture(s, &tmp);
+        }
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(exec, g, 0);
+    if (s) cudaStreamDestroy(s);
+    cudaGraphDestroy(g);
+    return e;
+}
+
+}  // namespace
+
+// Batched CGMethod::minimize over the packed replicas; see the kernels above.
+medyan_status cg_batch_run(PackedBatch& pb, int prec, const medyan_cg_params* p) {
+    const int R = pb.R;
+    if (!p || p->method < 0 || p->method > 2 || !(p->max_dist > 0) || !(p->lambda_max > 0))
+        return MEDYAN_ERR_INVALID_ARG;
+    if (R == 0) return MEDYAN_OK;
+    const size_t n3 = 3 * (size_t)pb.nb;
+    cudaStream_t s = pb.stream;
+    cudaError_t e = cudaSuccess;
+    for (DevBuf<double>* b : {&pb.d, &pb.dS, &pb.fcur, &pb.fnew, &pb.minE})
+        if (e == cudaSuccess) e = b->reserve(n3 ? n3 : 1);
+    if (e == cudaSuccess) e = pb.out.reserve((size_t)R * kMaxLambda * kOut);
+    if (e == cudaSuccess) e = pb.eout.reserve((size_t)R * 2 * kOut);
+    if (e == cudaSuccess) e = pb.st.reserve(R);
+    if (e == cudaSuccess) e = pb.Lr.reserve(R);
+    if (e == cudaSuccess) e = pb.Lg.reserve(1);
+    if (e == cudaSuccess) e = pb.Lzero.reserve(1);
+    if (e == cudaSuccess) e = pb.lam0.reserve(R);
+    if (e == cudaSuccess) e = pb.off.reserve(R);
+    if (e == cudaSuccess) e = pb.one.reserve(1);
+    if (e != cudaSuccess) return cuda_status(e);
+
+    std::vector<CGState> s0(R);
+    for (int r = 0; r < R; ++r) {
+        CGState& c = s0[r];
+        c = CGState{};
+        const int nbr = pb.base[r + 1] - pb.base[r];
+        c.method = p->method;
+        c.try_to_recover = p->try_to_recover;
+        c.energy_call_limit = p->energy_call_limit;
+        c.force_call_limit = p->force_call_limit > 3 * nbr ? p->force_call_limit : 3 * nbr;
+        c.max_dist = p->max_dist;
+        c.lambda_max = p->lambda_max;
+        c.grad_tol = p->grad_tol;
+        c.energy_rel_tol = p->energy_rel_tol;
+        c.status = MEDYAN_OK;
+        c.parity = 1;
+        c.grad_inf_norm = __builtin_inf();
+        c.energy_rel_change = __builtin_inf();
+        c.min_e = __builtin_inf();
+    }
+    LambdaSet z{};
+    z.K = 1;
+    const double one = 1.0;
+    const size_t bytes = sizeof(double) * n3;
+    e = pb.st.assign(s0.data(), R, s);
+    if (e == cudaSuccess) e = pb.Lzero.assign(&z, 1, s);
+    if (e == cudaSuccess) e = pb.one.assign(&one, 1, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(pb.Lr.raw(), 0, sizeof(LambdaSet) * R, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(pb.d.raw(), 0, bytes ? bytes : 8, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(pb.fcur.raw(), 0, bytes ? bytes : 8, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(pb.fnew.raw(), 0, bytes ? bytes : 8, s);
+    if (e != cudaSuccess) return cuda_status(e);
+
+    // energiesBefore, then the first force, F.F, d = F
+    b_energy_pass(pb, nullptr, pb.Lzero.raw(), s);
+    k_b_decide<<<1, 1, 0, s>>>(0, pb.st.raw(), pb.Lr.raw(), pb.out.raw(), pb.off.raw(), pb.es.fb_count, pb.es.bad);
+    k_b_record<<<(R + 127) / 128, 128, 0, s>>>(R, pb.st.raw(), pb.out.raw(), pb.eout.raw(), 1);
+    b_step(pb, prec, s);
+
+    if (pb.graph && (pb.graph_gen != pb.gen || pb.graph_prec != prec)) {
+        cudaGraphExecDestroy(pb.graph);
+        pb.graph = nullptr;
+    }
+    if (!pb.graph) {
+        e = b_build_graph(pb, prec, &pb.graph);
+        if (e != cudaSuccess) return cuda_status(e);
+        pb.graph_gen = pb.gen;
+        pb.graph_prec = prec;
+    }
+    e = cudaGraphLaunch(pb.graph, s);
+    if (e != cudaSuccess) return cuda_status(e);
+
+    // epilogue and energiesAfter
+    k_b_finalize<<<R, kVecThreads, 0, s>>>(pb.base_dev.raw(), pb.x.raw(), pb.minE.raw(), pb.st.raw());
+    b_energy_pass(pb, nullptr, pb.Lzero.raw(), s);
+    k_b_decide<<<1, 1, 0, s>>>(0, pb.st.raw(), pb.Lr.raw(), pb.out.raw(), pb.off.raw(), pb.es.fb_count, pb.es.bad);
+    k_b_record<<<(R + 127) / 128, 128, 0, s>>>(R, pb.st.raw(), pb.out.raw(), pb.eout.raw(), 0);
+    return cuda_status(cudaGetLastError());
 }
 
 }  // namespace mb
