@@ -450,7 +450,7 @@ __global__ void k_cond_iter(const CGState* __restrict__ st, cudaGraphConditional
 
 // Global pass plan from the replicas' lambda sets (one block).
 __global__ void k_b_plan(int R, CGState* __restrict__ st, LambdaSet* __restrict__ Lr, LambdaSet* __restrict__ Lg,
-                         double* __restrict__ lam0, int* __restrict__ off) {
+                         double* __restrict__ lam0, int* __restrict__ off, int* __restrict__ act) {
     __shared__ int e0s, maxt;
     if (threadIdx.x == 0) {
         e0s = 0;
@@ -469,8 +469,10 @@ __global__ void k_b_plan(int R, CGState* __restrict__ st, LambdaSet* __restrict_
         if (s.done || !s.ls_active || L.K <= 0) {
             lam0[r] = 0.0;
             off[r] = 0;
+            act[r] = 0;
             continue;
         }
+        act[r] = 1;
         const int ne = s.need_e0 ? 1 : 0;
         int t = L.K - ne;
         const int cap = kMaxLambda - e0;  // trial slots this pass can hold
@@ -495,12 +497,20 @@ __global__ void k_b_plan(int R, CGState* __restrict__ st, LambdaSet* __restrict_
 // dS = lam0_r * d (line search) or lam_move_r * d (force pass), per replica.
 __global__ void __launch_bounds__(kVecThreads) k_b_scale(const int* __restrict__ base, const double* __restrict__ d,
                                                          double* __restrict__ dS, const CGState* __restrict__ st,
-                                                         const double* __restrict__ lam0, int force_pass) {
+                                                         const double* __restrict__ lam0, int force_pass,
+                                                         int* __restrict__ act) {
     const int r = blockIdx.x;
     const CGState& s = st[r];
     double lam;
-    if (force_pass) lam = (s.done || s.skip_force) ? 0.0 : s.lam_move;
-    else lam = lam0[r];
+    if (force_pass) {
+        const bool on = !(s.done || s.skip_force);
+        lam = on ? s.lam_move : 0.0;
+        if (threadIdx.x == 0) act[r] = on ? 1 : 0;
+        if (!on) return;
+    } else {
+        lam = lam0[r];
+        if (!act[r]) return;
+    }
     const int i0 = 3 * base[r], i1 = 3 * base[r + 1];
     for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x) dS[i] = __dmul_rn(lam, d[i]);
 }
@@ -572,6 +582,10 @@ __global__ void __launch_bounds__(kVecThreads) k_b_reset(const int* __restrict__
     if (!st[r].reset_after_dir) return;
     const int i0 = 3 * base[r], i1 = 3 * base[r + 1];
     for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x) d[i] = fcur[i] + 0.0 * d[i];
+}
+
+__global__ void k_b_act_all(int R, int* __restrict__ act) {
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < R; r += gridDim.x * blockDim.x) act[r] = 1;
 }
 
 // energiesBefore (before = 1) or energiesAfter, per replica, from slot 0.
@@ -881,7 +895,8 @@ void b_energy_pass(PackedBatch& pb, const double* dS, const LambdaSet* L, cudaSt
 
 void b_step(PackedBatch& pb, int prec, cudaStream_t s) {
     const int R = pb.R;
-    k_b_scale<<<R, kVecThreads, 0, s>>>(pb.base_dev.raw(), pb.d.raw(), pb.dS.raw(), pb.st.raw(), pb.lam0.raw(), 1);
+    k_b_scale<<<R, kVecThreads, 0, s>>>(pb.base_dev.raw(), pb.d.raw(), pb.dS.raw(), pb.st.raw(), pb.lam0.raw(), 1,
+                                        pb.act.raw());
     const ForceTarget t{pb.fnew.raw(), nullptr, nullptr, nullptr, pb.dS.raw(), pb.one.raw()};
     launch_forces(pb.ch, pb.ff, prec, pb.x.raw(), t, pb.fs, s, &pb.fork);
     k_b_dots<<<R, kVecThreads, 0, s>>>(pb.base_dev.raw(), pb.x.raw(), pb.d.raw(), pb.fcur.raw(), pb.fnew.raw(),
@@ -893,8 +908,9 @@ void b_step(PackedBatch& pb, int prec, cudaStream_t s) {
 
 void b_ls_pass(PackedBatch& pb, cudaStream_t s) {
     const int R = pb.R;
-    k_b_plan<<<1, 256, 0, s>>>(R, pb.st.raw(), pb.Lr.raw(), pb.Lg.raw(), pb.lam0.raw(), pb.off.raw());
-    k_b_scale<<<R, kVecThreads, 0, s>>>(pb.base_dev.raw(), pb.d.raw(), pb.dS.raw(), pb.st.raw(), pb.lam0.raw(), 0);
+    k_b_plan<<<1, 256, 0, s>>>(R, pb.st.raw(), pb.Lr.raw(), pb.Lg.raw(), pb.lam0.raw(), pb.off.raw(), pb.act.raw());
+    k_b_scale<<<R, kVecThreads, 0, s>>>(pb.base_dev.raw(), pb.d.raw(), pb.dS.raw(), pb.st.raw(), pb.lam0.raw(), 0,
+                                        pb.act.raw());
     b_energy_pass(pb, pb.dS.raw(), pb.Lg.raw(), s);
     k_b_decide<<<(R + 127) / 128, 128, 0, s>>>(R, pb.st.raw(), pb.Lr.raw(), pb.out.raw(), pb.off.raw(),
                                                pb.es.fb_count, pb.es.bad);
@@ -1026,6 +1042,7 @@ medyan_status cg_batch_run(PackedBatch& pb, int prec, const medyan_cg_params* p)
     if (e != cudaSuccess) return cuda_status(e);
 
     // energiesBefore, then the first force, F.F, d = F
+    k_b_act_all<<<(R + 255) / 256, 256, 0, s>>>(R, pb.act.raw());
     b_energy_pass(pb, nullptr, pb.Lzero.raw(), s);
     k_b_decide<<<1, 1, 0, s>>>(0, pb.st.raw(), pb.Lr.raw(), pb.out.raw(), pb.off.raw(), pb.es.fb_count, pb.es.bad);
     k_b_record<<<(R + 127) / 128, 128, 0, s>>>(R, pb.st.raw(), pb.out.raw(), pb.eout.raw(), 1);
@@ -1046,6 +1063,7 @@ medyan_status cg_batch_run(PackedBatch& pb, int prec, const medyan_cg_params* p)
 
     // epilogue and energiesAfter
     k_b_finalize<<<R, kVecThreads, 0, s>>>(pb.base_dev.raw(), pb.x.raw(), pb.minE.raw(), pb.st.raw());
+    k_b_act_all<<<(R + 255) / 256, 256, 0, s>>>(R, pb.act.raw());
     b_energy_pass(pb, nullptr, pb.Lzero.raw(), s);
     k_b_decide<<<1, 1, 0, s>>>(0, pb.st.raw(), pb.Lr.raw(), pb.out.raw(), pb.off.raw(), pb.es.fb_count, pb.es.bad);
     k_b_record<<<(R + 127) / 128, 128, 0, s>>>(R, pb.st.raw(), pb.out.raw(), pb.eout.raw(), 0);

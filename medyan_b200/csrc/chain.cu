@@ -97,7 +97,7 @@ __global__ void __launch_bounds__(kThreads) k_chain_forces(const ChainDev ch, co
         if (fl & kLink) F = stretch_force<R>(c, cnext, lp.x, lp.y);
         if (fl & kBend) bend_force<R>(diff<R>(cprev, c), diff<R>(c, cnext), bp.x, bp.y, A, B);
         const T3<R> Fp = shfl_up3(F), Bp = shfl_up3(B), An = shfl_down3(A);
-        if (lane >= 1 && lane <= kWarpOut && in) {
+        if (lane >= 1 && lane <= kWarpOut && in && (!ch.act || ch.act[ch.rep[q]])) {
             // link (q-1, q) acts on q; link (q, q+1) reacts on q; bends centred
             // at q-1 (third bead), q (middle), q+1 (first bead); summed in double
             f[3 * q] = double(Fp.x) - double(F.x) + double(Bp.x) + (double(A.x) - double(B.x)) - double(An.x);
@@ -126,6 +126,7 @@ __global__ void __launch_bounds__(kThreads) k_chain_energy(const ChainDev ch, co
     int lo = 0, hi = n, w0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, ws = (gridDim.x * blockDim.x) >> 5;
     if (table) {
         const int4 t = table[blockIdx.x];
+        if (ch.act && !ch.act[t.x]) return;  // replica not in this pass
         lo = t.y;
         hi = t.z;
         w0 = threadIdx.x >> 5;

@@ -29,6 +29,7 @@ __global__ void __launch_bounds__(kExclBlock) k_excl_energy(const DeviceFF ff, c
                                                             int blk_off, int* __restrict__ fb_count,
                                                             int2* __restrict__ fb_list, int* __restrict__ bad) {
     __shared__ double smem[4 * 32];
+    if (ff.act && !ff.act[ff.rep_excl[blockIdx.x]]) return;  // batched: replica not in this pass
     const int i = blockIdx.x * kExclBlock + threadIdx.x;
     const bool move = d != nullptr;
     bool valid = i < ff.n_excl;
@@ -79,6 +80,7 @@ __global__ void __launch_bounds__(kExclBlock) k_excl_forces(const DeviceFF ff, c
                                                             const ForceTarget tgt, int* __restrict__ fb_count,
                                                             int* __restrict__ fb_list, int* __restrict__ status) {
     if (tgt.skip && *tgt.skip) return;
+    if (ff.act && !ff.act[ff.rep_excl[blockIdx.x]]) return;  // batched: replica not in this pass
     const int i = blockIdx.x * kExclBlock + threadIdx.x;
     if (i >= ff.n_excl) return;
     double* __restrict__ f = target_force(tgt);
@@ -394,6 +396,7 @@ __global__ void __launch_bounds__(kFinishThreads) k_energy_finish_batched(
     __shared__ int2 mine[kFallbackCap];
     __shared__ int nfb;
     const int r = blockIdx.x;
+    if (ff.act && !ff.act[r]) return;  // replica not in this pass
     const int K = lset ? lset->K : 1;
     const int total_blocks = nch + nbb + nbe;
     if (threadIdx.x == 0) {

@@ -40,6 +40,7 @@ __global__ void __launch_bounds__(kBlock) k_bonded_energy(const DeviceFF ff, con
                                                           double* __restrict__ partial, int nblk_total, int blk_off) {
     __shared__ double smem[4 * 32];
     const int b = blockIdx.x + ff.seg[S0];
+    if (ff.act && !ff.act[ff.rep_bonded[b]]) return;  // batched: replica not in this pass
     const int s = segment_of<S0, S1>(ff, b);
     const int i = (b - ff.seg[s]) * kBlock + threadIdx.x;
     const bool move = d != nullptr;
@@ -186,6 +187,7 @@ __global__ void __launch_bounds__(kBlock) k_bonded_forces(const DeviceFF ff, con
     double* __restrict__ f = target_force(tgt);
     const PosLoader P{x, tgt.d, tgt.lam ? *tgt.lam : 0.0};
     const int b = blockIdx.x + ff.seg[S0];
+    if (ff.act && !ff.act[ff.rep_bonded[b]]) return;  // batched: replica not in this pass
     const int s = segment_of<S0, S1>(ff, b);
     const int i = (b - ff.seg[s]) * kBlock + threadIdx.x;
     switch (s) {

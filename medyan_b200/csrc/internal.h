@@ -33,6 +33,12 @@ struct DeviceFF {
     // Block ranges of the bonded kernel: [seg[s], seg[s+1]) for
     // stretch, bend, linker, motor, branch, boundary.
     int seg[7];
+    // batched layouts only (null otherwise): act[r] != 0 when replica r takes
+    // part in the current pass; the replica of each bonded / excluded-volume
+    // block. Blocks of inactive replicas do nothing.
+    const int* act;
+    const int* rep_bonded;
+    const int* rep_excl;
 };
 
 // Filament chains (chain.cu) over the internal bead order: chain position p
@@ -42,6 +48,10 @@ struct ChainDev {
     const unsigned char* flags;  // bit 0: link (p, p+1); bit 1: bend centred at p
     const double2* link_p;       // (k, l0) of link (p, p+1)
     const double2* bend_p;       // (k, theta0) of the bend centred at p
+    // batched layouts only (null otherwise): replica of each position and the
+    // pass's active mask; positions of inactive replicas are not written
+    const int* rep;
+    const int* act;
 };
 
 struct ChainHost {

@@ -232,7 +232,26 @@ medyan_status pack_batch(PackedBatch& pb, const std::vector<medyan_mech*>& h) {
             table.push_back(make_int4(r, p0, p0 + 256 < pb.base[r + 1] ? p0 + 256 : pb.base[r + 1], 0));
     }
     pb.n_chain_blocks = (int)table.size();
+    // replica of every position, bonded block and excluded-volume block
+    std::vector<int> rb(nb), rbb(ff.seg[6] > 0 ? ff.seg[6] : 1, 0), rbe(tot[S_EXCL] / kExclBlock + 1, 0);
+    for (int r = 0; r < R; ++r) {
+        for (int p = pb.base[r]; p < pb.base[r + 1]; ++p) rb[p] = r;
+        for (int q = 0; q < 6; ++q)
+            for (int blk = rs[q * (R + 1) + r]; blk < rs[q * (R + 1) + r + 1]; ++blk) rbb[blk] = r;
+        for (int blk = re[r]; blk < re[r + 1]; ++blk) rbe[blk] = r;
+    }
     e = pb.chain_table.assign(table.data(), table.size(), s);
+    if (e == cudaSuccess) e = pb.rep_bead.assign(rb.data(), rb.size(), s);
+    if (e == cudaSuccess) e = pb.rep_bonded.assign(rbb.data(), rbb.size(), s);
+    if (e == cudaSuccess) e = pb.rep_excl.assign(rbe.data(), rbe.size(), s);
+    if (e == cudaSuccess) e = pb.act.reserve(R);
+    if (e == cudaSuccess) {
+        ff.act = pb.act.raw();
+        ff.rep_bonded = pb.rep_bonded.raw();
+        ff.rep_excl = pb.rep_excl.raw();
+        pb.ch.rep = pb.rep_bead.raw();
+        pb.ch.act = pb.act.raw();
+    }
     if (e == cudaSuccess) e = pb.rows.assign(rows.data(), rows.size(), s);
     if (e == cudaSuccess) e = pb.base_dev.assign(pb.base.data(), pb.base.size(), s);
 

@@ -42,6 +42,8 @@ struct PackedBatch {
     DevBuf<int4> chain_table;         // chain energy block -> (replica, first, end position)
     int n_chain_blocks = 0;
     DevBuf<int> rows;                 // chain[R+1] | seg[6][R+1] | excl[R+1] | excl pairs[R+1]
+    DevBuf<int> rep_bead, rep_bonded, rep_excl;  // replica of each position / bonded block / excl block
+    DevBuf<int> act;                  // replicas taking part in the current pass
 
     // energy / force scratch
     EnergyScratch es{};
