@@ -228,6 +228,9 @@ typedef struct medyan_cg_params {
     int32_t energy_call_limit;      /* 0 = no limit                             */
     int32_t force_call_limit;       /* raised to max(limit, 3*n_beads)          */
     int32_t try_to_recover;         /* tryToRecoverInLineSearchError            */
+    int32_t line_search;            /* lineSearchAlgorithm: 0 BACKTRACKING,
+                                       1 QUADRATIC (quadraticLineSearchV2,
+                                       CGMethod.hpp:521-765; backtracking in safe mode) */
 } medyan_cg_params;
 
 /* MinimizationResult, src/Mechanics/Minimizer/MinimizationTypes.hpp:10-64. */

@@ -69,7 +69,7 @@ struct ConjugateGradientParams {
     double maxDist = 1.0;
     double lambdaMax = 0.01;
     double lambdaRunningAverageProbability = 0.0;  // only 0 is supported
-    std::string lineSearchAlgorithm = "BACKTRACKING";  // only BACKTRACKING is supported
+    std::string lineSearchAlgorithm = "BACKTRACKING";  // BACKTRACKING, or QUADRATIC (any other value, as in the reference)
     double gradTol = 1e-1;
     double energyRelTol = 1e-9;
     int energyCallLimit = 0;
@@ -218,8 +218,8 @@ class CGMethod {
 public:
     static MinimizationResult minimize(const ConjugateGradientParams& p, std::vector<double>& coord,
                                        ForceFieldManager& ffm, std::vector<double>* outForce = nullptr) {
-        if (p.lineSearchAlgorithm != "BACKTRACKING" || p.lambdaRunningAverageProbability != 0.0)
-            throw Error(MEDYAN_ERR_UNSUPPORTED, "CGMethod::minimize: line search");
+        if (p.lambdaRunningAverageProbability != 0.0)
+            throw Error(MEDYAN_ERR_UNSUPPORTED, "CGMethod::minimize: running-average lambda");
         if ((int)coord.size() != 3 * ffm.numBeads()) throw Error(MEDYAN_ERR_INVALID_ARG, "CGMethod::minimize: coord");
         medyan_cg_params cp{};
         cp.method = p.descentSearchMethod == ConjugateGradientDescentSearch::steepest         ? MEDYAN_CG_STEEPEST
@@ -232,6 +232,8 @@ public:
         cp.energy_call_limit = p.energyCallLimit;
         cp.force_call_limit = p.forceCallLimit;
         cp.try_to_recover = p.tryToRecoverInLineSearchError ? 1 : 0;
+        // CGMethod.hpp:1319-1332: anything but BACKTRACKING is quadraticLineSearchV2
+        cp.line_search = p.lineSearchAlgorithm == "BACKTRACKING" ? 0 : 1;
         if (outForce) outForce->resize(coord.size());
         medyan_min_result r{};
         medyan_status s = medyan_cg_minimize(ffm.handle(), &cp, coord.data(), outForce ? outForce->data() : nullptr, &r);

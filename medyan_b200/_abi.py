@@ -78,6 +78,7 @@ class CGParams(C.Structure):
         ("energy_call_limit", C.c_int32),
         ("force_call_limit", C.c_int32),
         ("try_to_recover", C.c_int32),
+        ("line_search", C.c_int32),
     ]
 
 

@@ -41,6 +41,8 @@ namespace {
 constexpr int kVecThreads = 256;
 constexpr double kLambdaTol = 1e-8;      // CGMethod::LAMBDATOL (double build)
 constexpr double kBacktrackSlope = 0.4;  // CGMethod::BACKTRACKSLOPE
+constexpr double kLambdaQuadTol = 1e-3;   // CGMethod::LAMBDAQUADTOL
+constexpr int kQuadMaxModels = 100;       // bound on quadraticoptimization's loop
 constexpr int kOut = MEDYAN_FF_COUNT + 1;
 
 int vec_blocks(int n3) {
@@ -78,6 +80,10 @@ __device__ void begin_line_search(CGState& s, LambdaSet& L) {
     s.skip_force = 1;
     s.move_kind = 0;
     s.reduced_slope = (s.safe_mode ? 0.0 : kBacktrackSlope) * s.slope;
+    // QUADRATIC: quadraticLineSearchV2, except in safe mode (CGMethod.hpp:1322-1324)
+    s.q_mode = s.ls_quad && !s.safe_mode;
+    s.q_phase = 0;
+    s.q_maxe = -__builtin_inf();
     if (s.grad_inf_norm == 0.0) {  // "return zero if no forces": lambda 0, no energy call
         s.ls_immediate_fail = 1;
         L.K = 0;
@@ -116,8 +122,97 @@ __device__ void line_search_failed(CGState& s) {
     }
 }
 
+// End of a quadratic line search with step lq (CGMethod.hpp:637-649):
+// lambda = 0 below LAMBDATOL; TotalEnergy and newEnergy stay the
+// backtracking energy. The energy at the new point is evaluated at the start
+// of the next line search (need_e0), since lq was not the accepted trial.
+__device__ void quad_finish(CGState& s, LambdaSet& L, double lq) {
+    const double lam = (lq <= 0.0 || lq <= kLambdaTol) ? 0.0 : lq;
+    s.q_phase = 0;
+    s.ls_active = 0;
+    s.last_backtracks = s.backtracks;
+    L.K = 0;
+    s.total_energy = lam > 0 ? s.q_ebt : s.E_cur;
+    if (lam == 0.0) {
+        line_search_failed(s);
+        return;
+    }
+    s.lam_move = lam;
+    s.E_new = s.q_ebt;
+    s.move_kind = 1;
+    s.skip_force = 0;
+    s.q_used = 1;
+}
+
+// One model of quadraticoptimization (CGMethod.hpp:662-714): the parabola
+// through (x0,y0), (x1,y1), (x2,y2) and its vertex lq; either the search ends
+// or the next pass evaluates E(x + lq*d). The reference's loop has no bound;
+// after kQuadMaxModels models it returns x1 here.
+__device__ void quad_model(CGState& s, LambdaSet& L) {
+    if (s.q_iter >= kQuadMaxModels) {
+        quad_finish(s, L, s.q_x1);
+        return;
+    }
+    s.q_iter++;
+    const double x0 = s.q_x0, x1 = s.q_x1, x2 = s.q_x2, y0 = s.q_y0, y1 = s.q_y1, y2 = s.q_y2;
+    const double d = __dmul_rn(__dmul_rn(__dsub_rn(x0, x1), __dsub_rn(x0, x2)), __dsub_rn(x1, x2));
+    const double a = __dadd_rn(__dsub_rn(__dmul_rn(y0, __dsub_rn(x1, x2)), __dmul_rn(y1, __dsub_rn(x0, x2))),
+                               __dmul_rn(y2, __dsub_rn(x0, x1)));
+    const double t0 = __dmul_rn(__dmul_rn(y0, __dadd_rn(x1, x2)), __dsub_rn(x1, x2));
+    const double t1 = __dmul_rn(__dmul_rn(y1, __dadd_rn(x0, x2)), __dsub_rn(x0, x2));
+    const double t2 = __dmul_rn(__dmul_rn(y2, __dadd_rn(x0, x1)), __dsub_rn(x0, x1));
+    const double b = -__dadd_rn(__dsub_rn(t0, t1), t2);
+    const double lq = -b / __dmul_rn(2.0, a);
+    if (fabs(__dsub_rn(lq, x1)) / x1 < kLambdaQuadTol) {  // lambda converged
+        quad_finish(s, L, lq);
+        return;
+    }
+    if (a / d < 0) {  // no minimum: the backtracking lambda
+        quad_finish(s, L, s.q_bt);
+        return;
+    }
+    s.q_lq = lq;
+    L.K = 1;
+    L.lam[0] = lq;
+    s.k_trials = 1;
+}
+
+// Energy at the pending quadratic point (CGMethod.hpp:716-763): accept, or
+// replace one of the three points and build the next model.
+__device__ void quad_eval(CGState& s, LambdaSet& L, double eq) {
+    s.num_energy_call++;
+    const double lq = s.q_lq, x1 = s.q_x1, y1 = s.q_y1;
+    if (fabs(__dsub_rn(eq, y1)) / y1 < kLambdaQuadTol) {
+        quad_finish(s, L, lq);
+        return;
+    }
+    if (lq < x1) {
+        if (eq < s.q_y0 && eq < y1) {
+            s.q_x1 = lq;
+            s.q_y1 = eq;
+        } else {
+            s.q_x0 = lq;
+            s.q_y0 = eq;
+        }
+    } else if (x1 < lq) {
+        if (eq < y1 && eq < s.q_y2) {
+            s.q_x1 = lq;
+            s.q_y1 = eq;
+        } else {
+            s.q_x2 = lq;
+            s.q_y2 = eq;
+        }
+    } else {  // "Lambda out of range": the previous model's x1
+        quad_finish(s, L, x1);
+        return;
+    }
+    quad_model(s, L);
+}
+
 // After an energy pass: the reference's backtracking loop over the evaluated
-// trial lambdas (CGMethod.hpp:264-362).
+// trial lambdas (CGMethod.hpp:264-362), or the backtracking phase of
+// quadraticLineSearchV2 (:564-629) with its trial history, or one
+// quadratic-optimization point.
 __device__ void ls_decide(CGState& s, LambdaSet& Lr, const double* __restrict__ out) {
     LambdaSet* L = &Lr;
     s.reset_after_dir = 0;
@@ -139,6 +234,10 @@ __device__ void ls_decide(CGState& s, LambdaSet& Lr, const double* __restrict__ 
         s.need_e0 = 0;
         slot = 1;
     }
+    if (s.q_phase) {
+        quad_eval(s, *L, out[kOut - 1]);
+        return;
+    }
     if (s.ls_first_pass) {
         s.num_energy_call++;  // currentEnergy = energyFunc(coord)
         s.ls_first_pass = 0;
@@ -147,15 +246,26 @@ __device__ void ls_decide(CGState& s, LambdaSet& Lr, const double* __restrict__ 
         double lam = L->lam[slot];
         double E_lam = out[slot * kOut + kOut - 1];
         s.num_energy_call++;
-        const double ideal = -s.reduced_slope * lam;
+        // idealEnergyChange: -(slope*d.F)*lambda (backtracking), -slope*lambda*d.F (V2)
+        const double ideal = s.q_mode ? (-kBacktrackSlope * lam) * s.slope : -s.reduced_slope * lam;
         bool decided = false;
-        if (lam < 0 || ideal > 0) {
+        if (lam < 0 || ideal > 0) {  // V2 exits the program here; both end with lambda = 0
             decided = true;
             lam = 0.0;
         }
         const double dE = E_lam - s.E_cur;
         if (dE <= ideal) decided = true;
-        else lam *= 0.5;
+        else {
+            if (s.q_mode) {  // lambdavec/energyvec: the first trial, and the failed ones after it
+                if (s.backtracks == 0) {
+                    s.q_x2 = lam;
+                    s.q_y2 = E_lam;
+                } else if (E_lam > s.q_maxe) {
+                    s.q_maxe = E_lam;
+                }
+            }
+            lam *= 0.5;
+        }
         if (lam <= 0.0 || lam <= kLambdaTol) {
             decided = true;
             lam = 0.0;
@@ -168,6 +278,18 @@ __device__ void ls_decide(CGState& s, LambdaSet& Lr, const double* __restrict__ 
             L->K = 0;
             if (lam == 0.0) {
                 line_search_failed(s);
+            } else if (s.q_mode && s.backtracks > 0 && E_lam < s.E_cur && s.q_maxe > E_lam) {
+                // quadratic optimization through (0, E0), (lambda, E), (first lambda, its E)
+                s.ls_active = 1;
+                s.q_phase = 1;
+                s.q_iter = 0;
+                s.q_x0 = 0.0;
+                s.q_y0 = s.E_cur;
+                s.q_x1 = lam;
+                s.q_y1 = E_lam;
+                s.q_bt = lam;
+                s.q_ebt = E_lam;
+                quad_model(s, *L);
             } else {
                 s.lam_move = lam;
                 s.E_new = E_lam;
@@ -253,7 +375,8 @@ __device__ void dots_tail(CGState& s, double a, double b, double m) {
         s.energy_rel_change = fabs(s.E_new - s.prev_energy) / fabs(s.prev_energy);
         s.prev_energy = s.E_new;
         s.E_cur = s.E_new;
-        s.need_e0 = 0;
+        s.need_e0 = s.q_used;  // a quadratic step moved to a point whose energy is not known
+        s.q_used = 0;
         if (s.method == MEDYAN_CG_POLAK_RIBIERE) s.beta = dmax_ref(0.0, (s.new_grad - s.prev_grad) / s.last_fdotf);
         else if (s.method == MEDYAN_CG_FLETCHER_RIEVES) s.beta = s.new_grad / s.last_fdotf;
         else s.beta = 0.0;
@@ -759,7 +882,9 @@ namespace mb {
 // host synchronization; cg_collect reads the results.
 medyan_status cg_enqueue(medyan_mech* h, const medyan_cg_params* p, const double* coord_in) {
     if (!h || !p || !coord_in) return MEDYAN_ERR_INVALID_ARG;
-    if (p->method < 0 || p->method > 2 || !(p->max_dist > 0) || !(p->lambda_max > 0)) return MEDYAN_ERR_INVALID_ARG;
+    if (p->method < 0 || p->method > 2 || !(p->max_dist > 0) || !(p->lambda_max > 0) || p->line_search < 0 ||
+        p->line_search > 1)
+        return MEDYAN_ERR_INVALID_ARG;
     const int n3 = 3 * h->n_beads;
     cudaStream_t s = h->stream;
     cudaError_t e = h->cg_dir.reserve(n3 ? n3 : 1);
@@ -795,6 +920,7 @@ medyan_status cg_enqueue(medyan_mech* h, const medyan_cg_params* p, const double
     s0.lambda_max = p->lambda_max;
     s0.grad_tol = p->grad_tol;
     s0.energy_rel_tol = p->energy_rel_tol;
+    s0.ls_quad = p->line_search;
     s0.status = MEDYAN_OK;
     s0.parity = 1;  // the first force lands in f0
     s0.grad_inf_norm = __builtin_inf();
@@ -990,7 +1116,8 @@ cudaError_t b_build_graph(PackedBatch& pb, int prec, cudaGraphExec_t* exec) {
 // Batched CGMethod::minimize over the packed replicas; see the kernels above.
 medyan_status cg_batch_run(PackedBatch& pb, int prec, const medyan_cg_params* p) {
     const int R = pb.R;
-    if (!p || p->method < 0 || p->method > 2 || !(p->max_dist > 0) || !(p->lambda_max > 0))
+    if (!p || p->method < 0 || p->method > 2 || !(p->max_dist > 0) || !(p->lambda_max > 0) || p->line_search < 0 ||
+        p->line_search > 1)
         return MEDYAN_ERR_INVALID_ARG;
     if (R == 0) return MEDYAN_OK;
     const size_t n3 = 3 * (size_t)pb.nb;
@@ -1022,6 +1149,7 @@ medyan_status cg_batch_run(PackedBatch& pb, int prec, const medyan_cg_params* p)
         c.lambda_max = p->lambda_max;
         c.grad_tol = p->grad_tol;
         c.energy_rel_tol = p->energy_rel_tol;
+        c.ls_quad = p->line_search;
         c.status = MEDYAN_OK;
         c.parity = 1;
         c.grad_inf_norm = __builtin_inf();

@@ -96,6 +96,18 @@ struct CGState {
     double lam_move;       // step taken by the pending force pass
     double dmax;           // max |d_i| of the current search direction
     double min_e;
+    // quadratic line search (lineSearchAlgorithm QUADRATIC)
+    int ls_quad;           // parameter: 1 = quadraticLineSearchV2 outside safe mode
+    int q_mode;            // the current line search is quadraticLineSearchV2
+    int q_phase;           // quadratic-optimization passes in progress
+    int q_iter;            // quadratic models built in this line search
+    int q_used;            // the pending step came from a quadratic optimization
+    int q_pad;
+    double q_x0, q_x1, q_x2, q_y0, q_y1, q_y2;  // model points (lambda, energy)
+    double q_bt;           // backtracking lambda (returned when the model has no minimum)
+    double q_ebt;          // its energy (TotalEnergy and newEnergy of the search)
+    double q_maxe;         // largest energy of a failed trial after the first
+    double q_lq;           // lambda of the pending quadratic pass
 };
 
 }  // namespace mb

@@ -39,9 +39,11 @@ class EnergyReport:
 
 def conjugate_gradient_params(method: int = 2, max_dist: float = 1.0, lambda_max: float = 0.01,
                               grad_tol: float = 1.0, energy_rel_tol: float = 1e-9, energy_call_limit: int = 0,
-                              force_call_limit: int = 10000, try_to_recover: bool = True) -> CGParams:
+                              force_call_limit: int = 10000, try_to_recover: bool = True,
+                              line_search: str = "BACKTRACKING") -> CGParams:
     """ConjugateGradientParams (CGMethod.hpp:44-63); defaults are the
-    reference example's MAXDISTANCE/LAMBDAMAX and MechParams' tolerances."""
+    reference example's MAXDISTANCE/LAMBDAMAX and MechParams' tolerances.
+    line_search: "BACKTRACKING" or "QUADRATIC" (quadraticLineSearchV2)."""
     p = CGParams()
     p.method = method
     p.max_dist = max_dist
@@ -51,6 +53,7 @@ def conjugate_gradient_params(method: int = 2, max_dist: float = 1.0, lambda_max
     p.energy_call_limit = energy_call_limit
     p.force_call_limit = force_call_limit
     p.try_to_recover = 1 if try_to_recover else 0
+    p.line_search = {"BACKTRACKING": 0, "QUADRATIC": 1}[line_search]
     return p
 
 

@@ -1011,6 +1011,101 @@ static double cg_backtrack(CGState* st, const double* x, double maxDist, double 
     return lambda;
 }
 
+/* CGMethod::quadraticoptimization, CGMethod.hpp:644-765: iterated quadratic
+   model through (x0,y0), (x1,y1), (x2,y2). The reference loops until one of
+   its exits; the loop here stops after 100 models and returns x1. */
+static double cg_quad_opt(CGState* st, const double* x, int* nEnergy, double x0, double x1, double x2, double y0,
+                          double y1, double y2) {
+    const double btlambda = x1;
+    for (int it = 0; it < 100; ++it) {
+        const double d = (x0 - x1) * (x0 - x2) * (x1 - x2);
+        const double a = y0 * (x1 - x2) - y1 * (x0 - x2) + y2 * (x0 - x1);
+        const double b = -(y0 * (x1 + x2) * (x1 - x2) - y1 * (x0 + x2) * (x0 - x2) + y2 * (x0 + x1) * (x0 - x1));
+        const double lq = -b / (2 * a);
+        if (fabs(lq - x1) / x1 < 1e-3) return lq;  /* LAMBDAQUADTOL */
+        if (a / d < 0) return btlambda;           /* no minimum: the backtracking lambda */
+        for (int i = 0; i < st->ndof; ++i) st->coordLS[i] = x[i] + lq * st->searchDir[i];
+        const double eq = st->efn(st->ctx, st->coordLS);
+        ++*nEnergy;
+        if (fabs(eq - y1) / y1 < 1e-3) return lq;
+        if (lq < x1) {
+            if (eq < y0 && eq < y1) { x1 = lq; y1 = eq; }
+            else { x0 = lq; y0 = eq; }
+        } else if (x1 < lq) {
+            if (eq < y1 && eq < y2) { x1 = lq; y1 = eq; }
+            else { x2 = lq; y2 = eq; }
+        } else {
+            return x1;
+        }
+    }
+    return x1;
+}
+
+/* CGMethod::quadraticLineSearchV2, CGMethod.hpp:521-640: backtracking with
+   the Armijo slope 0.4, then, when at least one halving happened and a later
+   trial's energy was above the accepted one, quadratic optimization through
+   (0, E0), (lambda, E(lambda)) and (first lambda, its energy). The reference
+   exits the program when the ideal energy change is positive; that ends the
+   search with lambda = 0 here. */
+static double cg_quadratic(CGState* st, const double* x, double maxDist, double maxForce, double lambdaMax,
+                           int* nEnergy, double* newEnergy) {
+    *newEnergy = 0;
+    if (maxForce == 0.0) return 0.0;
+    double lambda = lambdaMax < maxDist / maxForce ? lambdaMax : maxDist / maxForce;
+    const double currentEnergy = st->efn(st->ctx, x);
+    ++*nEnergy;
+    const double slope = cg_dot(st->searchDir, st->force, st->ndof);
+    double energyLambda = 0.0, prevEnergy = 0.0, prevLambda = 0.0;
+    double lv[64], ev[64];
+    int nv = 0, iter = 0, done = 0;
+    while (!done) {
+        iter++;
+        for (int i = 0; i < st->ndof; ++i) st->coordLS[i] = x[i] + lambda * st->searchDir[i];
+        energyLambda = st->efn(st->ctx, st->coordLS);
+        ++*nEnergy;
+        const double ideal = -0.4 * lambda * slope;
+        if (ideal > 0) {
+            lambda = 0.0;
+            done = 1;
+            break;
+        }
+        if (energyLambda - currentEnergy <= ideal) done = 1;
+        else {
+            prevLambda = lambda;
+            prevEnergy = energyLambda;
+            lambda *= 0.5;
+        }
+        if (nv < 64) {
+            if (lambda <= 0.0 || lambda <= 1e-8) {
+                lv[nv] = 0.0;
+                ev[nv++] = currentEnergy;
+            } else if (done) {
+                lv[nv] = lambda;
+                ev[nv++] = energyLambda;
+            } else {
+                lv[nv] = prevLambda;
+                ev[nv++] = prevEnergy;
+            }
+        }
+        if (lambda <= 0.0 || lambda <= 1e-8) {
+            done = 1;
+            lambda = 0.0;
+        }
+    }
+    if (lambda > 0.0 && iter > 1 && energyLambda < currentEnergy) {
+        int quad = 0, i;
+        for (i = nv - 1; i >= 1; i--)
+            if (energyLambda < ev[i]) quad = 1;
+        if (quad) {
+            const double lq = cg_quad_opt(st, x, nEnergy, 0.0, lambda, lv[i], currentEnergy, energyLambda, ev[i]);
+            lambda = (lq <= 0.0 || lq <= 1e-8) ? 0.0 : lq;
+        }
+    }
+    st->TotalEnergy = lambda > 0 ? energyLambda : currentEnergy;
+    *newEnergy = energyLambda;
+    return lambda;
+}
+
 static double sys_energy(void* ctx, const double* x) { return oracle_energy((const medyan_system*)ctx, x, NULL); }
 static void sys_forces(void* ctx, const double* x, double* f) { oracle_forces((const medyan_system*)ctx, x, f); }
 static void sys_individual(void* ctx, const double* x, double* per) { oracle_energy((const medyan_system*)ctx, x, per); }
@@ -1082,8 +1177,11 @@ int32_t oracle_cg_minimize_cb(int32_t ndof, int32_t n_beads, const medyan_cg_par
         double beta = 0, newGrad = 0, prevGrad = 0, newEnergy = 0;
         numIter++;
         int nE = 0;
-        double lambda = cg_backtrack(&st, x, p->max_dist, r.grad_inf_norm, p->lambda_max, safeMode ? 0 : 0.4, &nE,
-                                     &newEnergy);
+        /* QUADRATIC uses quadraticLineSearchV2 except in safe mode (CGMethod.hpp:1319-1332) */
+        double lambda = (p->line_search && !safeMode)
+                            ? cg_quadratic(&st, x, p->max_dist, r.grad_inf_norm, p->lambda_max, &nE, &newEnergy)
+                            : cg_backtrack(&st, x, p->max_dist, r.grad_inf_norm, p->lambda_max, safeMode ? 0 : 0.4,
+                                           &nE, &newEnergy);
         r.num_energy_call += nE;
         if (lambda == 0) {
             if (p->try_to_recover) {

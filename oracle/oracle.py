@@ -172,8 +172,9 @@ class Reference:
 
 
 def cg_params(method=2, max_dist=1.0, lambda_max=0.01, grad_tol=1.0, energy_rel_tol=1e-9, energy_call_limit=0,
-              force_call_limit=10000, try_to_recover=1) -> CGParams:
+              force_call_limit=10000, try_to_recover=1, line_search=0) -> CGParams:
     p = CGParams()
+    p.line_search = line_search
     p.method = method
     p.max_dist = max_dist
     p.lambda_max = lambda_max

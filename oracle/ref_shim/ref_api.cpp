@@ -200,6 +200,7 @@ int medyan_ref_cg_minimize(const medyan_system* sys, const medyan_cg_params* p, 
     cg.energyCallLimit = p->energy_call_limit;
     cg.forceCallLimit = p->force_call_limit;
     cg.tryToRecoverInLineSearchError = p->try_to_recover != 0;
+    cg.lineSearchAlgorithm = p->line_search ? "QUADRATIC" : "BACKTRACKING";
     cg.reportOnCallLimit = true;
 
     const auto energyFunc = [&](floatingpoint* c) {
@@ -234,7 +235,8 @@ int medyan_ref_cg_minimize(const medyan_system* sys, const medyan_cg_params* p, 
         return MEDYAN_ERR_NONFINITE;
     }
     std::copy(coord.begin(), coord.begin() + ndof, coord_io);
-    if (force_out) std::copy(force.begin(), force.begin() + ndof, force_out);
+    // a failed line search returns before minimize fills outForce
+    if (force_out && (int)force.size() >= ndof) std::copy(force.begin(), force.begin() + ndof, force_out);
     if (out) {
         fill_report(res.energiesBefore, out->energy_before, &out->energy_before_total);
         fill_report(res.energiesAfter, out->energy_after, &out->energy_after_total);
@@ -276,6 +278,7 @@ int medyan_ref_cg_minimize_cb(int ndof, int n_beads, const medyan_cg_params* p, 
     cg.energyCallLimit = p->energy_call_limit;
     cg.forceCallLimit = p->force_call_limit;
     cg.tryToRecoverInLineSearchError = p->try_to_recover != 0;
+    cg.lineSearchAlgorithm = p->line_search ? "QUADRATIC" : "BACKTRACKING";
     const auto energyFunc = [&](floatingpoint* c) { return efn(ctx, c); };
     const auto forceFunc = [&](floatingpoint* c, floatingpoint* f, int) { ffn(ctx, c, f); };
     const auto energyFuncIndividual = [&](floatingpoint* c) {
@@ -304,7 +307,8 @@ int medyan_ref_cg_minimize_cb(int ndof, int n_beads, const medyan_cg_params* p, 
         return MEDYAN_ERR_NONFINITE;
     }
     std::copy(coord.begin(), coord.begin() + ndof, coord_io);
-    if (force_out) std::copy(force.begin(), force.begin() + ndof, force_out);
+    // a failed line search returns before minimize fills outForce
+    if (force_out && (int)force.size() >= ndof) std::copy(force.begin(), force.begin() + ndof, force_out);
     if (out) {
         fill_report(res.energiesBefore, out->energy_before, &out->energy_before_total);
         fill_report(res.energiesAfter, out->energy_after, &out->energy_after_total);

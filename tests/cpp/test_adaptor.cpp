@@ -268,9 +268,9 @@ int run_gpu() {
     CHECK(rel(r.energiesAfter.total, ro.energy_after_total) <= 1e-10);
     CHECK((int)fout.size() == nd);
 
-    // an unsupported line search is refused, not approximated
+    // an unsupported option is refused, not approximated
     ConjugateGradientParams q = p;
-    q.lineSearchAlgorithm = "QUADRATIC";
+    q.lambdaRunningAverageProbability = 0.5;
     threw = false;
     try {
         CGMethod::minimize(q, xg, ffm2);

@@ -22,10 +22,13 @@ def replicas(oracle, n=6, seed=5, cyl_range=(200, 800)):
     return out
 
 
+@pytest.mark.parametrize("line_search", ["BACKTRACKING", "QUADRATIC"])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_batch_matches_single(gpu_lib, oracle, precision):
+def test_batch_matches_single(gpu_lib, oracle, precision, line_search):
     reps = replicas(oracle)
-    p = cgp(grad_tol=1e-4, energy_rel_tol=1e-14, energy_call_limit=40)
+    p = cgp(grad_tol=1e-4, energy_rel_tol=1e-14, energy_call_limit=40, line_search=line_search)
+    # the quadratic model's vertex divides energy differences: rounding grows there
+    tol = 1e-7 if line_search == "BACKTRACKING" else 1e-6
     with BatchMinimizer([sv for sv, _ in reps], precision) as b:
         st, xs, fs, rs = b.minimize([x for _, x in reps], p)
     for r, (sv, x) in enumerate(reps):
@@ -37,12 +40,12 @@ def test_batch_matches_single(gpu_lib, oracle, precision):
         # accumulate with atomics, so equal to rounding, not bit for bit)
         assert (rs[r].num_energy_call, rs[r].num_force_call, rs[r].num_iter) == \
             (r1.num_energy_call, r1.num_force_call, r1.num_iter)
-        assert np.abs(xs[r] - x1).max() <= 1e-7
-        assert np.abs(fs[r] - f1).max() <= 1e-7 * np.abs(f1).max()
+        assert np.abs(xs[r] - x1).max() <= tol
+        assert np.abs(fs[r] - f1).max() <= tol * np.abs(f1).max()
         if precision == "fp64":
             so, xo, fo, ro = oracle.minimize(sv, x, p)
             assert (rs[r].num_energy_call, rs[r].num_iter) == (ro.num_energy_call, ro.num_iter)
-            assert np.abs(xs[r] - xo).max() <= 1e-7
+            assert np.abs(xs[r] - xo).max() <= tol
 
 
 def test_batch_converges_each_replica(gpu_lib, oracle):

@@ -64,6 +64,38 @@ def test_converges_like_oracle(gpu_lib, oracle):
     assert 0.5 * ro.num_iter <= rg.num_iter <= 2 * ro.num_iter
 
 
+@pytest.mark.parametrize("method", [0, 2])
+def test_quadratic_short_run_matches_oracle(gpu_lib, oracle, method):
+    """lineSearchAlgorithm QUADRATIC: quadraticLineSearchV2's backtracking
+    phase, its trial history and the quadratic-optimization passes."""
+    sv, x = small_net(oracle)
+    kw = dict(method=method, grad_tol=1e-4, energy_rel_tol=1e-14, energy_call_limit=40)
+    p = cgp(line_search="QUADRATIC", **kw)
+    so, xo, fo, ro = oracle.minimize(sv, x, p)
+    # this run takes quadratic steps: it leaves the backtracking trajectory
+    _, xb, _, _ = oracle.minimize(sv, x, cgp(**kw))
+    assert np.abs(xb - xo).max() > 1e-3
+    sg, xg, fg, rg = gpu_min(sv, x, p)
+    assert sg == so == 0
+    assert (rg.num_energy_call, rg.num_force_call, rg.num_iter) == (ro.num_energy_call, ro.num_force_call, ro.num_iter)
+    # the model's vertex -b/2a divides differences of energies that agree to
+    # 1e-12 relative: coordinates agree to 1e-6 nm rather than 1e-7
+    errs = (np.abs(xg - xo).max(), abs(rg.energy_after_total - ro.energy_after_total) / abs(ro.energy_after_total),
+            np.abs(fg - fo).max() / np.abs(fo).max())
+    assert errs[0] <= 1e-6 and errs[1] <= 1e-9 and errs[2] <= 1e-6, errs
+
+
+def test_quadratic_converges_like_oracle(gpu_lib, oracle):
+    sv, x = small_net(oracle)
+    p = cgp(grad_tol=1.0, line_search="QUADRATIC")
+    so, xo, fo, ro = oracle.minimize(sv, x, p)
+    sg, xg, fg, rg = gpu_min(sv, x, p)
+    assert sg == so == 0
+    assert rg.grad_inf_norm < 1.0 or rg.energy_rel_change < 1e-9
+    assert abs(rg.energy_after_total - ro.energy_after_total) <= 1e-2 * abs(ro.energy_after_total)
+    assert 0.5 * ro.num_iter <= rg.num_iter <= 2 * ro.num_iter
+
+
 def frustrated_triangles(n=200, seed=0):
     # spring triangles with incompatible rest lengths (10, 10, 25): a unique
     # minimum (up to rigid motion) with nonzero energy
@@ -116,10 +148,11 @@ def degenerate_system():
     return sv, x
 
 
+@pytest.mark.parametrize("line_search", ["BACKTRACKING", "QUADRATIC"])
 @pytest.mark.parametrize("recover", [0, 1])
-def test_line_search_failure_paths(gpu_lib, oracle, recover):
+def test_line_search_failure_paths(gpu_lib, oracle, recover, line_search):
     sv, x = degenerate_system()
-    p = cgp(grad_tol=1e-3, try_to_recover=bool(recover))
+    p = cgp(grad_tol=1e-3, try_to_recover=bool(recover), line_search=line_search)
     so, xo, fo, ro = oracle.minimize(sv, x, p)
     sg, xg, fg, rg = gpu_min(sv, x, p)
     assert sg == so
@@ -134,3 +167,7 @@ def test_rejects_bad_params(gpu_lib, oracle):
     sv, x = small_net(oracle)
     with pytest.raises(MedyanError):
         gpu_min(sv, x, cgp(method=5))
+    p = cgp()
+    p.line_search = 2
+    with pytest.raises(MedyanError):
+        gpu_min(sv, x, p)

@@ -174,18 +174,22 @@ def run_cb(lib, fname, n, params, x0, cbs):
     return st, x, f, r
 
 
+@pytest.mark.parametrize("line_search", [0, 1])
 @pytest.mark.parametrize("method", [0, 1, 2])
-def test_cg_harmonic(oracle, unit, method):
+def test_cg_harmonic(oracle, unit, method, line_search):
     cg = unit["cg_harmonic"]
     p = cg_params(method=method, grad_tol=cg["params"]["gradTol"], max_dist=cg["params"]["maxDist"],
-                  lambda_max=cg["params"]["lambdaMax"], try_to_recover=0)
+                  lambda_max=cg["params"]["lambdaMax"], try_to_recover=0, line_search=line_search)
     cbs = harmonic_callbacks(cg["opt"], cg["weight"])
     strict = Reference(strict=True) if Reference.available(strict=True) else None
     for init in cg["inits"]:
         st, x, f, r = run_cb(oracle.lib, "oracle_cg_minimize_cb", cg["n"], p, init, cbs)
         assert st == 0 and r.error_flags == 0
         assert np.all(np.abs(f) <= cg["params"]["gradTol"])
-        if strict is not None:
+        # QUADRATIC: the reference's quadraticLineSearchV2 evaluates each trial
+        # at a stale coordLineSearch (test_quadratic_reference_defect); the
+        # oracle restates the algorithm as written and is checked alone
+        if strict is not None and line_search == 0:
             st2, x2, f2, r2 = run_cb(strict.lib, "medyan_ref_cg_minimize_cb", cg["n"], p, init, cbs)
             assert st2 == st and np.array_equal(x, x2) and np.array_equal(f, f2)
             assert (r.num_energy_call, r.num_force_call) == (r2.num_energy_call, r2.num_force_call)
@@ -201,3 +205,37 @@ def test_cg_trajectory_bitwise_vs_strict_reference(oracle, nets):
     assert np.array_equal(xo, xr) and np.array_equal(fo, fr)
     assert (ro.num_energy_call, ro.num_force_call) == (rr.num_energy_call, rr.num_force_call)
     assert ro.energy_after_total == rr.energy_after_total
+
+
+def test_quadratic_line_search_converges(oracle, nets):
+    """QUADRATIC (quadraticLineSearchV2 + quadraticoptimization, CGMethod.hpp:521-765)
+    as written: every accepted step lowers the energy and the run converges."""
+    sv, x = network_system(nets, "cfg0")
+    e0, _ = oracle.energy(sv, x)
+    st, xo, fo, ro = oracle.minimize(sv, x, cg_params(grad_tol=1.0, line_search=1))
+    assert st == 0 and ro.error_flags == 0
+    assert np.abs(fo).max() < 1.0
+    # the soft network stops at gradTol = 1 pN on a plateau: the backtracking
+    # run from the same start ends within a few percent of the same energy
+    st_b, xb, _, rb = oracle.minimize(sv, x, cg_params(grad_tol=1.0))
+    assert st_b == 0 and ro.energy_after_total < 0.6 * e0
+    assert abs(ro.energy_after_total - rb.energy_after_total) <= 0.05 * abs(rb.energy_after_total)
+
+
+@pytest.mark.skipif(not Reference.available(strict=True), reason="reference build not present")
+def test_quadratic_reference_defect(oracle, unit):
+    """The reference's quadraticLineSearchV2 calls moveAlongSearchDir(coord, lambda)
+    (coord += lambda*d, in place) and then energyFunc(coordLineSearch), a buffer
+    it never fills: every trial sees the same stale energy, the Armijo test
+    cannot pass, and the first line search returns lambda = 0 after moving
+    coord by the sum of the trial steps. Pinned here on the harmonic problem
+    of TestCGMethod.cpp so the difference from the oracle stays documented."""
+    cg = unit["cg_harmonic"]
+    p = cg_params(method=2, grad_tol=cg["params"]["gradTol"], max_dist=cg["params"]["maxDist"],
+                  lambda_max=cg["params"]["lambdaMax"], try_to_recover=0, line_search=1)
+    cbs = harmonic_callbacks(cg["opt"], cg["weight"])
+    init = cg["inits"][0]
+    st, x, f, r = run_cb(oracle.lib, "oracle_cg_minimize_cb", cg["n"], p, init, cbs)
+    st2, x2, f2, r2 = run_cb(Reference(strict=True).lib, "medyan_ref_cg_minimize_cb", cg["n"], p, init, cbs)
+    assert st == 0 and r.error_flags == 0
+    assert r2.error_flags & 1  # errorLineSearch
