@@ -240,7 +240,8 @@ def run_ours(args, rank: int, world: int) -> dict:
                    "step": "total energy + forces of all force fields", "parallelism": f"replicas x{world}"},
         "e2e": {"value": world * K / e2e_t, "unit": "force-evals/s", "h2d_bytes_per_step": 8 * x.size,
                 "d2h_bytes_per_step": 8 * x.size + 8 * 11},
-        "gpu_launches": K * 8,  # chain, bonded, excluded-volume, fallback (forces); chain, bonded, excluded-volume, finish (energy)
+        # kernel nodes of the energy and force pass graphs the timed steps launch
+        "gpu_launches": K * (L.medyan_mech_pass_kernel_count(h, 0) + L.medyan_mech_pass_kernel_count(h, 1)),
         "clocks": clocks.summary(),
         "wall_s_timed_region": wall,
         "accuracy_vs_fp64": {"rel_force_err": rel_force_err, "rel_energy_err": rel_energy_err},

@@ -201,6 +201,12 @@ medyan_status medyan_mech_enqueue_forces(medyan_mech* h);
 medyan_status medyan_mech_synchronize(medyan_mech* h);
 /* The handle's cudaStream_t, for event timing or stream ordering. */
 void* medyan_mech_stream(medyan_mech* h);
+/* Kernel launches in one standalone pass (which: 0 energy, 1 forces, 2 both)
+   as the handle builds it for its current force fields (the kernel nodes of
+   the pass graph; empty force-field groups launch nothing). Builds the pass
+   graph if needed; -1 on error. A diagnostic with no counterpart in the
+   reference. */
+int32_t medyan_mech_pass_kernel_count(medyan_mech* h, int32_t which);
 /* Device pointers of the coordinate and force arrays (double[3*n_beads]) and
    of the energy output (double[MEDYAN_FF_COUNT + 1]: per force field, then total).
    The device arrays hold the beads in the library's internal order (filament

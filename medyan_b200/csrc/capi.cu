@@ -302,24 +302,47 @@ cudaError_t coords_to_host(medyan_mech* h, const double* dev, double* host, cuda
     return e;
 }
 
-cudaError_t launch_pass(medyan_mech* h, int which) {
-    if (!h->pass_graph[which] || h->pass_graph_gen[which] != h->ff_gen) {
-        if (h->pass_graph[which]) cudaGraphExecDestroy(h->pass_graph[which]);
-        h->pass_graph[which] = nullptr;
-        cudaError_t e = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal);
-        if (e != cudaSuccess) return e;
-        if (which != kPassForces) enqueue_energy(h, h->x.raw(), nullptr, h->lam_zero.raw(), h->stream);
-        if (which != kPassEnergy) enqueue_forces(h, h->x.raw(), h->f.raw(), h->stream);
-        cudaGraph_t g = nullptr;
-        e = cudaStreamEndCapture(h->stream, &g);
-        if (e == cudaSuccess) e = cudaGraphInstantiate(&h->pass_graph[which], g, 0);
-        if (g) cudaGraphDestroy(g);
-        if (e != cudaSuccess) {
-            h->pass_graph[which] = nullptr;
-            return e;
-        }
-        h->pass_graph_gen[which] = h->ff_gen;
+static cudaError_t count_kernel_nodes(cudaGraph_t g, int* out) {
+    size_t n = 0;
+    cudaError_t e = cudaGraphGetNodes(g, nullptr, &n);
+    if (e != cudaSuccess) return e;
+    std::vector<cudaGraphNode_t> nodes(n);
+    if (n) e = cudaGraphGetNodes(g, nodes.data(), &n);
+    int k = 0;
+    for (size_t i = 0; i < n && e == cudaSuccess; ++i) {
+        cudaGraphNodeType t;
+        e = cudaGraphNodeGetType(nodes[i], &t);
+        if (e == cudaSuccess && t == cudaGraphNodeTypeKernel) ++k;
     }
+    *out = k;
+    return e;
+}
+
+// Captures and instantiates pass `which` when the force fields changed.
+cudaError_t ensure_pass_graph(medyan_mech* h, int which) {
+    if (h->pass_graph[which] && h->pass_graph_gen[which] == h->ff_gen) return cudaSuccess;
+    if (h->pass_graph[which]) cudaGraphExecDestroy(h->pass_graph[which]);
+    h->pass_graph[which] = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return e;
+    if (which != kPassForces) enqueue_energy(h, h->x.raw(), nullptr, h->lam_zero.raw(), h->stream);
+    if (which != kPassEnergy) enqueue_forces(h, h->x.raw(), h->f.raw(), h->stream);
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(h->stream, &g);
+    if (e == cudaSuccess) e = count_kernel_nodes(g, &h->pass_kernels[which]);
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&h->pass_graph[which], g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        h->pass_graph[which] = nullptr;
+        return e;
+    }
+    h->pass_graph_gen[which] = h->ff_gen;
+    return cudaSuccess;
+}
+
+cudaError_t launch_pass(medyan_mech* h, int which) {
+    cudaError_t e = ensure_pass_graph(h, which);
+    if (e != cudaSuccess) return e;
     return cudaGraphLaunch(h->pass_graph[which], h->stream);
 }
 
@@ -507,6 +530,13 @@ medyan_status medyan_mech_synchronize(medyan_mech* h) {
 }
 
 void* medyan_mech_stream(medyan_mech* h) { return h ? (void*)h->stream : nullptr; }
+
+int32_t medyan_mech_pass_kernel_count(medyan_mech* h, int32_t which) {
+    if (!h || which < 0 || which > 2) return -1;
+    if (cudaSetDevice(h->device) != cudaSuccess) return -1;
+    if (ensure_pass_graph(h, which) != cudaSuccess) return -1;
+    return h->pass_kernels[which];
+}
 
 medyan_status medyan_mech_device_buffers(medyan_mech* h, double** coord, double** force, double** energy) {
     if (!h) return MEDYAN_ERR_INVALID_ARG;

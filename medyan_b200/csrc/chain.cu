@@ -108,15 +108,16 @@ __global__ void __launch_bounds__(kThreads) k_chain_forces(const ChainDev ch, co
 }
 
 // Energies. Each warp owns 32 consecutive positions and each lane the link
-// and bend of its own position, at up to kMaxLambda step sizes from one read
-// of x and d. A fixed grid (grid-stride over warp tiles) keeps the per-block
-// partial sums deterministic.
-template <class R>
-__global__ void __launch_bounds__(kThreads) k_chain_energy(const ChainDev ch, const double* __restrict__ x,
-                                                           const double* __restrict__ d,
-                                                           const LambdaSet* __restrict__ lset,
-                                                           double* __restrict__ partial, int nblk_total, int blk_off,
-                                                           const int4* __restrict__ table) {
+// and bend of its own position, at up to KMAX step sizes from one read of x
+// and d (MOVE), or at x itself (a plain pass: one evaluation, copied to every
+// requested slot). A fixed grid (grid-stride over warp tiles) keeps the
+// per-block partial sums deterministic. The plain variant holds no trial
+// state, which keeps it at four blocks per SM.
+template <class R, int KMAX, bool MOVE>
+__global__ void __launch_bounds__(kThreads, KMAX == 1 ? 4 : 2)
+    k_chain_energy(const ChainDev ch, const double* __restrict__ x, const double* __restrict__ d,
+                   const LambdaSet* __restrict__ lset, double* __restrict__ partial, int nblk_total, int blk_off,
+                   const int4* __restrict__ table) {
     __shared__ double sm[4 * 32];
     const int n = ch.n_pos;
     const int K = lset ? lset->K : 1;
@@ -132,56 +133,61 @@ __global__ void __launch_bounds__(kThreads) k_chain_energy(const ChainDev ch, co
         w0 = threadIdx.x >> 5;
         ws = blockDim.x >> 5;
     }
-    double acc[kMaxLambda][2];
+    double acc[KMAX][2];
 #pragma unroll
-    for (int k = 0; k < kMaxLambda; ++k) acc[k][0] = acc[k][1] = 0.0;
+    for (int k = 0; k < KMAX; ++k) acc[k][0] = acc[k][1] = 0.0;
     for (int w = w0; lo + (long long)w * 32 < hi; w += ws) {
         const int q = lo + w * 32 + lane;
         const bool in = q < hi;
         const int qe = lane == 0 ? q - 1 : q + 1;
-        const V3 c = pos_of(x, n, q), dc = d ? pos_of(d, n, q) : V3{0.0, 0.0, 0.0};
+        const V3 c = pos_of(x, n, q), dc = MOVE ? pos_of(d, n, q) : V3{0.0, 0.0, 0.0};
         V3 ce{0.0, 0.0, 0.0}, de{0.0, 0.0, 0.0};
         if (lane == 0 || lane == 31) {
             ce = pos_of(x, n, qe);
-            if (d) de = pos_of(d, n, qe);
+            if (MOVE) de = pos_of(d, n, qe);
         }
         const unsigned char fl = in ? ch.flags[q] : 0;
         const double2 lp = in ? ch.link_p[q] : double2{0.0, 0.0};
         const double2 bp = in ? ch.bend_p[q] : double2{0.0, 0.0};
-        V3 cp = shfl_up3(c), cn = shfl_down3(c), dp = shfl_up3(dc), dn = shfl_down3(dc);
-        if (lane == 0) {
-            cp = ce;
-            dp = de;
+        V3 cp = shfl_up3(c), cn = shfl_down3(c);
+        if (lane == 0) cp = ce;
+        if (lane == 31) cn = ce;
+        if (!MOVE) {
+            if (fl & kLink) acc[0][0] += stretch_energy<R>(c, cn, lp.x, lp.y);
+            if (fl & kBend) acc[0][1] += bend_energy<R>(diff<R>(cp, c), diff<R>(c, cn), bp.x, bp.y);
+            continue;
         }
-        if (lane == 31) {
-            cn = ce;
-            dn = de;
-        }
+        V3 dp = shfl_up3(dc), dn = shfl_down3(dc);
+        if (lane == 0) dp = de;
+        if (lane == 31) dn = de;
         if (fl) {
 #pragma unroll
-            for (int k = 0; k < kMaxLambda; ++k) {
+            for (int k = 0; k < KMAX; ++k) {
                 if (k >= K) break;
                 const double lam = lset ? lset->lam[k] : 0.0;
-                const V3 Pc = d ? move3(c, lam, dc) : c, Pn = d ? move3(cn, lam, dn) : cn;
+                const V3 Pc = move3(c, lam, dc), Pn = move3(cn, lam, dn);
                 if (fl & kLink) acc[k][0] += stretch_energy<R>(Pc, Pn, lp.x, lp.y);
                 if (fl & kBend) {
-                    const V3 Pp = d ? move3(cp, lam, dp) : cp;
+                    const V3 Pp = move3(cp, lam, dp);
                     acc[k][1] += bend_energy<R>(diff<R>(Pp, Pc), diff<R>(Pc, Pn), bp.x, bp.y);
                 }
             }
         }
     }
 #pragma unroll
-    for (int k = 0; k < kMaxLambda; ++k) {
+    for (int k = 0; k < KMAX; ++k) {
         if (k >= K) break;
         double e[2] = {acc[k][0], acc[k][1]};
         block_sum<2>(e, sm);
         if (threadIdx.x == 0) {
-            double* o = partial + ((size_t)k * nblk_total + blk_off + blockIdx.x) * 4;
-            o[0] = e[0];
-            o[1] = e[1];
-            o[2] = 0.0;
-            o[3] = 0.0;
+            // a plain pass writes its one evaluation to every requested slot
+            for (int kk = k; kk < (MOVE ? k + 1 : K); ++kk) {
+                double* o = partial + ((size_t)kk * nblk_total + blk_off + blockIdx.x) * 4;
+                o[0] = e[0];
+                o[1] = e[1];
+                o[2] = 0.0;
+                o[3] = 0.0;
+            }
         }
     }
 }
@@ -235,10 +241,13 @@ void launch_chain_energy(const ChainDev& ch, int prec, const double* x, const do
     if (ch.n_pos <= 0) return;
     const int g = table ? table_blocks : chain_blocks(ch);
     if (g <= 0) return;
-    if (prec == MEDYAN_PREC_MIXED)
-        k_chain_energy<float><<<g, kThreads, 0, s>>>(ch, x, d, lam, partial, nblk_total, blk_off, table);
-    else
-        k_chain_energy<double><<<g, kThreads, 0, s>>>(ch, x, d, lam, partial, nblk_total, blk_off, table);
+    if (prec == MEDYAN_PREC_MIXED) {
+        if (d) k_chain_energy<float, kMaxLambda, true><<<g, kThreads, 0, s>>>(ch, x, d, lam, partial, nblk_total, blk_off, table);
+        else k_chain_energy<float, 1, false><<<g, kThreads, 0, s>>>(ch, x, d, lam, partial, nblk_total, blk_off, table);
+    } else {
+        if (d) k_chain_energy<double, kMaxLambda, true><<<g, kThreads, 0, s>>>(ch, x, d, lam, partial, nblk_total, blk_off, table);
+        else k_chain_energy<double, 1, false><<<g, kThreads, 0, s>>>(ch, x, d, lam, partial, nblk_total, blk_off, table);
+    }
 }
 
 void launch_to_internal(int n3, const int* order, const double* ext, double* in, cudaStream_t s) {

@@ -21,7 +21,7 @@ namespace {
 
 __device__ __forceinline__ V3 at(const V3& x, const V3& d, double lam, bool move) { return move ? move3(x, lam, d) : x; }
 
-template <class R>
+template <class R, bool MOVE>
 __global__ void __launch_bounds__(kExclBlock) k_excl_energy(const DeviceFF ff, const double* __restrict__ x,
                                                             const double* __restrict__ d,
                                                             const LambdaSet* __restrict__ lset,
@@ -31,7 +31,7 @@ __global__ void __launch_bounds__(kExclBlock) k_excl_energy(const DeviceFF ff, c
     __shared__ double smem[4 * 32];
     if (ff.act && !ff.act[ff.rep_excl[blockIdx.x]]) return;  // batched: replica not in this pass
     const int i = blockIdx.x * kExclBlock + threadIdx.x;
-    const bool move = d != nullptr;
+    const bool move = MOVE;
     bool valid = i < ff.n_excl;
     V3 X[4] = {}, D[4] = {};
     double krs = 0;
@@ -318,41 +318,80 @@ __global__ void __launch_bounds__(kFinishThreads) k_energy_finish(const DeviceFF
         }
         __syncthreads();
     }
-    // per-slot sums: warp w takes (lambda, slot) combos w, w + nwarps, ...;
-    // each lane sums rows lane, lane + 32, ... of the slot's row ranges, eight
-    // loads in flight at a time, then the warp reduces (fixed order)
+    // per-slot sums: each thread loads rows t, t + blockDim, ... of a lambda's
+    // row set in one round, adds each row's columns into the slot its range
+    // belongs to (chain rows: slots 0 and 1; bonded segment s: slot s, or
+    // slots 4-7 for branching, slot 9 for the boundary; excluded-volume rows:
+    // slot 8), and the block reduces the ten per-thread sums in a fixed tree
+    __shared__ double wsum[kFinishThreads / 32][MEDYAN_FF_COUNT];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-    auto range_sum = [&](const double* base, int b0, int b1, int j) {
-        double acc = 0.0;
-        int b = b0 + lane;
-        for (; b + 32 * 7 < b1; b += 32 * 8) {
-            double v[8];
+    int seg[7];
 #pragma unroll
-            for (int u = 0; u < 8; ++u) v[u] = __ldcg(base + (size_t)(b + 32 * u) * 4 + j);
-#pragma unroll
-            for (int u = 0; u < 8; ++u) acc += v[u];
-        }
-        for (; b < b1; b += 32) acc += __ldcg(base + (size_t)b * 4 + j);
-        return acc;
-    };
-    for (int combo = warp; combo < K * MEDYAN_FF_COUNT; combo += nwarp) {
-        const int k = combo / MEDYAN_FF_COUNT, slot = combo % MEDYAN_FF_COUNT;
-        // row ranges: chain rows [0, nch), bonded rows nch + seg[], excluded-volume rows after
-        int b0 = 0, b1 = 0, j = 0, c1 = 0, cj = 0;
-        switch (slot) {
-            case 0: c1 = nch; cj = 0; b0 = nch + ff.seg[0]; b1 = nch + ff.seg[1]; break;
-            case 1: c1 = nch; cj = 1; b0 = nch + ff.seg[1]; b1 = nch + ff.seg[2]; break;
-            case 2: b0 = nch + ff.seg[2]; b1 = nch + ff.seg[3]; break;
-            case 3: b0 = nch + ff.seg[3]; b1 = nch + ff.seg[4]; break;
-            case 4: case 5: case 6: case 7: b0 = nch + ff.seg[4]; b1 = nch + ff.seg[5]; j = slot - 4; break;
-            case 8: b0 = nch + nbb; b1 = nch + nbb + nbe; break;
-            default: b0 = nch + ff.seg[5]; b1 = nch + ff.seg[6]; break;
-        }
+    for (int i = 0; i < 7; ++i) seg[i] = ff.seg[i];
+    constexpr int kRows = 2;
+    for (int k = 0; k < K; ++k) {
         const double* base = partial + (size_t)k * total_blocks * 4;
-        double sv = range_sum(base, b0, b1, j) + range_sum(base, 0, c1, cj);
+        double acc[MEDYAN_FF_COUNT];
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) sv += __shfl_down_sync(0xffffffffu, sv, o);
-        if (lane == 0) sums[k][slot] = sv;
+        for (int i = 0; i < MEDYAN_FF_COUNT; ++i) acc[i] = 0.0;
+        for (int r0 = 0; r0 < total_blocks; r0 += kRows * blockDim.x) {
+            double2 lo[kRows], hi[kRows];
+#pragma unroll
+            for (int u = 0; u < kRows; ++u) {
+                const int r = r0 + u * blockDim.x + threadIdx.x;
+                if (r < total_blocks) {
+                    const double2* row = reinterpret_cast<const double2*>(base + (size_t)r * 4);
+                    lo[u] = __ldcg(row);
+                    hi[u] = __ldcg(row + 1);
+                } else {
+                    lo[u] = hi[u] = double2{0.0, 0.0};
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kRows; ++u) {
+                const int r = r0 + u * blockDim.x + threadIdx.x;
+                if (r >= total_blocks) continue;
+                if (r < nch) {
+                    acc[0] += lo[u].x;
+                    acc[1] += lo[u].y;
+                    continue;
+                }
+                const int rb = r - nch;
+                if (rb >= nbb) {
+                    acc[MEDYAN_FF_EXCLUDED_VOLUME] += lo[u].x;
+                } else if (rb < seg[4]) {
+                    const int sg = rb < seg[1] ? 0 : rb < seg[2] ? 1 : rb < seg[3] ? 2 : 3;
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+                        if (i == sg) acc[i] += lo[u].x;
+                } else if (rb < seg[5]) {
+                    acc[4] += lo[u].x;
+                    acc[5] += lo[u].y;
+                    acc[6] += hi[u].x;
+                    acc[7] += hi[u].y;
+                } else {
+                    acc[9] += lo[u].x;
+                }
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < MEDYAN_FF_COUNT; ++i) {
+            double v = acc[i];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+            if (lane == 0) wsum[warp][i] = v;
+        }
+        __syncthreads();
+        if (warp == 0) {
+#pragma unroll
+            for (int i = 0; i < MEDYAN_FF_COUNT; ++i) {
+                double v = lane < nwarp ? wsum[lane][i] : 0.0;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+                if (lane == 0) sums[k][i] = v;
+            }
+        }
+        __syncthreads();
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -511,7 +550,12 @@ void launch_excl_energy(const DeviceFF& ff, int prec, const double* x, const dou
     // FP64 in both precision modes: the analytic integral (differences of
     // arctangents, JJ = -(triple product)^2) loses ~1e-6 relative in float.
     (void)prec;
-    k_excl_energy<double><<<nbe, kExclBlock, 0, s>>>(ff, x, d, lam, es.partial, total,
+    if (d)
+        k_excl_energy<double, true><<<nbe, kExclBlock, 0, s>>>(ff, x, d, lam, es.partial, total,
+                                                     es.n_blocks_chain + es.n_blocks_bonded, es.fb_count, es.fb_list,
+                                                     es.bad);
+    else
+        k_excl_energy<double, false><<<nbe, kExclBlock, 0, s>>>(ff, x, d, lam, es.partial, total,
                                                      es.n_blocks_chain + es.n_blocks_bonded, es.fb_count, es.fb_list,
                                                      es.bad);
 }

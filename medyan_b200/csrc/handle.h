@@ -123,6 +123,7 @@ struct medyan_mech {
     // [0] energy, [1] forces, [2] energy then forces
     cudaGraphExec_t pass_graph[3] = {nullptr, nullptr, nullptr};
     long long pass_graph_gen[3] = {-1, -1, -1};
+    int pass_kernels[3] = {0, 0, 0};      // kernel nodes of each pass graph
 
     mb::DeviceFF ff{};
     mb::EnergyScratch es{};

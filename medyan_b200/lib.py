@@ -36,6 +36,7 @@ PROTOTYPES = {
     "medyan_mech_enqueue_forces": (C.c_int32, [_vp]),
     "medyan_mech_synchronize": (C.c_int32, [_vp]),
     "medyan_mech_stream": (_vp, [_vp]),
+    "medyan_mech_pass_kernel_count": (C.c_int32, [_vp, C.c_int32]),
     "medyan_mech_device_buffers": (C.c_int32, [_vp, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp)]),
     "medyan_cg_minimize": (C.c_int32, [_vp, _vp, _pd, _pd, _vp]),
     "medyan_nl_build": (C.c_int32, [_vp, _pd, C.c_int32, _vp, _pi, C.c_int64, _pi64]),

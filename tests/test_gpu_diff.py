@@ -214,12 +214,21 @@ def minimized(base, nb, x0, s_k, s_l0):
         ff.vectorize_all_force_fields(system_for(base, nb, s_k, s_l0))
         st, x, f, r = ff.minimize(x0, CG_PARAMS)
         assert st == 0, st
-        for _ in range(6):
+        for _ in range(10):
             f = ff.compute_forces(x)
-            if np.abs(f).max() < 1e-9:
+            fn = np.abs(f).max()
+            if fn < 1e-9:
                 break
-            x = x + cg_solve(ff.hvp, f, tol=1e-9, maxit=500)
-            ff.set_coords(x)
+            step = cg_solve(ff.hvp, f, tol=1e-9, maxit=500)
+            # damped: the truss's near-null rotation modes can make a full
+            # Newton step overshoot; halve until the residual force drops
+            t = 1.0
+            while True:
+                xt = x + t * step
+                if np.abs(ff.compute_forces(xt)).max() < fn or t < 1e-6:
+                    break
+                t *= 0.5
+            x = xt
         assert np.abs(ff.compute_forces(x)).max() < 1e-7
     return x
 

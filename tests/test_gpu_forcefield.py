@@ -124,3 +124,17 @@ def test_rejects_bad_bead_index(gpu_lib):
     with pytest.raises(MedyanError) as e:
         ForceFieldManager().vectorize_all_force_fields(sv)
     assert e.value.status == 2
+
+
+def test_pass_kernel_count(gpu_lib, nets):
+    # the kernel launches one standalone pass makes (the count bench.py reports)
+    sv, x = network_system(nets, "branched")
+    with ForceFieldManager() as ff:
+        ff.vectorize_all_force_fields(sv)
+        L, h = ff.lib, ff.handle
+        ne, nf, nb = (L.medyan_mech_pass_kernel_count(h, w) for w in range(3))
+        assert ne > 0 and nf > 0 and nb == ne + nf
+        assert L.medyan_mech_pass_kernel_count(h, 3) == -1
+        # building the graphs for the count does not disturb evaluation
+        e, per, f = ff.evaluate(x)
+        assert np.isfinite(e)
