@@ -124,59 +124,86 @@ __device__ __forceinline__ bool bad_force(R x) {
 
 // Analytic pair forces (:578-882). Returns false when any component is
 // non-finite or above 1e15 (the caller then uses the quadrature fallback).
+//
+// The kernel is bound by FP64 throughput, and division is the costliest FP64
+// operation in the formula. The expression is the reference's, regrouped so
+// that each of the four arctangent blocks (A: a,c,e; E: a,|c1-c4|^2,g;
+// B: b,c,F; F: b,|c3-c2|^2,h) divides once for 1/Q and twice for its two
+// weights, instead of about a dozen times (x/Q, x/Q^2, x/Q^3 become
+// products with 1/Q). Results agree with the reference's order to rounding;
+// the forces are summed with atomics and so are not bitwise in any case.
+template <class R>
+struct ExclBlockF {
+    R iQ, cN, cQ, cd, c1, T;  // 1/Q, the four coefficients, N/Q*ATG
+};
+
+template <class R>
+__device__ __forceinline__ ExclBlockF<R> excl_force_block(R alpha, R beta, R gam, R u1, R u2, R N) {
+    ExclBlockF<R> o;
+    const R P = sqrt(alpha * beta);
+    const R Q = sqrt(stdmax<R>(R(0), (P + gam) * (P - gam)));
+    const R iQ = R(1) / Q;
+    const R ATG = atan_r<R>(u1 * iQ) - atan_r<R>(u2 * iQ);
+    const R Q2 = Q * Q, iQ2 = iQ * iQ;
+    const R W1 = Q2 / (Q2 + u1 * u1);
+    const R W2 = Q2 / (Q2 + u2 * u2);
+    const R NiQ2 = N * iQ2;
+    o.iQ = iQ;
+    o.cN = ATG * iQ;
+    o.cQ = -(ATG * NiQ2) + (-W1 * u1 + W2 * u2) * NiQ2 * iQ;
+    o.cd = (W1 - W2) * NiQ2;
+    o.c1 = W1 * NiQ2;
+    o.T = N * iQ * ATG;
+    return o;
+}
+
 template <class R>
 __device__ __forceinline__ bool excl_force(const V3& c1, V3 c2, const V3& c3, const V3& c4, double kRS,
                                            T3<R> (&fo)[4]) {
     if (in_plane(c1, c2, c3, c4)) c2 = move_bead2_out_of_plane(c1, c2, c3, 0.01);
-    ExclS<R> S;
-    excl_scalars<R>(c1, c2, c3, c4, S);
-    const R a = S.a, b = S.b, c = S.c, d = S.d, e = S.e, F = S.F;
-    const R AA = S.AA, BB = S.BB, CC = S.CC, DD = S.DD, EE = S.EE, FF = S.FF, GG = S.GG, HH = S.HH;
-    const R JJ = S.JJ, ATG1 = S.ATG1, ATG2 = S.ATG2, ATG3 = S.ATG3, ATG4 = S.ATG4;
+    T3<R> r12 = diff<R>(c1, c2), r34 = diff<R>(c3, c4), r31 = diff<R>(c3, c1), r14 = diff<R>(c1, c4),
+          r32 = diff<R>(c3, c2);
+    const R a = dot(r12, r12), b = dot(r34, r34), c = dot(r31, r31);
+    const R d = dot(r12, r34), e = dot(r12, r31), F = dot(r34, r31);
+    const R g = dot(r12, r14), h = dot(r34, r32), I = dot(r34, r14);
+    R dx = R(c1.x - c4.x), dy = R(c1.y - c4.y), dz = R(c1.z - c4.z);
+    const R sqD = (dx * dx + dy * dy + dz * dz);
+    dx = R(c3.x - c2.x);
+    dy = R(c3.y - c2.y);
+    dz = R(c3.z - c2.z);
+    const R sqE = (dx * dx + dy * dy + dz * dz);
+    T3<R> vA{R(c1.x - c2.x), R(c1.y - c2.y), R(c1.z - c2.z)};
+    T3<R> vB{R(c3.x - c4.x), R(c3.y - c4.y), R(c3.z - c4.z)};
+    T3<R> vC{R(c3.x - c1.x), R(c3.y - c1.y), R(c3.z - c1.z)};
+    const R cpx = vA.y * vB.z - vA.z * vB.y;
+    const R cpy = vA.z * vB.x - vA.x * vB.z;
+    const R cpz = vA.x * vB.y - vA.y * vB.x;
+    const R JJ0 = cpx * vC.x + cpy * vC.y + cpz * vC.z;
+    const R JJ = -JJ0 * JJ0;
+    const R CC = d * e - a * F, GG = d * g - a * I, DD = b * e - d * F, HH = CC + GG - DD;
+    const ExclBlockF<R> A = excl_force_block<R>(a, c, e, a + e, e, CC);
+    const ExclBlockF<R> E = excl_force_block<R>(a, sqD, g, a + e - d, e - d, GG);
+    const ExclBlockF<R> B = excl_force_block<R>(b, c, F, F, F - b, DD);
+    const ExclBlockF<R> Fb = excl_force_block<R>(b, sqE, h, d + F, d + F - b, HH);
     const R invJJ = R(1) / JJ;
-    const R sumBlock = CC / AA * ATG1 + GG / EE * ATG2 + DD / BB * ATG3 + HH / FF * ATG4;
-    const R enFactor = R(kRS) * invJJ / R(2);
-    const R A1 = AA * AA / (AA * AA + (a + e) * (a + e));
-    const R A2 = AA * AA / (AA * AA + e * e);
-    const R E1 = EE * EE / (EE * EE + (a + e - d) * (a + e - d));
-    const R E2 = EE * EE / (EE * EE + (e - d) * (e - d));
-    const R B1 = BB * BB / (BB * BB + F * F);
-    const R B2 = BB * BB / (BB * BB + (F - b) * (F - b));
-    const R F1 = FF * FF / (FF * FF + (d + F) * (d + F));
-    const R F2 = FF * FF / (FF * FF + (d + F - b) * (d + F - b));
-    const R bA_C = ATG1 / AA;
-    const R bA_A = -(ATG1 * CC) / (AA * AA) + (-A1 * (a + e) + A2 * e) * CC / (AA * AA * AA);
-    const R bA_e = ((A1 - A2) * CC) / (AA * AA);
-    const R bA_a = (A1 * CC) / (AA * AA);
-    const R bE_G = ATG2 / EE;
-    const R bE_E = -(ATG2 * GG) / (EE * EE) + (-E1 * (a + e - d) + E2 * (e - d)) * GG / (EE * EE * EE);
-    const R bE_emd = ((E1 - E2) * GG) / (EE * EE);
-    const R bE_a = (E1 * GG) / (EE * EE);
-    const R bB_D = ATG3 / BB;
-    const R bB_B = -(ATG3 * DD) / (BB * BB) + (-B1 * F + B2 * (F - b)) * DD / (BB * BB * BB);
-    const R bB_fmb = ((B1 - B2) * DD) / (BB * BB);
-    const R bB_b = (B1 * DD) / (BB * BB);
-    const R bF_H = ATG4 / FF;
-    const R bF_F = -(ATG4 * HH) / (FF * FF) + (-F1 * (d + F) + F2 * (d + F - b)) * HH / (FF * FF * FF);
-    const R bF_dpfmb = ((F1 - F2) * HH) / (FF * FF);
-    const R bF_b = (F1 * HH) / (FF * FF);
-    const R b11 = bA_C * (-2 * F) + bA_A * (c / AA) + bA_a * 2 + bE_G * (2 * (F - b)) + bE_E * ((b + c - 2 * F) / EE) +
-                  bE_a * 2 + bF_H * (-2 * b) + bF_F * (b / FF);
-    const R b12 = bA_C * e + bE_G * (2 * d - e) + bE_E * ((e - d) / EE) + bE_emd * (-1) + bB_D * (-F) +
-                  bF_H * (2 * d + F) + bF_F * (-(d + F) / FF) + bF_dpfmb;
-    const R b13 = bA_C * d + bA_A * (-e / AA) + bA_e + bE_G * (-d) + bE_E * (-(e - d) / EE) + bE_emd + bB_D * b +
-                  bF_H * (-b) + bF_F * (b / FF);
-    const R b21 = b12;
-    const R b22 = bE_G * (-2 * a) + bE_E * (a / EE) + bB_D * (2 * e) + bB_B * (c / BB) + bB_fmb * (-2) + bB_b * 2 +
-                  bF_H * (-2 * (a + e)) + bF_F * ((a + c + 2 * e) / FF) + bF_dpfmb * (-2) + bF_b * 2;
-    const R b23 = bA_C * (-a) + bE_G * a + bE_E * (-a / EE) + bB_D * (-d) + bB_B * (-F / BB) + bB_fmb + bF_H * d +
-                  bF_F * (-(d + F) / FF) + bF_dpfmb;
-    const R b31 = b13;
-    const R b32 = b23;
-    const R b33 = bA_A * (a / AA) + bE_E * (a / EE) + bB_B * (b / BB) + bF_F * (b / FF);
+    const R sumBlock = A.T + E.T + B.T + Fb.T;
+    const R enFactor = R(kRS) * invJJ * R(0.5);
+    // b_ij of the reference (:747-781) with x/Q written as x*(1/Q)
+    const R b11 = A.cN * (-2 * F) + A.cQ * (c * A.iQ) + A.c1 * 2 + E.cN * (2 * (F - b)) +
+                  E.cQ * ((b + c - 2 * F) * E.iQ) + E.c1 * 2 + Fb.cN * (-2 * b) + Fb.cQ * (b * Fb.iQ);
+    const R b12 = A.cN * e + E.cN * (2 * d - e) + E.cQ * ((e - d) * E.iQ) - E.cd + B.cN * (-F) +
+                  Fb.cN * (2 * d + F) + Fb.cQ * (-(d + F) * Fb.iQ) + Fb.cd;
+    const R b13 = A.cN * d + A.cQ * (-e * A.iQ) + A.cd + E.cN * (-d) + E.cQ * (-(e - d) * E.iQ) + E.cd + B.cN * b +
+                  Fb.cN * (-b) + Fb.cQ * (b * Fb.iQ);
+    const R b22 = E.cN * (-2 * a) + E.cQ * (a * E.iQ) + B.cN * (2 * e) + B.cQ * (c * B.iQ) + B.cd * (-2) + B.c1 * 2 +
+                  Fb.cN * (-2 * (a + e)) + Fb.cQ * ((a + c + 2 * e) * Fb.iQ) + Fb.cd * (-2) + Fb.c1 * 2;
+    const R b23 = A.cN * (-a) + E.cN * a + E.cQ * (-a * E.iQ) + B.cN * (-d) + B.cQ * (-F * B.iQ) + B.cd + Fb.cN * d +
+                  Fb.cQ * (-(d + F) * Fb.iQ) + Fb.cd;
+    const R b33 = A.cQ * (a * A.iQ) + E.cQ * (a * E.iQ) + B.cQ * (b * B.iQ) + Fb.cQ * (b * Fb.iQ);
+    const R b21 = b12, b31 = b13, b32 = b23;
     const R J11 = 2 * (-b * c + F * F), J12 = 2 * (c * d - e * F), J13 = 2 * (b * e - d * F);
-    const R J21 = 2 * (c * d - e * F), J22 = 2 * (-a * c + e * e), J23 = 2 * (-d * e + a * F);
-    const R J31 = 2 * (b * e - d * F), J32 = 2 * (-d * e + a * F), J33 = 2 * (d * d - a * b);
+    const R J21 = J12, J22 = 2 * (-a * c + e * e), J23 = 2 * (-d * e + a * F);
+    const R J31 = J13, J32 = J23, J33 = 2 * (d * d - a * b);
     const R q = -invJJ * sumBlock;
     R dv[4][3];
     dv[0][0] = enFactor * (q * (J31 - J11) + (b31 - b11));
@@ -191,7 +218,7 @@ __device__ __forceinline__ bool excl_force(const V3& c1, V3 c2, const V3& c3, co
     dv[3][0] = enFactor * (q * (J21) + (b21));
     dv[3][1] = enFactor * (q * (J22) + (b22));
     dv[3][2] = enFactor * (q * (J23) + (b23));
-    const T3<R> u = diff<R>(c1, c2), v = diff<R>(c3, c4), w = diff<R>(c3, c1);
+    const T3<R> u = r12, v = r34, w = diff<R>(c3, c1);
     bool bad = false;
 #pragma unroll
     for (int bi = 0; bi < 4; ++bi) {
