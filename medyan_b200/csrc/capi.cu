@@ -364,6 +364,8 @@ medyan_status medyan_mech::init() {
     if (e == cudaSuccess) e = e_fb_count.reserve(1);
     if (e == cudaSuccess) e = e_bad.reserve(kMaxLambda);
     if (e == cudaSuccess) e = e_fb_list.reserve(kFallbackCap);
+    if (e == cudaSuccess) e = e_stage.reserve((size_t)kMaxLambda * kFinishBlocks * MEDYAN_FF_COUNT);
+    if (e == cudaSuccess) e = e_ticket.reserve(1);
     if (e == cudaSuccess) e = f_fb_count.reserve(1);
     if (e == cudaSuccess) e = f_fb_list.reserve(kFallbackCap);
     if (e == cudaSuccess) e = force_status.reserve(1);
@@ -372,6 +374,7 @@ medyan_status medyan_mech::init() {
     cudaMemsetAsync(x.raw(), 0, sizeof(double) * (n3 ? n3 : 1), stream);
     cudaMemsetAsync(e_fb_count.raw(), 0, sizeof(int), stream);
     cudaMemsetAsync(e_bad.raw(), 0, sizeof(int) * kMaxLambda, stream);
+    cudaMemsetAsync(e_ticket.raw(), 0, sizeof(unsigned int), stream);
     cudaMemsetAsync(f_fb_count.raw(), 0, sizeof(int), stream);
     cudaMemsetAsync(force_status.raw(), 0, sizeof(int), stream);
     LambdaSet z{};
@@ -382,6 +385,8 @@ medyan_status medyan_mech::init() {
     es.fb_list = e_fb_list.raw();
     es.bad = e_bad.raw();
     es.out = energy_out.raw();
+    es.stage = e_stage.raw();
+    es.ticket = e_ticket.raw();
     fs.fb_count = f_fb_count.raw();
     fs.fb_list = f_fb_list.raw();
     fs.status = force_status.raw();

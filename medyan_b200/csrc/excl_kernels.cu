@@ -265,29 +265,132 @@ __global__ void __launch_bounds__(kBlock) k_excl_force_fallback(const DeviceFF f
 }
 
 constexpr int kFinishThreads = 1024;
+constexpr int kSplitFinishThreads = 256;
 
-// Sums the per-block energy partials of each force field (one warp per
-// (lambda, slot) pair, rows in a fixed order, so the result is deterministic),
-// evaluates the energyN fallback for queued pairs in (slot, pair) order, and
-// applies ForceFieldManager::computeEnergy's rule
-// (ForceFieldManager.cpp:137-176): a force field at or below -1 makes the
-// total +inf.
-__global__ void __launch_bounds__(kFinishThreads) k_energy_finish(const DeviceFF ff, const double* __restrict__ x,
-                                                                  const double* __restrict__ d,
-                                                                  const LambdaSet* __restrict__ lset,
-                                                                  const double* __restrict__ partial, int nch,
-                                                                  int nbb, int nbe, int* __restrict__ fb_count,
-                                                                  int2* __restrict__ fb_list, int* __restrict__ bad,
-                                                                  double* __restrict__ out) {
+// Slot sums of one block's share [r_lo, r_hi) of a lambda's partial rows:
+// each thread adds its rows' columns into the slot their range belongs to
+// (chain rows: slots 0 and 1; bonded segment s: slot s, or slots 4-7 for
+// branching, slot 9 for the boundary; excluded-volume rows: slot 8), then the
+// block reduces in a fixed tree. Valid in thread 0 of warp 0 (out[slot]).
+__device__ void finish_rows(const DeviceFF& ff, const double* __restrict__ base, int r_lo, int r_hi, int nch,
+                            int nbb, double* wsum /* [32][MEDYAN_FF_COUNT] */, double* out) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    int seg[7];
+#pragma unroll
+    for (int i = 0; i < 7; ++i) seg[i] = ff.seg[i];
+    double acc[MEDYAN_FF_COUNT];
+#pragma unroll
+    for (int i = 0; i < MEDYAN_FF_COUNT; ++i) acc[i] = 0.0;
+    constexpr int kRows = 2;
+    for (int r0 = r_lo; r0 < r_hi; r0 += kRows * blockDim.x) {
+        double2 lo[kRows], hi[kRows];
+#pragma unroll
+        for (int u = 0; u < kRows; ++u) {
+            const int r = r0 + u * blockDim.x + threadIdx.x;
+            if (r < r_hi) {
+                const double2* row = reinterpret_cast<const double2*>(base + (size_t)r * 4);
+                lo[u] = __ldcg(row);
+                hi[u] = __ldcg(row + 1);
+            } else {
+                lo[u] = hi[u] = double2{0.0, 0.0};
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kRows; ++u) {
+            const int r = r0 + u * blockDim.x + threadIdx.x;
+            if (r >= r_hi) continue;
+            if (r < nch) {
+                acc[0] += lo[u].x;
+                acc[1] += lo[u].y;
+                continue;
+            }
+            const int rb = r - nch;
+            if (rb >= nbb) {
+                acc[MEDYAN_FF_EXCLUDED_VOLUME] += lo[u].x;
+            } else if (rb < seg[4]) {
+                const int sg = rb < seg[1] ? 0 : rb < seg[2] ? 1 : rb < seg[3] ? 2 : 3;
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+                    if (i == sg) acc[i] += lo[u].x;
+            } else if (rb < seg[5]) {
+                acc[4] += lo[u].x;
+                acc[5] += lo[u].y;
+                acc[6] += hi[u].x;
+                acc[7] += hi[u].y;
+            } else {
+                acc[9] += lo[u].x;
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < MEDYAN_FF_COUNT; ++i) {
+        double v = acc[i];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) wsum[warp * MEDYAN_FF_COUNT + i] = v;
+    }
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int i = 0; i < MEDYAN_FF_COUNT; ++i) {
+            double v = lane < nwarp ? wsum[lane * MEDYAN_FF_COUNT + i] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+            if (lane == 0) out[i] = v;
+        }
+    }
+    __syncthreads();
+}
+
+// Sums the per-block energy partials of each force field, evaluates the
+// energyN fallback for queued pairs in (slot, pair) order, and applies
+// ForceFieldManager::computeEnergy's rule (ForceFieldManager.cpp:137-176): a
+// force field at or below -1 makes the total +inf.
+//
+// With stage/ticket the rows are split over gridDim.x blocks: block b sums
+// its share into stage[k][b][slot], and the last block to arrive (ticket)
+// adds the shares in block order and finishes. With one block and no stage
+// the block does everything. Either way every sum is taken in a fixed order,
+// so the result does not depend on scheduling.
+__global__ void __launch_bounds__(kSplitFinishThreads) k_energy_finish(
+    const DeviceFF ff, const double* __restrict__ x, const double* __restrict__ d, const LambdaSet* __restrict__ lset,
+    const double* __restrict__ partial, int nch, int nbb, int nbe, int* __restrict__ fb_count,
+    int2* __restrict__ fb_list, int* __restrict__ bad, double* __restrict__ out, double* __restrict__ stage,
+    unsigned int* __restrict__ ticket) {
     __shared__ double red[4 * 32];
+    __shared__ double wsum[(kSplitFinishThreads / 32) * MEDYAN_FF_COUNT];
     __shared__ double sums[kMaxLambda][MEDYAN_FF_COUNT];
     __shared__ double fbE[kMaxLambda];
     __shared__ int nfb;
+    __shared__ bool last;
     const int K = lset ? lset->K : 1;
     const int total_blocks = nch + nbb + nbe;
+    const int G = gridDim.x;
+    const int chunk = (total_blocks + G - 1) / G;
+    const int r_lo = min(total_blocks, (int)blockIdx.x * chunk), r_hi = min(total_blocks, r_lo + chunk);
+    for (int k = 0; k < K; ++k) {
+        double* dst = G > 1 ? stage + ((size_t)k * G + blockIdx.x) * MEDYAN_FF_COUNT : sums[k];
+        finish_rows(ff, partial + (size_t)k * total_blocks * 4, r_lo, r_hi, nch, nbb, wsum, dst);
+    }
+    if (G > 1) {
+        // last-block-done: publish this block's shares, take a ticket
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == (unsigned)G - 1;
+        __syncthreads();
+        if (!last) return;
+        __threadfence();
+        if (threadIdx.x < K * MEDYAN_FF_COUNT) {
+            const int k = threadIdx.x / MEDYAN_FF_COUNT, slot = threadIdx.x % MEDYAN_FF_COUNT;
+            double v = 0.0;
+            for (int b = 0; b < G; ++b) v += __ldcg(stage + ((size_t)k * G + b) * MEDYAN_FF_COUNT + slot);
+            sums[k][slot] = v;
+        }
+        if (threadIdx.x == 0) *ticket = 0u;
+    }
+    // queued fallback pairs: energyN in (slot, pair) order
     if (threadIdx.x == 0) {
         int n = min(*fb_count, kFallbackCap);
-        // deterministic order: sort queued (pair, slot) by slot, then pair
         for (int a = 1; a < n; ++a) {
             int2 v = fb_list[a];
             int b = a - 1;
@@ -318,82 +421,6 @@ __global__ void __launch_bounds__(kFinishThreads) k_energy_finish(const DeviceFF
         }
         __syncthreads();
     }
-    // per-slot sums: each thread loads rows t, t + blockDim, ... of a lambda's
-    // row set in one round, adds each row's columns into the slot its range
-    // belongs to (chain rows: slots 0 and 1; bonded segment s: slot s, or
-    // slots 4-7 for branching, slot 9 for the boundary; excluded-volume rows:
-    // slot 8), and the block reduces the ten per-thread sums in a fixed tree
-    __shared__ double wsum[kFinishThreads / 32][MEDYAN_FF_COUNT];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-    int seg[7];
-#pragma unroll
-    for (int i = 0; i < 7; ++i) seg[i] = ff.seg[i];
-    constexpr int kRows = 2;
-    for (int k = 0; k < K; ++k) {
-        const double* base = partial + (size_t)k * total_blocks * 4;
-        double acc[MEDYAN_FF_COUNT];
-#pragma unroll
-        for (int i = 0; i < MEDYAN_FF_COUNT; ++i) acc[i] = 0.0;
-        for (int r0 = 0; r0 < total_blocks; r0 += kRows * blockDim.x) {
-            double2 lo[kRows], hi[kRows];
-#pragma unroll
-            for (int u = 0; u < kRows; ++u) {
-                const int r = r0 + u * blockDim.x + threadIdx.x;
-                if (r < total_blocks) {
-                    const double2* row = reinterpret_cast<const double2*>(base + (size_t)r * 4);
-                    lo[u] = __ldcg(row);
-                    hi[u] = __ldcg(row + 1);
-                } else {
-                    lo[u] = hi[u] = double2{0.0, 0.0};
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < kRows; ++u) {
-                const int r = r0 + u * blockDim.x + threadIdx.x;
-                if (r >= total_blocks) continue;
-                if (r < nch) {
-                    acc[0] += lo[u].x;
-                    acc[1] += lo[u].y;
-                    continue;
-                }
-                const int rb = r - nch;
-                if (rb >= nbb) {
-                    acc[MEDYAN_FF_EXCLUDED_VOLUME] += lo[u].x;
-                } else if (rb < seg[4]) {
-                    const int sg = rb < seg[1] ? 0 : rb < seg[2] ? 1 : rb < seg[3] ? 2 : 3;
-#pragma unroll
-                    for (int i = 0; i < 4; ++i)
-                        if (i == sg) acc[i] += lo[u].x;
-                } else if (rb < seg[5]) {
-                    acc[4] += lo[u].x;
-                    acc[5] += lo[u].y;
-                    acc[6] += hi[u].x;
-                    acc[7] += hi[u].y;
-                } else {
-                    acc[9] += lo[u].x;
-                }
-            }
-        }
-#pragma unroll
-        for (int i = 0; i < MEDYAN_FF_COUNT; ++i) {
-            double v = acc[i];
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-            if (lane == 0) wsum[warp][i] = v;
-        }
-        __syncthreads();
-        if (warp == 0) {
-#pragma unroll
-            for (int i = 0; i < MEDYAN_FF_COUNT; ++i) {
-                double v = lane < nwarp ? wsum[lane][i] : 0.0;
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-                if (lane == 0) sums[k][i] = v;
-            }
-        }
-        __syncthreads();
-    }
-    __syncthreads();
     if (threadIdx.x == 0) {
         for (int k = 0; k < K; ++k) {
             double* o = out + k * (MEDYAN_FF_COUNT + 1);
@@ -562,8 +589,10 @@ void launch_excl_energy(const DeviceFF& ff, int prec, const double* x, const dou
 
 void launch_excl_energy_fallback_and_finish(const DeviceFF& ff, const double* x, const double* d,
                                             const LambdaSet* lam, const EnergyScratch& es, cudaStream_t s) {
-    k_energy_finish<<<1, kFinishThreads, 0, s>>>(ff, x, d, lam, es.partial, es.n_blocks_chain, es.n_blocks_bonded,
-                                         es.n_blocks_excl, es.fb_count, es.fb_list, es.bad, es.out);
+    const int g = es.stage && es.ticket ? kFinishBlocks : 1;
+    k_energy_finish<<<g, kSplitFinishThreads, 0, s>>>(ff, x, d, lam, es.partial, es.n_blocks_chain,
+                                                      es.n_blocks_bonded, es.n_blocks_excl, es.fb_count, es.fb_list,
+                                                      es.bad, es.out, es.stage, es.ticket);
 }
 
 void launch_excl_forces(const DeviceFF& ff, int prec, const double* x, const ForceTarget& t, const ForceScratch& fs,

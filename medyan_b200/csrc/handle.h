@@ -165,6 +165,8 @@ struct medyan_mech {
     mb::DevBuf<double> x, f, partial, energy_out;
     mb::DevBuf<int> e_fb_count, e_bad, f_fb_count, f_fb_list, force_status;
     mb::DevBuf<int2> e_fb_list;
+    mb::DevBuf<double> e_stage;
+    mb::DevBuf<unsigned int> e_ticket;
     mb::DevBuf<mb::LambdaSet> lam_zero;
 
     // conjugate gradient (cg.cu)

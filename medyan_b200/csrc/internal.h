@@ -74,6 +74,11 @@ struct EnergyScratch {
     int2* fb_list;        // (pair, lambda slot)
     int* bad;             // per lambda slot: fallback failed / queue overflow
     double* out;          // [kMaxLambda][MEDYAN_FF_COUNT + 1]: per FF, then total
+    // split finish (null: one block does it all): per-block slot sums
+    // [kMaxLambda][kFinishBlocks][MEDYAN_FF_COUNT] and the arrival ticket
+    // (zero between passes; the last block resets it)
+    double* stage;
+    unsigned int* ticket;
     int n_blocks_chain;
     int n_blocks_bonded;
     int n_blocks_excl;
@@ -155,6 +160,7 @@ void launch_energy_producers(const ChainDev& ch, const DeviceFF& ff, const doubl
 cudaError_t init_excl_kernels();
 
 int bonded_blocks(const DeviceFF& ff);
+constexpr int kFinishBlocks = 8;  // blocks of the split energy finish
 constexpr int kExclBlock = 64;  // small blocks: the pair count is low and each pair is heavy
 inline int excl_blocks(const DeviceFF& ff) { return (ff.n_excl + kExclBlock - 1) / kExclBlock; }
 

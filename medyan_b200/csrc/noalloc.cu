@@ -130,6 +130,8 @@ extern "C" medyan_status medyan_excl_energy_noalloc(const double* d_coords, int3
     es.fb_list = reinterpret_cast<int2*>(scratch + kFbListOff);
     es.bad = bad;
     es.out = scratch + kOutOff;
+    es.stage = nullptr;  // one-block finish: no arrival ticket to keep
+    es.ticket = nullptr;
     es.n_blocks_chain = 0;
     es.n_blocks_bonded = 0;
     es.n_blocks_excl = excl_blocks(ff);

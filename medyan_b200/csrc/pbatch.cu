@@ -277,6 +277,8 @@ medyan_status pack_batch(PackedBatch& pb, const std::vector<medyan_mech*>& h) {
     es.fb_list = pb.e_fb_list.raw();
     es.bad = pb.e_bad.raw();
     es.out = nullptr;  // batched results go to pb.out
+    es.stage = nullptr;
+    es.ticket = nullptr;
     pb.fs.fb_count = pb.f_fb_count.raw();
     pb.fs.fb_list = pb.f_fb_list.raw();
     pb.fs.status = pb.force_status.raw();
