@@ -198,6 +198,9 @@ medyan_status medyan_mech_evaluate(medyan_mech* h, const double* coord, double* 
    status of the enqueued passes. */
 medyan_status medyan_mech_enqueue_energy(medyan_mech* h);
 medyan_status medyan_mech_enqueue_forces(medyan_mech* h);
+/* Energy and forces at the handle's coordinates in one pass (what
+   medyan_mech_evaluate runs), the two sets of kernels side by side. */
+medyan_status medyan_mech_enqueue_evaluate(medyan_mech* h);
 medyan_status medyan_mech_synchronize(medyan_mech* h);
 /* The handle's cudaStream_t, for event timing or stream ordering. */
 void* medyan_mech_stream(medyan_mech* h);

@@ -325,8 +325,14 @@ cudaError_t ensure_pass_graph(medyan_mech* h, int which) {
     h->pass_graph[which] = nullptr;
     cudaError_t e = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return e;
-    if (which != kPassForces) enqueue_energy(h, h->x.raw(), nullptr, h->lam_zero.raw(), h->stream);
-    if (which != kPassEnergy) enqueue_forces(h, h->x.raw(), h->f.raw(), h->stream);
+    if (which == kPassBoth)
+        launch_evaluate(h->chain, h->ff, h->prec, h->x.raw(), h->lam_zero.raw(),
+                        ForceTarget{h->f.raw(), nullptr, nullptr, nullptr, nullptr, nullptr}, h->es, h->fs, h->stream,
+                        &h->fork);
+    else if (which == kPassEnergy)
+        enqueue_energy(h, h->x.raw(), nullptr, h->lam_zero.raw(), h->stream);
+    else
+        enqueue_forces(h, h->x.raw(), h->f.raw(), h->stream);
     cudaGraph_t g = nullptr;
     e = cudaStreamEndCapture(h->stream, &g);
     if (e == cudaSuccess) e = count_kernel_nodes(g, &h->pass_kernels[which]);
@@ -354,6 +360,7 @@ medyan_status medyan_mech::init() {
     for (int k = 0; k < kForkWays && e == cudaSuccess; ++k)
         e = cudaStreamCreateWithFlags(&fork.side[k], cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&fork.fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&fork.mid, cudaEventDisableTiming);
     for (int k = 0; k < kForkWays && e == cudaSuccess; ++k)
         e = cudaEventCreateWithFlags(&fork.join[k], cudaEventDisableTiming);
     if (e == cudaSuccess) e = init_excl_kernels();
@@ -404,6 +411,7 @@ medyan_mech::~medyan_mech() {
     for (auto& sd : fork.side)
         if (sd) cudaStreamDestroy(sd);
     if (fork.fork) cudaEventDestroy(fork.fork);
+    if (fork.mid) cudaEventDestroy(fork.mid);
     for (auto& ev : fork.join)
         if (ev) cudaEventDestroy(ev);
     if (stream) cudaStreamDestroy(stream);
@@ -521,6 +529,11 @@ medyan_status medyan_mech_enqueue_energy(medyan_mech* h) {
 medyan_status medyan_mech_enqueue_forces(medyan_mech* h) {
     if (!h) return MEDYAN_ERR_INVALID_ARG;
     return cuda_status(launch_pass(h, kPassForces));
+}
+
+medyan_status medyan_mech_enqueue_evaluate(medyan_mech* h) {
+    if (!h) return MEDYAN_ERR_INVALID_ARG;
+    return cuda_status(launch_pass(h, kPassBoth));
 }
 
 medyan_status medyan_mech_synchronize(medyan_mech* h) {

@@ -333,10 +333,10 @@ void launch_energy_producers(const ChainDev& ch, const DeviceFF& ff, const doubl
                              const int4* chain_table, int chain_table_blocks) {
     // five branches: chain | excluded volume | linker, motor | branching |
     // boundary, filament leftovers
-    cudaStream_t b[kForkWays] = {s, s, s, s};
+    cudaStream_t b[4] = {s, s, s, s};
     if (fk) {
-        fork_to(fk, s, kForkWays);
-        for (int k = 0; k < kForkWays; ++k) b[k] = fk->side[k];
+        fork_to(fk, s, 4);
+        for (int k = 0; k < 4; ++k) b[k] = fk->side[k];
     }
     launch_excl_energy(ff, MEDYAN_PREC_FP64, x, d, lam, es, b[0]);
     bonded_energy_group<2, 4>(ff, x, d, lam, es, b[1]);
@@ -345,7 +345,7 @@ void launch_energy_producers(const ChainDev& ch, const DeviceFF& ff, const doubl
     bonded_energy_group<0, 2>(ff, x, d, lam, es, b[3]);
     launch_chain_energy(ch, MEDYAN_PREC_FP64, x, d, lam, es.partial, es.total(), 0, s, chain_table,
                         chain_table_blocks);
-    if (fk) join_from(fk, s, kForkWays);
+    if (fk) join_from(fk, s, 4);
 }
 
 void launch_energy(const ChainDev& ch, const DeviceFF& ff, int prec, const double* x, const double* d,
@@ -364,7 +364,7 @@ void launch_forces(const ChainDev& ch, const DeviceFF& ff, int prec, const doubl
     // branches: excluded volume | linker, motor | branching | boundary,
     // filament leftovers
     launch_chain_forces(ch, prec, x, t, s);
-    cudaStream_t b[kForkWays] = {s, s, s, s};
+    cudaStream_t b[4] = {s, s, s, s};
     if (fk) {
         fork_to(fk, s, 3);
         for (int k = 0; k < 3; ++k) b[k + 1] = fk->side[k];
@@ -375,6 +375,44 @@ void launch_forces(const ChainDev& ch, const DeviceFF& ff, int prec, const doubl
     bonded_forces_group<0, 2>(ff, prec, x, t, b[3]);
     launch_excl_forces(ff, prec, x, t, fs, s);
     if (fk) join_from(fk, s, 3);
+}
+
+void launch_evaluate(const ChainDev& ch, const DeviceFF& ff, int prec, const double* x, const LambdaSet* lam,
+                     const ForceTarget& t, const EnergyScratch& es, const ForceScratch& fs, cudaStream_t s,
+                     const Fork* fk) {
+    if (!fk) {
+        launch_energy(ch, ff, prec, x, nullptr, lam, es, s, nullptr);
+        launch_forces(ch, ff, prec, x, t, fs, s, nullptr);
+        return;
+    }
+    // side 0: excluded-volume energy, then the finish once sides 1-4 are done;
+    // sides 1-4: bonded groups and chain energy; main: chain forces, then
+    // the excluded-volume forces; sides 5-7: bonded forces after the chain
+    // forces (which initialize the force array)
+    fork_to(fk, s, kForkWays);
+    launch_excl_energy(ff, MEDYAN_PREC_FP64, x, nullptr, lam, es, fk->side[0]);
+    bonded_energy_group<2, 4>(ff, x, nullptr, lam, es, fk->side[1]);
+    bonded_energy_group<4, 5>(ff, x, nullptr, lam, es, fk->side[2]);
+    bonded_energy_group<5, 6>(ff, x, nullptr, lam, es, fk->side[3]);
+    bonded_energy_group<0, 2>(ff, x, nullptr, lam, es, fk->side[3]);
+    launch_chain_energy(ch, MEDYAN_PREC_FP64, x, nullptr, lam, es.partial, es.total(), 0, fk->side[4], nullptr, 0);
+    launch_chain_forces(ch, prec, x, t, s);
+    cudaEventRecord(fk->mid, s);
+    for (int k = 5; k < 8; ++k) cudaStreamWaitEvent(fk->side[k], fk->mid, 0);
+    bonded_forces_group<2, 4>(ff, prec, x, t, fk->side[5]);
+    bonded_forces_group<4, 5>(ff, prec, x, t, fk->side[6]);
+    bonded_forces_group<5, 6>(ff, prec, x, t, fk->side[7]);
+    bonded_forces_group<0, 2>(ff, prec, x, t, fk->side[7]);
+    launch_excl_forces(ff, prec, x, t, fs, s);
+    for (int k = 1; k < 5; ++k) {
+        cudaEventRecord(fk->join[k], fk->side[k]);
+        cudaStreamWaitEvent(fk->side[0], fk->join[k], 0);
+    }
+    launch_excl_energy_fallback_and_finish(ff, x, nullptr, lam, es, fk->side[0]);
+    for (int k : {0, 5, 6, 7}) {
+        cudaEventRecord(fk->join[k], fk->side[k]);
+        cudaStreamWaitEvent(s, fk->join[k], 0);
+    }
 }
 
 }  // namespace mb

@@ -112,10 +112,11 @@ struct ForceScratch {
 // independent kernels on separate streams joined back into the caller's
 // stream; under stream capture the fork and join become graph edges, so the
 // kernels are parallel branches of the graph.
-constexpr int kForkWays = 4;
+constexpr int kForkWays = 8;
 struct Fork {
     cudaStream_t side[kForkWays];
     cudaEvent_t fork, join[kForkWays];
+    cudaEvent_t mid;  // a point inside a pass that later branches wait for
 };
 
 // Launchers (ff_kernels.cu / excl_kernels.cu / chain.cu). prec: MEDYAN_PREC_*.
@@ -125,6 +126,12 @@ void launch_energy(const ChainDev& ch, const DeviceFF& ff, int prec, const doubl
                    const LambdaSet* lam, const EnergyScratch& es, cudaStream_t s, const Fork* fk = nullptr);
 void launch_forces(const ChainDev& ch, const DeviceFF& ff, int prec, const double* x, const ForceTarget& t,
                    const ForceScratch& fs, cudaStream_t s, const Fork* fk = nullptr);
+// Energy (at x, one step size: lam) and forces at x in one pass: the energy
+// producers and the force kernels run side by side (with fk), the energy
+// finish after its producers.
+void launch_evaluate(const ChainDev& ch, const DeviceFF& ff, int prec, const double* x, const LambdaSet* lam,
+                     const ForceTarget& t, const EnergyScratch& es, const ForceScratch& fs, cudaStream_t s,
+                     const Fork* fk);
 void launch_chain_forces(const ChainDev& ch, int prec, const double* x, const ForceTarget& t, cudaStream_t s);
 // table (optional): block b evaluates positions [table[b].y, table[b].z) of one
 // replica (batched layouts), table_blocks blocks; else a grid-stride pass.
