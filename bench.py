@@ -290,7 +290,7 @@ def roofline(achieved_gbs: float, nbytes: int) -> dict:
         with open(prof) as fh:
             traffic = json.load(fh).get("bytes_per_launch")
     return {"bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s", "frac": achieved_gbs / peak,
-            "traffic": traffic, "peak_source": src, "kernel": "force pass (bonded + excluded-volume kernels)",
+            "traffic": traffic, "peak_source": src, "kernel": "force pass (chain, bonded groups, excluded volume), timed alone",
             "algorithmic_bytes_per_launch": nbytes}
 
 
