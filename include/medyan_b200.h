@@ -362,6 +362,20 @@ medyan_status medyan_mech_param_grad(medyan_mech* h, int32_t ff, const double* v
    float forces). */
 medyan_status medyan_mech_hvp(medyan_mech* h, const double* v, double* hv);
 
+/* ForceFieldManager::computeHessian (src/Mechanics/ForceField/ForceFieldManager.cpp:354-398):
+   the dense finite-difference Hessian at the handle's coordinates, row i
+   the perturbed degree of freedom, column j the force component (caller's
+   bead order, ndof = 3*n_beads, row-major host array of ndof*ndof doubles):
+     H[i*ndof + j] = (float)(-(F_j(x + delta e_i) - F_j(x - delta e_i)) / (2*delta)),
+   each entry rounded to float as the reference stores it, delta the
+   reference's float hessDelta. 2*ndof force passes; the coordinates are
+   restored exactly. The reference's eigenmode analysis (symmetrization,
+   eigensolve, participation ratios, :400-480) works on this matrix and is
+   left to the caller (medyan_b200.forcefield.hessian_modes). Use an FP64
+   handle. ndof above MEDYAN_HESSIAN_MAX_DOF: MEDYAN_ERR_INVALID_ARG. */
+#define MEDYAN_HESSIAN_MAX_DOF 24576
+medyan_status medyan_mech_hessian(medyan_mech* h, float delta, double* H);
+
 /* ------------------------------------------------------------------------ */
 /* Batched minimization of independent networks                              */
 /* ------------------------------------------------------------------------ */

@@ -156,6 +156,17 @@ class ForceFieldManager:
             L.check(st, "medyan_mech_hvp")
         return hv
 
+    def hessian(self, delta: float = 1e-4) -> np.ndarray:
+        """ForceFieldManager::computeHessian (ForceFieldManager.cpp:354-398):
+        the dense finite-difference Hessian at the current coordinates,
+        H[i, j] = float(-(F_j(x + delta e_i) - F_j(x - delta e_i)) / (2 delta))."""
+        n = 3 * self.n_beads
+        H = np.zeros((n, n))
+        st = self.lib.medyan_mech_hessian(self.handle, C.c_float(delta), _dp(H))
+        if st not in (0, 3):
+            L.check(st, "medyan_mech_hessian")
+        return H
+
     # -- neighbor lists ----------------------------------------------------
     def set_cylinders(self, cylinders, nl_params, boundary_params) -> None:
         self._cyl = (cylinders, nl_params, boundary_params)
@@ -286,3 +297,38 @@ def neighbor_pairs(cylinders, coord, n_beads: int, nl_params) -> np.ndarray:
     L.check(lib.medyan_nl_build(cylinders.ref(), _dp(x), n_beads, C.byref(nl_params), pairs.ctypes.data_as(_pi),
                                 n.value, C.byref(n)), "medyan_nl_build")
     return pairs[: 2 * n.value].reshape(-1, 2)
+
+
+@dataclass
+class HessianModes:
+    """The eigenmode analysis of ForceFieldManager::computeHessian
+    (ForceFieldManager.cpp:400-480): eigenvalues in ascending order, the
+    eigenvectors as columns, and the two participation ratios per mode,
+    IPRI = sum_i v_i^4 and IPRII = sum_beads (sum_k v_{3b+k}^2)^2."""
+    evalues: np.ndarray
+    evectors: np.ndarray
+    IPRI: np.ndarray
+    IPRII: np.ndarray
+
+
+def hessian_modes(H: np.ndarray) -> HessianModes:
+    """Symmetrize 0.5 (H^T + H) and take its full eigendecomposition (the
+    reference's dense branch, SelfAdjointEigenSolver; its sparse branch asks
+    Spectra for the ndof - 1 smallest, the first ndof - 1 of these), then the
+    participation ratios. The eigensolve runs on the GPU through torch when
+    one is present."""
+    Hs = 0.5 * (H.T + H)
+    try:
+        import torch
+        if torch.cuda.is_available():
+            w, v = torch.linalg.eigh(torch.from_numpy(Hs).cuda())
+            w, v = w.cpu().numpy(), v.cpu().numpy()
+        else:
+            w, v = np.linalg.eigh(Hs)
+    except ImportError:
+        w, v = np.linalg.eigh(Hs)
+    sq = v * v
+    ipri = np.sum(sq * sq, axis=0)
+    per_bead = sq.reshape(-1, 3, sq.shape[1]).sum(axis=1)
+    iprii = np.sum(per_bead * per_bead, axis=0)
+    return HessianModes(w, v, ipri, iprii)

@@ -1428,3 +1428,31 @@ int64_t oracle_boundary_vectorize(const medyan_cylinders* c, const double* x, co
     }
     return m;
 }
+
+/* ForceFieldManager::computeHessian, ForceFieldManager.cpp:354-398: for each
+   degree of freedom i, forces at copies of the coordinates with x_i + delta
+   and x_i - delta (delta a float, as the reference's hessDelta), and
+   H[i][j] = (float)(-(Fp[j] - Fm[j]) / (2 * delta)) stored in a double. */
+void oracle_hessian(const medyan_system* s, const double* x, float delta, double* H) {
+    const int n = 3 * s->n_beads;
+    double* cp = (double*)malloc(sizeof(double) * (size_t)n);
+    double* cm = (double*)malloc(sizeof(double) * (size_t)n);
+    double* fp = (double*)malloc(sizeof(double) * (size_t)n);
+    double* fm = (double*)malloc(sizeof(double) * (size_t)n);
+    for (int i = 0; i < n; ++i) {
+        memcpy(cp, x, sizeof(double) * (size_t)n);
+        memcpy(cm, x, sizeof(double) * (size_t)n);
+        cp[i] += delta;
+        cm[i] -= delta;
+        oracle_forces(s, cp, fp);
+        oracle_forces(s, cm, fm);
+        for (int j = 0; j < n; ++j) {
+            float h = -(fp[j] - fm[j]) / (2 * delta);
+            H[(size_t)i * n + j] = h;
+        }
+    }
+    free(cp);
+    free(cm);
+    free(fp);
+    free(fm);
+}

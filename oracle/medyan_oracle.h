@@ -51,6 +51,8 @@ void oracle_boundary_forces(const double* x, double* f, const medyan_system* s);
 /* ForceFieldManager semantics. */
 double oracle_energy(const medyan_system* s, const double* x, double* e_per_ff);
 void oracle_forces(const medyan_system* s, const double* x, double* f);
+/* ForceFieldManager::computeHessian: dense FD Hessian, row-major 3N x 3N. */
+void oracle_hessian(const medyan_system* s, const double* x, float delta, double* H);
 
 /* CGMethod::minimize driven by callbacks: energy(x), forces(x, f) and the
    per-force-field energies (x, per[MEDYAN_FF_COUNT]). n_beads only sets the

@@ -57,6 +57,8 @@ class Oracle:
         L.oracle_excl_vectorize.argtypes = [C.c_void_p, _pi, C.c_int64, _pi, _pd, _pd]
         L.oracle_boundary_vectorize.restype = C.c_int64
         L.oracle_boundary_vectorize.argtypes = [C.c_void_p, _pd, C.c_void_p, _pi, _pd, _pd, _pi]
+        L.oracle_hessian.restype = None
+        L.oracle_hessian.argtypes = [C.c_void_p, _pd, C.c_float, _pd]
         L.oracle_excl_pair_energy.restype = C.c_double
         L.oracle_excl_pair_energy.argtypes = [_pd, _pd, _pd, _pd, C.c_double]
 
@@ -79,6 +81,13 @@ class Oracle:
         r = MinResult()
         st = self.lib.oracle_cg_minimize(sv.ref(), C.byref(params), _dp(x), _dp(f), C.byref(r))
         return st, x, f, r
+
+    def hessian(self, sv: SystemView, x: np.ndarray, delta: float) -> np.ndarray:
+        x = f64(x)
+        n = x.size
+        H = np.zeros((n, n))
+        self.lib.oracle_hessian(sv.ref(), _dp(x), C.c_float(delta), _dp(H))
+        return H
 
     def neighbor_pairs(self, cyl_view, x: np.ndarray, n_beads: int, nl_params) -> tuple[int, np.ndarray]:
         x = f64(x)
