@@ -362,6 +362,53 @@ medyan_status medyan_mech_param_grad(medyan_mech* h, int32_t ff, const double* v
    float forces). */
 medyan_status medyan_mech_hvp(medyan_mech* h, const double* v, double* hv);
 
+/* ---- after a minimization: inputs of the chemical rate changers ----
+   MController::afterMinimization_ (src/Controller/MController.h:238-268)
+   runs ffm.assignallforcemags() and ffm.computeAuxParams(), whose
+   computeLoadForces fills the filament tips' load forces. */
+
+/* The force magnitudes each force field stores during its force pass and
+   assignforcemags adds to the chemistry's objects
+   (ForceFieldManager::assignallforcemags, ForceFieldManager.cpp:346-351), at
+   the handle's coordinates, FP64, caller's interaction order; each array may
+   be null:
+     linker_stretch[i] = f0/invL = k (L - l0) of linker i, the value
+       LinkerStretching::assignforcemags adds to MLinker::stretchForce
+       (LinkerStretchingHarmonic.cpp:227-293, LinkerStretching.cpp:118-123);
+     motor_stretch[i]: the same for motor i (MotorGhostStretching.cpp:125-130);
+     branch_force[3*i .. 3*i+2]: the force each enabled branching force
+       field puts on the third bead of branch point i, summed in force-field
+       order (stretching, bending, dihedral, position), the value their
+       assignforcemags add to MBranchingPoint::branchForce. */
+medyan_status medyan_mech_force_magnitudes(medyan_mech* h, double* linker_stretch, double* motor_stretch,
+                                           double* branch_force);
+
+/* Filament tips whose boundary load forces are wanted. Cylinder indices
+   refer to the list given to medyan_mech_set_cylinders. */
+typedef struct medyan_load_tips {
+    int32_t n_tips;
+    const int32_t* cylinder;        /* the tip's cylinder                       */
+    const int32_t* plus_end;        /* 1: plus end (load on bead2, growing from
+                                       bead1 to bead2); 0: minus end (bead1)   */
+    const int32_t* n_mon;           /* cylinderNumMon of the tip bead's type   */
+    const double* mon_size;         /* monomerSize of that type                */
+} medyan_load_tips;
+
+/* BoundaryCylinderRepulsion::computeLoadForces with the exponential
+   repulsion (BoundaryCylinderRepulsion.cpp:125-196, BoundaryCylinderRepulsionExp.cpp:113-118):
+   for each boundary plane whose neighbor list (the last
+   medyan_mech_rebuild_neighbors) holds the tip's cylinder, and each monomer
+   position i < n_mon of the tip, newCoord = tip bead + i*mon_size*dir (dir
+   the unit vector from the other bead to the tip bead),
+     load[i] += max(-normal . dir, 0) * k exp(-distance(newCoord)/screen_length)/screen_length,
+   with normal = (a, b, c) of the plane and distance its signed distance. The
+   loads of tip t are load_out[o_t .. o_t + n_mon[t]), o_t = sum of the earlier
+   tips' n_mon; capacity is the length of load_out. Loads start at zero (the
+   reference resets them in ForceFieldManager::computeLoadForces). No
+   boundary: all zero. */
+medyan_status medyan_mech_boundary_load_forces(medyan_mech* h, const medyan_load_tips* tips, double* load_out,
+                                               int64_t capacity);
+
 /* ForceFieldManager::computeHessian (src/Mechanics/ForceField/ForceFieldManager.cpp:354-398):
    the dense finite-difference Hessian at the handle's coordinates, row i
    the perturbed degree of freedom, column j the force component (caller's

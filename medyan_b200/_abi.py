@@ -125,6 +125,10 @@ class MedyanCylinders(C.Structure):
     ]
 
 
+class LoadTips(C.Structure):
+    _fields_ = [("n_tips", C.c_int32), ("cylinder", _pi), ("plus_end", _pi), ("n_mon", _pi), ("mon_size", _pd)]
+
+
 class NLParams(C.Structure):
     _fields_ = [("rmax", C.c_float), ("rmin", C.c_float), ("grid_size", C.c_double * 3)]
 

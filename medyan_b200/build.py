@@ -16,11 +16,11 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libmedyan_b200.so")
 
-SOURCES = ["capi.cu", "ff_kernels.cu", "chain.cu", "excl_kernels.cu", "nl.cu", "cg.cu", "batch.cu", "pbatch.cu", "diff.cu", "hessian.cu", "noalloc.cu"]
+SOURCES = ["capi.cu", "ff_kernels.cu", "chain.cu", "excl_kernels.cu", "nl.cu", "cg.cu", "batch.cu", "pbatch.cu", "diff.cu", "hessian.cu", "aux.cu", "noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + os.path.join(ROOT, "include"),
           "-I" + CSRC, "--expt-relaxed-constexpr"]
-PER_FILE = {"excl_kernels.cu": ["--fmad=false"]}
+PER_FILE = {"excl_kernels.cu": ["--fmad=false"], "aux.cu": ["--fmad=false"]}
 
 
 def nvcc() -> str:

@@ -272,6 +272,47 @@ __global__ void k_boundary_write(CylDev c, const double* __restrict__ x, const d
     }
 }
 
+// BoundaryCylinderRepulsion::computeLoadForces with the exponential
+// repulsion (BoundaryCylinderRepulsion.cpp:125-196, BoundaryCylinderRepulsionExp.cpp:113-118):
+// one block per tip, threads over the tip's monomer positions; planes in
+// order, each plane whose neighbor list (member[p*n + cyl] > 0, from the last
+// build) holds the tip's cylinder adds its term.
+__global__ void k_boundary_load(CylDev c, const double* __restrict__ x, const double4* __restrict__ planes,
+                                int n_planes, const int* __restrict__ member, double k, double slen, int n_tips,
+                                const int* __restrict__ tip_cyl, const int* __restrict__ tip_plus,
+                                const int* __restrict__ tip_nmon, const double* __restrict__ tip_mon,
+                                const long long* __restrict__ tip_off, double* __restrict__ out) {
+    for (int t = blockIdx.x; t < n_tips; t += gridDim.x) {
+        const int ci = tip_cyl[t];
+        const bool plus = tip_plus[t] != 0;
+        const double* bo = x + 3 * (size_t)(plus ? c.b1[ci] : c.b2[ci]);
+        const double* bd = x + 3 * (size_t)(plus ? c.b2[ci] : c.b1[ci]);
+        // normalizedVector(bd - bo)
+        const double vx = bd[0] - bo[0], vy = bd[1] - bo[1], vz = bd[2] - bo[2];
+        const double m = sqrt(vx * vx + vy * vy + vz * vz);
+        const double dir[3] = {vx / m, vy / m, vz / m};
+        const int nmon = tip_nmon[t];
+        const double mon = tip_mon[t];
+        double* o = out + tip_off[t];
+        for (int i = threadIdx.x; i < nmon; i += blockDim.x) {
+            const double s = i * mon;
+            const double p[3] = {bd[0] + s * dir[0], bd[1] + s * dir[1], bd[2] + s * dir[2]};
+            double load = 0.0;
+            for (int q = 0; q < n_planes; ++q) {
+                if (member[(size_t)q * c.n + ci] <= 0) continue;
+                const double4 pl = planes[q];
+                const double proj0 = -(pl.x * dir[0] + pl.y * dir[1] + pl.z * dir[2]);
+                const double proj = proj0 < 0.0 ? 0.0 : proj0;  // std::max(.., 0.0)
+                const double dist =
+                    (pl.x * p[0] + pl.y * p[1] + pl.z * p[2] + pl.w) / sqrt(pl.x * pl.x + pl.y * pl.y + pl.z * pl.z);
+                const double R = -dist / slen;
+                load += proj * (k * exp(R) / slen);
+            }
+            o[i] = load;
+        }
+    }
+}
+
 }  // namespace
 
 // Device buffers of one neighbor-list builder (grow-only).
@@ -287,6 +328,7 @@ struct NLBuilder {
     medyan_boundary_params bp{};
     std::vector<double> plane_host;
     bool has_boundary = false;
+    bool boundary_built = false;  // bcount holds the last build's plane membership
     int n = 0;
 
     CylDev view() const {
@@ -296,6 +338,7 @@ struct NLBuilder {
 
     cudaError_t set(const medyan_cylinders* c, cudaStream_t s) {
         n = c->n_cyl;
+        boundary_built = false;
         std::vector<int> zeros(n, 0), neg(n, -1);
         std::vector<double> dz(n, 0.0);
         cudaError_t e;
@@ -411,7 +454,9 @@ struct NLBuilder {
         h->ff.n_boundary = tot;
         h->ff.n_planes = np;
         *total = tot;
-        return cuda_status(cudaGetLastError());
+        e = cudaGetLastError();
+        boundary_built = e == cudaSuccess;
+        return cuda_status(e);
     }
 
     std::vector<double4> planes_host4() const {
@@ -571,3 +616,48 @@ medyan_status medyan_mech_get_excl_volume(medyan_mech* h, int32_t* beads_out, do
 }
 
 }  // extern "C"
+
+extern "C" medyan_status medyan_mech_boundary_load_forces(medyan_mech* h, const medyan_load_tips* tips,
+                                                          double* load_out, int64_t capacity) {
+    if (!h || !tips || tips->n_tips < 0) return MEDYAN_ERR_INVALID_ARG;
+    const int nt = tips->n_tips;
+    if (nt == 0) return MEDYAN_OK;
+    if (!tips->cylinder || !tips->plus_end || !tips->n_mon || !tips->mon_size || !load_out)
+        return MEDYAN_ERR_INVALID_ARG;
+    NLBuilder* b = reinterpret_cast<NLBuilder*>(h->nl);
+    if (!b) return MEDYAN_ERR_INVALID_ARG;  // no cylinder list: medyan_mech_set_cylinders first
+    std::vector<long long> off(nt);
+    long long tot = 0;
+    for (int t = 0; t < nt; ++t) {
+        if (tips->n_mon[t] < 0 || tips->cylinder[t] < 0 || tips->cylinder[t] >= b->n) return MEDYAN_ERR_INVALID_ARG;
+        off[t] = tot;
+        tot += tips->n_mon[t];
+    }
+    if (tot > capacity) return MEDYAN_ERR_CAPACITY;
+    if (!b->has_boundary || b->bp.n_planes <= 0) {
+        std::fill(load_out, load_out + tot, 0.0);
+        return MEDYAN_OK;
+    }
+    if (!b->boundary_built) return MEDYAN_ERR_INVALID_ARG;  // medyan_mech_rebuild_neighbors first
+    if (tot == 0) return MEDYAN_OK;
+    cudaError_t e = cudaSetDevice(h->device);
+    cudaStream_t s = h->stream;
+    DevBuf<int> cyl, plus, nmon;
+    DevBuf<double> mon, out;
+    DevBuf<long long> doff;
+    if (e == cudaSuccess) e = cyl.assign(tips->cylinder, nt, s);
+    if (e == cudaSuccess) e = plus.assign(tips->plus_end, nt, s);
+    if (e == cudaSuccess) e = nmon.assign(tips->n_mon, nt, s);
+    if (e == cudaSuccess) e = mon.assign(tips->mon_size, nt, s);
+    if (e == cudaSuccess) e = doff.assign(off.data(), nt, s);
+    if (e == cudaSuccess) e = out.reserve(tot);
+    if (e != cudaSuccess) return cuda_status(e);
+    const int g = nt < 148 * 8 ? nt : 148 * 8;
+    k_boundary_load<<<g, 128, 0, s>>>(b->view(), h->x.raw(), b->planes.raw(), b->bp.n_planes, b->bcount.raw(),
+                                      b->bp.k, b->bp.screen_length, nt, cyl.raw(), plus.raw(), nmon.raw(),
+                                      mon.raw(), doff.raw(), out.raw());
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(load_out, out.raw(), sizeof(double) * tot, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    return cuda_status(e);
+}

@@ -167,6 +167,35 @@ class ForceFieldManager:
             L.check(st, "medyan_mech_hessian")
         return H
 
+    # -- after a minimization --------------------------------------------
+    def force_magnitudes(self):
+        """ForceFieldManager::assignallforcemags inputs at the current
+        coordinates: (linker tensions k(L - l0), motor tensions, branch-point
+        forces [n_branch, 3])."""
+        sv = self._system
+        n = (sv.count("linker_beads", 4), sv.count("motor_beads", 4), sv.count("branch_beads", 4))
+        lin, mot, br = np.zeros(max(n[0], 1)), np.zeros(max(n[1], 1)), np.zeros(max(3 * n[2], 1))
+        L.check(self.lib.medyan_mech_force_magnitudes(self.handle, _dp(lin), _dp(mot), _dp(br)),
+                "medyan_mech_force_magnitudes")
+        return lin[: n[0]], mot[: n[1]], br[: 3 * n[2]].reshape(-1, 3)
+
+    def boundary_load_forces(self, cylinder, plus_end, n_mon, mon_size):
+        """BoundaryCylinderRepulsion::computeLoadForces on filament tips:
+        one array of n_mon[t] loads per tip (cylinder indices into the list
+        given to set_cylinders)."""
+        from ._abi import LoadTips
+        cyl = np.ascontiguousarray(cylinder, np.int32)
+        plus = np.ascontiguousarray(plus_end, np.int32)
+        nm = np.ascontiguousarray(n_mon, np.int32)
+        ms = f64(mon_size)
+        total = int(nm.sum())
+        out = np.zeros(max(total, 1))
+        tips = LoadTips(len(cyl), cyl.ctypes.data_as(_pi), plus.ctypes.data_as(_pi), nm.ctypes.data_as(_pi),
+                        ms.ctypes.data_as(_pd))
+        L.check(self.lib.medyan_mech_boundary_load_forces(self.handle, C.byref(tips), _dp(out), total),
+                "medyan_mech_boundary_load_forces")
+        return np.split(out[:total], np.cumsum(nm)[:-1])
+
     # -- neighbor lists ----------------------------------------------------
     def set_cylinders(self, cylinders, nl_params, boundary_params) -> None:
         self._cyl = (cylinders, nl_params, boundary_params)

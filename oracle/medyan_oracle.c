@@ -1456,3 +1456,90 @@ void oracle_hessian(const medyan_system* s, const double* x, float delta, double
     free(fp);
     free(fm);
 }
+
+/* The force magnitudes of ForceFieldManager::assignallforcemags
+   (ForceFieldManager.cpp:346-351): linker and motor stretchforce = f0/invL
+   (LinkerStretchingHarmonic.cpp:227-293, MotorGhostStretchingHarmonic.cpp:274-339),
+   and per branch point the force each enabled branching force field puts on
+   the third bead of its bead set, added in force-field order (stretching,
+   bending, dihedral, position; their forces() store f3 as stretchforce).
+   The branch value is read off each force field's forces on an otherwise
+   empty force array, which is the third bead's contribution whenever the
+   bead set's beads are distinct, as in every branch point. */
+void oracle_force_magnitudes(const medyan_system* s, const double* x, double* lin, double* mot, double* br) {
+    double v1[3], v2[3];
+    for (int pass = 0; pass < 2; ++pass) {
+        const int32_t n = pass ? s->n_motor : s->n_linker;
+        const int32_t* bs = pass ? s->motor_beads : s->linker_beads;
+        const double *k = pass ? s->motor_k : s->linker_k, *l0 = pass ? s->motor_l0 : s->linker_l0;
+        const double *p1 = pass ? s->motor_pos1 : s->linker_pos1, *p2 = pass ? s->motor_pos2 : s->linker_pos2;
+        double* out = pass ? mot : lin;
+        if (!out) continue;
+        for (int32_t i = 0; i < n; ++i) {
+            midpt(v1, x + bs[4 * i], x + bs[4 * i + 1], p1[i]);
+            midpt(v2, x + bs[4 * i + 2], x + bs[4 * i + 3], p2[i]);
+            double dist = tpd(v1, v2);
+            double invL = 1 / dist;
+            double f0 = k[i] * (dist - l0[i]) * invL;
+            out[i] = f0 / invL;
+        }
+    }
+    if (!br || s->n_branch == 0) return;
+    double* tmp = (double*)calloc(3 * (size_t)s->n_beads, sizeof(double));
+    for (int32_t i = 0; i < s->n_branch; ++i) {
+        const int32_t* b = s->branch_beads + 4 * i;
+        double acc[3] = {0.0, 0.0, 0.0};
+        for (int ffi = 0; ffi < 4; ++ffi) {
+            if (!has_br(s, ffi)) continue;
+            if (ffi == 0)
+                oracle_branch_stretch_forces(x, tmp, 1, b, s->branch_stretch_k + i, s->branch_stretch_l0 + i,
+                                             s->branch_pos + i);
+            else if (ffi == 1)
+                oracle_branch_bend_forces(x, tmp, 1, b, s->branch_bend_k + i, s->branch_bend_theta0 + i);
+            else if (ffi == 2)
+                oracle_branch_dihedral_forces(x, tmp, 1, b, s->branch_dihedral_k + i, s->branch_pos + i);
+            else
+                oracle_branch_position_forces(x, tmp, 1, b, s->branch_position_k + i, s->branch_pos + i);
+            for (int d = 0; d < 3; ++d) acc[d] += tmp[b[2] + d];
+            for (int j = 0; j < 4; ++j)
+                for (int d = 0; d < 3; ++d) tmp[b[j] + d] = 0.0;
+        }
+        for (int d = 0; d < 3; ++d) br[3 * i + d] = acc[d];
+    }
+    free(tmp);
+}
+
+/* BoundaryCylinderRepulsion::computeLoadForces with BoundaryCylinderRepulsionExp
+   (BoundaryCylinderRepulsion.cpp:125-196, BoundaryCylinderRepulsionExp.cpp:113-118):
+   the tip's cylinder is a neighbor of a plane when its midpoint lies within
+   the boundary cutoff (the boundary neighbor list, as oracle_boundary_vectorize);
+   loads of tip t at out[offset_t + i], i < n_mon[t]. */
+void oracle_boundary_load_forces(const medyan_cylinders* c, const double* x, const medyan_boundary_params* b,
+                                 int32_t n_tips, const int32_t* cyl, const int32_t* plus_end, const int32_t* n_mon,
+                                 const double* mon_size, double* out) {
+    int64_t o = 0;
+    for (int32_t t = 0; t < n_tips; ++t) {
+        const int32_t ci = cyl[t];
+        const double* bo = x + 3 * (int64_t)(plus_end[t] ? c->bead1[ci] : c->bead2[ci]);
+        const double* bd = x + 3 * (int64_t)(plus_end[t] ? c->bead2[ci] : c->bead1[ci]);
+        double v[3] = {bd[0] - bo[0], bd[1] - bo[1], bd[2] - bo[2]};
+        double m = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        double dir[3] = {v[0] / m, v[1] / m, v[2] / m};
+        for (int32_t i = 0; i < n_mon[t]; ++i) out[o + i] = 0.0;
+        double mid[3];
+        midpt(mid, x + 3 * (int64_t)c->bead1[ci], x + 3 * (int64_t)c->bead2[ci], 0.5);
+        for (int32_t p = 0; p < b->n_planes; ++p) {
+            const double* pl = b->plane_eq + 4 * p;
+            if (!(plane_distance(pl, mid) < (double)b->cutoff)) continue;
+            for (int32_t i = 0; i < n_mon[t]; ++i) {
+                double sft = i * mon_size[t];
+                double nc[3] = {bd[0] + sft * dir[0], bd[1] + sft * dir[1], bd[2] + sft * dir[2]};
+                double proj = -(pl[0] * dir[0] + pl[1] * dir[1] + pl[2] * dir[2]);
+                if (proj < 0.0) proj = 0.0;
+                double R = -plane_distance(pl, nc) / b->screen_length;
+                out[o + i] += proj * (b->k * exp(R) / b->screen_length);
+            }
+        }
+        o += n_mon[t];
+    }
+}

@@ -51,6 +51,12 @@ void oracle_boundary_forces(const double* x, double* f, const medyan_system* s);
 /* ForceFieldManager semantics. */
 double oracle_energy(const medyan_system* s, const double* x, double* e_per_ff);
 void oracle_forces(const medyan_system* s, const double* x, double* f);
+/* ForceFieldManager::assignallforcemags inputs: linker/motor tensions, branch-point forces (3 per branch). */
+void oracle_force_magnitudes(const medyan_system* s, const double* x, double* lin, double* mot, double* br);
+/* BoundaryCylinderRepulsion::computeLoadForces on filament tips. */
+void oracle_boundary_load_forces(const medyan_cylinders* c, const double* x, const medyan_boundary_params* b,
+                                 int32_t n_tips, const int32_t* cyl, const int32_t* plus_end, const int32_t* n_mon,
+                                 const double* mon_size, double* out);
 /* ForceFieldManager::computeHessian: dense FD Hessian, row-major 3N x 3N. */
 void oracle_hessian(const medyan_system* s, const double* x, float delta, double* H);
 

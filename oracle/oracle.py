@@ -57,6 +57,10 @@ class Oracle:
         L.oracle_excl_vectorize.argtypes = [C.c_void_p, _pi, C.c_int64, _pi, _pd, _pd]
         L.oracle_boundary_vectorize.restype = C.c_int64
         L.oracle_boundary_vectorize.argtypes = [C.c_void_p, _pd, C.c_void_p, _pi, _pd, _pd, _pi]
+        L.oracle_force_magnitudes.restype = None
+        L.oracle_force_magnitudes.argtypes = [C.c_void_p, _pd, _pd, _pd, _pd]
+        L.oracle_boundary_load_forces.restype = None
+        L.oracle_boundary_load_forces.argtypes = [C.c_void_p, _pd, C.c_void_p, C.c_int32, _pi, _pi, _pi, _pd, _pd]
         L.oracle_hessian.restype = None
         L.oracle_hessian.argtypes = [C.c_void_p, _pd, C.c_float, _pd]
         L.oracle_excl_pair_energy.restype = C.c_double
@@ -81,6 +85,24 @@ class Oracle:
         r = MinResult()
         st = self.lib.oracle_cg_minimize(sv.ref(), C.byref(params), _dp(x), _dp(f), C.byref(r))
         return st, x, f, r
+
+    def force_magnitudes(self, sv: SystemView, x: np.ndarray):
+        x = f64(x)
+        nl, nm, nb = sv.count("linker_beads", 4), sv.count("motor_beads", 4), sv.count("branch_beads", 4)
+        lin, mot, br = np.zeros(max(nl, 1)), np.zeros(max(nm, 1)), np.zeros(max(3 * nb, 1))
+        self.lib.oracle_force_magnitudes(sv.ref(), _dp(x), _dp(lin), _dp(mot), _dp(br))
+        return lin[:nl], mot[:nm], br[: 3 * nb].reshape(-1, 3)
+
+    def boundary_load_forces(self, cyl_view, x, bparams, cylinder, plus_end, n_mon, mon_size):
+        x = f64(x)
+        cyl = i32(cylinder)
+        plus = i32(plus_end)
+        nm = i32(n_mon)
+        ms = f64(mon_size)
+        out = np.zeros(max(int(nm.sum()), 1))
+        self.lib.oracle_boundary_load_forces(cyl_view.ref(), _dp(x), C.byref(bparams), len(cyl), _ip(cyl), _ip(plus),
+                                             _ip(nm), _dp(ms), _dp(out))
+        return np.split(out[: int(nm.sum())], np.cumsum(nm)[:-1])
 
     def hessian(self, sv: SystemView, x: np.ndarray, delta: float) -> np.ndarray:
         x = f64(x)
