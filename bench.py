@@ -139,6 +139,9 @@ def run_ours(args, rank: int, world: int) -> dict:
         ff.set_cylinders(net.cylinders_view(), net.nl_params(), bp)
         ff.rebuild_neighbor_lists()
         ff.lib.medyan_mech_synchronize(ff.handle)
+        # block and tile shapes per potential for this network (autotuner,
+        # at setup, outside every timed region)
+        ff.tuned_shapes = ff.autotune(reps=10)
         return ff
 
     ff = make(args.precision)
@@ -253,6 +256,7 @@ def run_ours(args, rank: int, world: int) -> dict:
         "dtype": "f32+f64" if args.precision == "mixed" else "f64",
         "data": "synthetic (seeded network generator, reference initializer rules)",
         "config": {"workload": WORKLOAD, "precision": args.precision, "n_beads": net.n_beads,
+                   "launch_shapes": ff.tuned_shapes,
                    "interactions": counts, "l2": "flushed (256 MiB write) before each timed step",
                    "step": "total energy + forces of all force fields", "parallelism": f"replicas x{world}"},
         "e2e": {"value": world * K / e2e_t, "unit": "force-evals/s", "h2d_bytes_per_step": 8 * x.size,
@@ -341,6 +345,7 @@ def batch_extras(n_replicas: int = 256) -> dict:
             for r, net in enumerate(nets):
                 bp, _ = net.boundary_params()
                 b.rebuild_neighbor_lists(r, xs[r], net.cylinders_view(), net.nl_params(), bp)
+            shapes = b.autotune(reps=3)
             b.minimize(xs, warm)
             torch.cuda.synchronize()
             t0 = time.perf_counter()
@@ -363,7 +368,8 @@ def batch_extras(n_replicas: int = 256) -> dict:
         its = [r.num_iter for r in rs]
         out[prec] = {"seconds": dt, "minimizations_per_s": n_replicas / dt,
                      "one_at_a_time_minimizations_per_s": m / seq, "iterations_mean": float(np.mean(its)),
-                     "iterations_max": int(max(its)), "statuses": sorted(set(int(v) for v in st))}
+                     "iterations_max": int(max(its)), "statuses": sorted(set(int(v) for v in st)),
+                     "launch_shapes": shapes}
     return out
 
 

@@ -362,6 +362,34 @@ medyan_status medyan_mech_param_grad(medyan_mech* h, int32_t ff, const double* v
    float forces). */
 medyan_status medyan_mech_hvp(medyan_mech* h, const double* v, double* hv);
 
+/* ---- launch shapes and the autotuner (no counterpart in the reference,
+   whose kernels run on the CPU) ----
+   Block and tile shapes per potential. Every shape gives the same physics;
+   the energy reduction tree, and so the last bits of the energies, depend on
+   the shape (deterministic for a given shape). */
+typedef struct medyan_launch_shapes {
+    int32_t bonded_threads;         /* records (= threads) per block of the bonded
+                                       potentials (linker, motor, branching,
+                                       boundary, leftover filament terms): 128, 256, 512 */
+    int32_t excl_threads;           /* pairs (= threads) per block of the
+                                       excluded-volume kernels: 32, 64, 128 */
+    int32_t chain_threads;          /* threads per block of the filament-chain
+                                       force kernel (30 beads per warp): 128, 256, 512 */
+    int32_t chain_energy_blocks_per_sm; /* fixed grid of the filament-chain energy
+                                       kernel, in blocks of 256 per SM: 2, 4, 8 */
+} medyan_launch_shapes;
+
+/* The defaults are 256, 64, 256, 4. Setting shapes re-derives the block
+   tables and invalidates the handle's captured passes (rebuilt on next use). */
+medyan_status medyan_mech_set_shapes(medyan_mech* h, const medyan_launch_shapes* shapes);
+medyan_status medyan_mech_get_shapes(medyan_mech* h, medyan_launch_shapes* shapes);
+/* Picks the shapes for this handle's network: coordinate descent over the
+   four fields above (each candidate timed as the mean of `reps` evaluate
+   passes after two warm-up passes, CUDA events on the handle's stream, at
+   the handle's current coordinates), keeps the fastest and reports it in
+   *chosen (may be null). */
+medyan_status medyan_mech_autotune(medyan_mech* h, int32_t reps, medyan_launch_shapes* chosen);
+
 /* ---- after a minimization: inputs of the chemical rate changers ----
    MController::afterMinimization_ (src/Controller/MController.h:238-268)
    runs ffm.assignallforcemags() and ffm.computeAuxParams(), whose
@@ -451,6 +479,22 @@ medyan_status medyan_batch_minimize(medyan_batch* b, const medyan_cg_params* p, 
 /* Energy and forces of every replica (e_totals: double[n]). */
 medyan_status medyan_batch_evaluate(medyan_batch* b, const double* const* coords, double* e_totals,
                                     double* const* forces_out);
+
+/* Shapes of a batch's packed layout (each replica's records are padded to
+   whole blocks, so small replicas favour small blocks). Defaults 256, 64,
+   256, 256. Setting them repacks on the next batched call. */
+typedef struct medyan_batch_shapes {
+    int32_t bonded_threads;         /* 128, 256, 512 */
+    int32_t excl_threads;           /* 32, 64, 128 */
+    int32_t chain_threads;          /* 128, 256, 512 */
+    int32_t chain_chunk;            /* positions per chain-energy block: 256, 512, 1024 */
+} medyan_batch_shapes;
+medyan_status medyan_batch_set_shapes(medyan_batch* b, const medyan_batch_shapes* shapes);
+medyan_status medyan_batch_get_shapes(medyan_batch* b, medyan_batch_shapes* shapes);
+/* Coordinate descent over the four fields, each candidate timed as the mean
+   of `reps` packed evaluate passes (energy and forces of every replica at
+   its handle's current coordinates); keeps the fastest. */
+medyan_status medyan_batch_autotune(medyan_batch* b, int32_t reps, medyan_batch_shapes* chosen);
 
 /* ------------------------------------------------------------------------ */
 /* Excluded-volume energy without device allocation                          */

@@ -125,6 +125,22 @@ class MedyanCylinders(C.Structure):
     ]
 
 
+class LaunchShapes(C.Structure):
+    _fields_ = [("bonded_threads", C.c_int32), ("excl_threads", C.c_int32), ("chain_threads", C.c_int32),
+                ("chain_energy_blocks_per_sm", C.c_int32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class BatchShapes(C.Structure):
+    _fields_ = [("bonded_threads", C.c_int32), ("excl_threads", C.c_int32), ("chain_threads", C.c_int32),
+                ("chain_chunk", C.c_int32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class LoadTips(C.Structure):
     _fields_ = [("n_tips", C.c_int32), ("cylinder", _pi), ("plus_end", _pi), ("n_mon", _pi), ("mon_size", _pd)]
 

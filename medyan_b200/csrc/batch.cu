@@ -119,6 +119,81 @@ medyan_status medyan_batch_minimize(medyan_batch* b, const medyan_cg_params* p, 
     return worst;
 }
 
+static bool in3(int v, int a, int b, int c) { return v == a || v == b || v == c; }
+
+medyan_status medyan_batch_set_shapes(medyan_batch* b, const medyan_batch_shapes* sh) {
+    if (!b || !sh) return MEDYAN_ERR_INVALID_ARG;
+    if (!in3(sh->bonded_threads, 128, 256, 512) || !in3(sh->excl_threads, 32, 64, 128) ||
+        !in3(sh->chain_threads, 128, 256, 512) || !in3(sh->chain_chunk, 256, 512, 1024))
+        return MEDYAN_ERR_INVALID_ARG;
+    PackedBatch& pb = b->pb;
+    if (pb.stream) {
+        cudaError_t e = cudaStreamSynchronize(pb.stream);
+        if (e != cudaSuccess) return cuda_status(e);
+    }
+    pb.bonded_block = sh->bonded_threads;
+    pb.excl_block = sh->excl_threads;
+    pb.chain_threads = sh->chain_threads;
+    pb.chain_chunk = sh->chain_chunk;
+    pb.repack = true;
+    if (pb.graph) {  // captured with the old layout
+        cudaGraphExecDestroy(pb.graph);
+        pb.graph = nullptr;
+    }
+    return MEDYAN_OK;
+}
+
+medyan_status medyan_batch_get_shapes(medyan_batch* b, medyan_batch_shapes* sh) {
+    if (!b || !sh) return MEDYAN_ERR_INVALID_ARG;
+    const PackedBatch& pb = b->pb;
+    *sh = medyan_batch_shapes{pb.bonded_block, pb.excl_block, pb.chain_threads, pb.chain_chunk};
+    return MEDYAN_OK;
+}
+
+medyan_status medyan_batch_autotune(medyan_batch* b, int32_t reps, medyan_batch_shapes* chosen) {
+    if (!b || reps <= 0) return MEDYAN_ERR_INVALID_ARG;
+    if (b->h.empty()) return MEDYAN_OK;
+    PackedBatch& pb = b->pb;
+    const int prec = b->h[0]->prec;
+    // pack with the given shapes, take each replica's current coordinates, time
+    auto trial = [&](const medyan_batch_shapes& sh, float* ms) -> medyan_status {
+        medyan_status st = medyan_batch_set_shapes(b, &sh);
+        if (st == MEDYAN_OK) st = pack_batch(pb, b->h);
+        if (st != MEDYAN_OK) return st;
+        for (size_t r = 0; r < b->h.size(); ++r) {
+            const medyan_mech* h = b->h[r];
+            if (!h->n_beads) continue;
+            cudaError_t e = cudaMemcpyAsync(pb.x.raw() + 3 * (size_t)pb.base[r], h->x.raw(),
+                                            sizeof(double) * 3 * (size_t)h->n_beads, cudaMemcpyDeviceToDevice,
+                                            pb.stream);
+            if (e != cudaSuccess) return cuda_status(e);
+        }
+        return cg_batch_time_evaluate(pb, prec, reps, ms);
+    };
+    medyan_batch_shapes best{};
+    medyan_status st = medyan_batch_get_shapes(b, &best);
+    float best_ms = 0.0f;
+    if (st == MEDYAN_OK) st = trial(best, &best_ms);
+    const int sets[4][3] = {{128, 256, 512}, {32, 64, 128}, {128, 256, 512}, {256, 512, 1024}};
+    for (int f = 0; f < 4 && st == MEDYAN_OK; ++f) {
+        for (int c = 0; c < 3 && st == MEDYAN_OK; ++c) {
+            medyan_batch_shapes t = best;
+            int32_t* field[4] = {&t.bonded_threads, &t.excl_threads, &t.chain_threads, &t.chain_chunk};
+            if (*field[f] == sets[f][c]) continue;
+            *field[f] = sets[f][c];
+            float ms = 0.0f;
+            st = trial(t, &ms);
+            if (st == MEDYAN_OK && ms < best_ms) {
+                best_ms = ms;
+                best = t;
+            }
+        }
+    }
+    if (st == MEDYAN_OK) st = medyan_batch_set_shapes(b, &best);
+    if (st == MEDYAN_OK && chosen) *chosen = best;
+    return st;
+}
+
 medyan_status medyan_batch_evaluate(medyan_batch* b, const double* const* coords, double* e_totals,
                                     double* const* forces_out) {
     if (!b || (!b->h.empty() && (!coords || !e_totals || !forces_out))) return MEDYAN_ERR_INVALID_ARG;

@@ -254,7 +254,8 @@ medyan_status refresh_device_ff(medyan_mech* h) {
     h->chain.bend_p = h->chain_bend_p.raw();
     const int counts[6] = {ff.n_stretch, ff.n_bend, ff.n_linker, ff.n_motor, ff.n_branch, ff.n_boundary};
     ff.seg[0] = 0;
-    for (int q = 0; q < 6; ++q) ff.seg[q + 1] = ff.seg[q] + (counts[q] + kBlock - 1) / kBlock;
+    const int bb = bonded_block_of(ff);
+    for (int q = 0; q < 6; ++q) ff.seg[q + 1] = ff.seg[q] + (counts[q] + bb - 1) / bb;
     h->es.n_blocks_chain = h->chain.n_pos > 0 ? chain_blocks(h->chain) : 0;
     h->es.n_blocks_bonded = ff.seg[6];
     h->es.n_blocks_excl = excl_blocks(ff);

@@ -1113,6 +1113,49 @@ cudaError_t b_build_graph(PackedBatch& pb, int prec, cudaGraphExec_t* exec) {
 
 }  // namespace
 
+medyan_status cg_batch_time_evaluate(PackedBatch& pb, int prec, int reps, float* ms) {
+    const int R = pb.R;
+    if (R == 0 || reps <= 0) return MEDYAN_ERR_INVALID_ARG;
+    const size_t n3 = 3 * (size_t)pb.nb;
+    cudaStream_t s = pb.stream;
+    cudaError_t e = pb.fnew.reserve(n3 ? n3 : 1);
+    if (e == cudaSuccess) e = pb.out.reserve((size_t)R * kMaxLambda * kOut);
+    LambdaSet z{};
+    z.K = 1;
+    if (e == cudaSuccess) e = pb.Lzero.assign(&z, 1, s);
+    if (e != cudaSuccess) return cuda_status(e);
+    const ForceTarget t{pb.fnew.raw(), nullptr, nullptr, nullptr, nullptr, nullptr};
+    auto pass = [&] {
+        b_energy_pass(pb, nullptr, pb.Lzero.raw(), s);
+        // the CG's decide step clears the fallback queue; do it here
+        cudaMemsetAsync(pb.es.fb_count, 0, sizeof(int), s);
+        cudaMemsetAsync(pb.es.bad, 0, sizeof(int) * kMaxLambda, s);
+        launch_forces(pb.ch, pb.ff, prec, pb.x.raw(), t, pb.fs, s, &pb.fork);
+    };
+    k_b_act_all<<<(R + 255) / 256, 256, 0, s>>>(R, pb.act.raw());
+    pass();
+    pass();
+    cudaEvent_t a = nullptr, b = nullptr;
+    e = cudaEventCreate(&a);
+    if (e == cudaSuccess) e = cudaEventCreate(&b);
+    if (e == cudaSuccess) e = cudaEventRecord(a, s);
+    for (int i = 0; i < reps && e == cudaSuccess; ++i) {
+        pass();
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(b, s);
+    if (e == cudaSuccess) e = cudaEventSynchronize(b);
+    float t_ms = 0.0f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&t_ms, a, b);
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+    if (e == cudaSuccess) e = cudaMemsetAsync(pb.fs.status, 0, sizeof(int), s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_status(e);
+    *ms = t_ms / (float)reps;
+    return MEDYAN_OK;
+}
+
 // Batched CGMethod::minimize over the packed replicas; see the kernels above.
 medyan_status cg_batch_run(PackedBatch& pb, int prec, const medyan_cg_params* p) {
     const int R = pb.R;

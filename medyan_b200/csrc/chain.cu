@@ -68,7 +68,7 @@ __device__ __forceinline__ V3 pos_of(const double* __restrict__ x, int n, int q)
 // position from their neighbours by shuffles. No shared memory, no block
 // barriers; every position is written exactly once.
 template <class R>
-__global__ void __launch_bounds__(kThreads) k_chain_forces(const ChainDev ch, const double* __restrict__ x,
+__global__ void __launch_bounds__(kMaxShapeThreads) k_chain_forces(const ChainDev ch, const double* __restrict__ x,
                                                            const ForceTarget tgt) {
     if (tgt.skip && *tgt.skip) return;
     double* __restrict__ f = target_force(tgt);
@@ -218,21 +218,23 @@ int reorder_blocks(int n3) {
 }  // namespace
 
 int chain_blocks(const ChainDev& ch) {
-    // energy: one 32-position tile per warp, at most 4 blocks per SM
+    // energy: one 32-position tile per warp, at most energy_blocks_per_sm
+    // blocks per SM (4 by default)
     const int per_block = 32 * (kThreads / 32);
     const int b = (ch.n_pos + per_block - 1) / per_block;
-    const int cap = 148 * 4;
+    const int cap = 148 * (ch.energy_blocks_per_sm > 0 ? ch.energy_blocks_per_sm : 4);
     return b < 1 ? 1 : (b < cap ? b : cap);
 }
 
 void launch_chain_forces(const ChainDev& ch, int prec, const double* x, const ForceTarget& t, cudaStream_t s) {
     if (ch.n_pos <= 0) return;
-    const int per_block = kWarpOut * (kThreads / 32);
+    const int threads = ch.force_threads > 0 ? ch.force_threads : kThreads;
+    const int per_block = kWarpOut * (threads / 32);
     const int g = (ch.n_pos + per_block - 1) / per_block;
     if (prec == MEDYAN_PREC_MIXED)
-        k_chain_forces<float><<<g, kThreads, 0, s>>>(ch, x, t);
+        k_chain_forces<float><<<g, threads, 0, s>>>(ch, x, t);
     else
-        k_chain_forces<double><<<g, kThreads, 0, s>>>(ch, x, t);
+        k_chain_forces<double><<<g, threads, 0, s>>>(ch, x, t);
 }
 
 void launch_chain_energy(const ChainDev& ch, int prec, const double* x, const double* d, const LambdaSet* lam,

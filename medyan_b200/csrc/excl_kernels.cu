@@ -19,10 +19,12 @@ namespace mb {
 
 namespace {
 
+constexpr int kMaxExclThreads = 128;  // largest tunable excluded-volume block
+
 __device__ __forceinline__ V3 at(const V3& x, const V3& d, double lam, bool move) { return move ? move3(x, lam, d) : x; }
 
 template <class R, bool MOVE>
-__global__ void __launch_bounds__(kExclBlock) k_excl_energy(const DeviceFF ff, const double* __restrict__ x,
+__global__ void __launch_bounds__(kMaxExclThreads) k_excl_energy(const DeviceFF ff, const double* __restrict__ x,
                                                             const double* __restrict__ d,
                                                             const LambdaSet* __restrict__ lset,
                                                             double* __restrict__ partial, int nblk_total,
@@ -30,7 +32,7 @@ __global__ void __launch_bounds__(kExclBlock) k_excl_energy(const DeviceFF ff, c
                                                             int2* __restrict__ fb_list, int* __restrict__ bad) {
     __shared__ double smem[4 * 32];
     if (ff.act && !ff.act[ff.rep_excl[blockIdx.x]]) return;  // batched: replica not in this pass
-    const int i = blockIdx.x * kExclBlock + threadIdx.x;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool move = MOVE;
     bool valid = i < ff.n_excl;
     V3 X[4] = {}, D[4] = {};
@@ -76,12 +78,12 @@ __device__ __forceinline__ V3 pos_at(const double* __restrict__ x, const ForceTa
 }
 
 template <class R>
-__global__ void __launch_bounds__(kExclBlock) k_excl_forces(const DeviceFF ff, const double* __restrict__ x,
+__global__ void __launch_bounds__(kMaxExclThreads) k_excl_forces(const DeviceFF ff, const double* __restrict__ x,
                                                             const ForceTarget tgt, int* __restrict__ fb_count,
                                                             int* __restrict__ fb_list, int* __restrict__ status) {
     if (tgt.skip && *tgt.skip) return;
     if (ff.act && !ff.act[ff.rep_excl[blockIdx.x]]) return;  // batched: replica not in this pass
-    const int i = blockIdx.x * kExclBlock + threadIdx.x;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= ff.n_excl) return;
     double* __restrict__ f = target_force(tgt);
     const double lam = tgt.lam ? *tgt.lam : 0.0;
@@ -578,11 +580,11 @@ void launch_excl_energy(const DeviceFF& ff, int prec, const double* x, const dou
     // arctangents, JJ = -(triple product)^2) loses ~1e-6 relative in float.
     (void)prec;
     if (d)
-        k_excl_energy<double, true><<<nbe, kExclBlock, 0, s>>>(ff, x, d, lam, es.partial, total,
+        k_excl_energy<double, true><<<nbe, excl_block_of(ff), 0, s>>>(ff, x, d, lam, es.partial, total,
                                                      es.n_blocks_chain + es.n_blocks_bonded, es.fb_count, es.fb_list,
                                                      es.bad);
     else
-        k_excl_energy<double, false><<<nbe, kExclBlock, 0, s>>>(ff, x, d, lam, es.partial, total,
+        k_excl_energy<double, false><<<nbe, excl_block_of(ff), 0, s>>>(ff, x, d, lam, es.partial, total,
                                                      es.n_blocks_chain + es.n_blocks_bonded, es.fb_count, es.fb_list,
                                                      es.bad);
 }
@@ -600,7 +602,7 @@ void launch_excl_forces(const DeviceFF& ff, int prec, const double* x, const For
     const int nbe = excl_blocks(ff);
     if (nbe <= 0) return;
     (void)prec;  // FP64 in both modes, as for the energy
-    k_excl_forces<double><<<nbe, kExclBlock, 0, s>>>(ff, x, t, fs.fb_count, fs.fb_list, fs.status);
+    k_excl_forces<double><<<nbe, excl_block_of(ff), 0, s>>>(ff, x, t, fs.fb_count, fs.fb_list, fs.status);
     k_excl_force_fallback<<<1, kBlock, 0, s>>>(ff, x, t, fs.fb_count, fs.fb_list, fs.status);
 }
 

@@ -34,7 +34,7 @@ __device__ constexpr bool has_seg(int c) { return S0 <= c && c < S1; }
 __device__ __forceinline__ V3 at(const V3& x, const V3& d, double lam, bool move) { return move ? move3(x, lam, d) : x; }
 
 template <class R, int S0, int S1>
-__global__ void __launch_bounds__(kBlock) k_bonded_energy(const DeviceFF ff, const double* __restrict__ x,
+__global__ void __launch_bounds__(kMaxShapeThreads) k_bonded_energy(const DeviceFF ff, const double* __restrict__ x,
                                                           const double* __restrict__ d,
                                                           const LambdaSet* __restrict__ lset,
                                                           double* __restrict__ partial, int nblk_total, int blk_off) {
@@ -42,7 +42,7 @@ __global__ void __launch_bounds__(kBlock) k_bonded_energy(const DeviceFF ff, con
     const int b = blockIdx.x + ff.seg[S0];
     if (ff.act && !ff.act[ff.rep_bonded[b]]) return;  // batched: replica not in this pass
     const int s = segment_of<S0, S1>(ff, b);
-    const int i = (b - ff.seg[s]) * kBlock + threadIdx.x;
+    const int i = (b - ff.seg[s]) * blockDim.x + threadIdx.x;
     const bool move = d != nullptr;
     V3 X[4] = {}, D[4] = {};
     double4 pa = {}, pb = {};
@@ -181,7 +181,7 @@ struct PosLoader {
 };
 
 template <class R, int S0, int S1>
-__global__ void __launch_bounds__(kBlock) k_bonded_forces(const DeviceFF ff, const double* __restrict__ x,
+__global__ void __launch_bounds__(kMaxShapeThreads) k_bonded_forces(const DeviceFF ff, const double* __restrict__ x,
                                                           const ForceTarget tgt) {
     if (tgt.skip && *tgt.skip) return;
     double* __restrict__ f = target_force(tgt);
@@ -189,7 +189,7 @@ __global__ void __launch_bounds__(kBlock) k_bonded_forces(const DeviceFF ff, con
     const int b = blockIdx.x + ff.seg[S0];
     if (ff.act && !ff.act[ff.rep_bonded[b]]) return;  // batched: replica not in this pass
     const int s = segment_of<S0, S1>(ff, b);
-    const int i = (b - ff.seg[s]) * kBlock + threadIdx.x;
+    const int i = (b - ff.seg[s]) * blockDim.x + threadIdx.x;
     switch (s) {
         case 0:
             if (has_seg<S0, S1>(0) && i < ff.n_stretch) {
@@ -300,7 +300,7 @@ void bonded_energy_group(const DeviceFF& ff, const double* x, const double* d, c
                          const EnergyScratch& es, cudaStream_t s) {
     const int nb = ff.seg[S1] - ff.seg[S0];
     if (nb > 0)
-        k_bonded_energy<double, S0, S1><<<nb, kBlock, 0, s>>>(ff, x, d, lam, es.partial, es.total(),
+        k_bonded_energy<double, S0, S1><<<nb, bonded_block_of(ff), 0, s>>>(ff, x, d, lam, es.partial, es.total(),
                                                                es.n_blocks_chain);
 }
 
@@ -309,9 +309,9 @@ void bonded_forces_group(const DeviceFF& ff, int prec, const double* x, const Fo
     const int nb = ff.seg[S1] - ff.seg[S0];
     if (nb <= 0) return;
     if (prec == MEDYAN_PREC_MIXED)
-        k_bonded_forces<float, S0, S1><<<nb, kBlock, 0, s>>>(ff, x, t);
+        k_bonded_forces<float, S0, S1><<<nb, bonded_block_of(ff), 0, s>>>(ff, x, t);
     else
-        k_bonded_forces<double, S0, S1><<<nb, kBlock, 0, s>>>(ff, x, t);
+        k_bonded_forces<double, S0, S1><<<nb, bonded_block_of(ff), 0, s>>>(ff, x, t);
 }
 
 void fork_to(const Fork* fk, cudaStream_t s, int n) {

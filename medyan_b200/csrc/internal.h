@@ -39,6 +39,10 @@ struct DeviceFF {
     const int* act;
     const int* rep_bonded;
     const int* rep_excl;
+    // launch shapes (0: the defaults kBlock / kExclBlock): interaction
+    // records (= threads) per block of the bonded and excluded-volume kernels
+    int bonded_block;
+    int excl_block;
 };
 
 // Filament chains (chain.cu) over the internal bead order: chain position p
@@ -52,6 +56,10 @@ struct ChainDev {
     // pass's active mask; positions of inactive replicas are not written
     const int* rep;
     const int* act;
+    // launch shapes (0: defaults): threads per block of the force kernel,
+    // blocks per SM of the energy kernel's fixed grid
+    int force_threads;
+    int energy_blocks_per_sm;
 };
 
 struct ChainHost {
@@ -169,6 +177,9 @@ cudaError_t init_excl_kernels();
 int bonded_blocks(const DeviceFF& ff);
 constexpr int kFinishBlocks = 8;  // blocks of the split energy finish
 constexpr int kExclBlock = 64;  // small blocks: the pair count is low and each pair is heavy
-inline int excl_blocks(const DeviceFF& ff) { return (ff.n_excl + kExclBlock - 1) / kExclBlock; }
+inline int excl_block_of(const DeviceFF& ff) { return ff.excl_block > 0 ? ff.excl_block : kExclBlock; }
+inline int bonded_block_of(const DeviceFF& ff) { return ff.bonded_block > 0 ? ff.bonded_block : kBlock; }
+inline int excl_blocks(const DeviceFF& ff) { return (ff.n_excl + excl_block_of(ff) - 1) / excl_block_of(ff); }
+constexpr int kMaxShapeThreads = 512;  // largest block any tunable kernel is launched with
 
 }  // namespace mb

@@ -57,7 +57,7 @@ medyan_status pack_batch(PackedBatch& pb, const std::vector<medyan_mech*>& h) {
     const int R = (int)h.size();
     long long gen = 0;
     for (auto* r : h) gen += r->ff_gen;
-    if (pb.R == R && pb.gen == gen && (int)pb.base.size() == R + 1) return MEDYAN_OK;
+    if (!pb.repack && pb.R == R && pb.gen == gen && (int)pb.base.size() == R + 1) return MEDYAN_OK;
     cudaError_t e = cudaSuccess;
     if (!pb.stream) {
         e = cudaStreamCreateWithFlags(&pb.stream, cudaStreamNonBlocking);
@@ -98,7 +98,7 @@ medyan_status pack_batch(PackedBatch& pb, const std::vector<medyan_mech*>& h) {
         const int n[S_N] = {f.n_stretch, f.n_bend, f.n_linker, f.n_motor, f.n_branch, f.n_boundary, f.n_excl};
         for (int k = 0; k < S_N; ++k) {
             cnt[k][r] = n[k];
-            off[k][r + 1] = off[k][r] + pad_to(n[k], k == S_EXCL ? kExclBlock : kBlock);
+            off[k][r + 1] = off[k][r] + pad_to(n[k], k == S_EXCL ? pb.excl_block : pb.bonded_block);
         }
     }
     for (int k = 0; k < S_N; ++k) tot[k] = off[k][R];
@@ -211,8 +211,12 @@ medyan_status pack_batch(PackedBatch& pb, const std::vector<medyan_mech*>& h) {
     ff.planes = pb.planes.raw();
     const int counts[6] = {ff.n_stretch, ff.n_bend, ff.n_linker, ff.n_motor, ff.n_branch, ff.n_boundary};
     ff.seg[0] = 0;
-    for (int q = 0; q < 6; ++q) ff.seg[q + 1] = ff.seg[q] + (counts[q] + kBlock - 1) / kBlock;
+    const int B = pb.bonded_block, X = pb.excl_block, P = pb.chain_chunk;
+    ff.bonded_block = B;
+    ff.excl_block = X;
+    for (int q = 0; q < 6; ++q) ff.seg[q + 1] = ff.seg[q] + (counts[q] + B - 1) / B;
     pb.ch = ChainDev{nb, pb.flags.raw(), pb.link_p.raw(), pb.bend_p.raw()};
+    pb.ch.force_threads = pb.chain_threads;
 
     // chain energy chunks and per-replica row ranges
     std::vector<int4> table;
@@ -224,16 +228,16 @@ medyan_status pack_batch(PackedBatch& pb, const std::vector<medyan_mech*>& h) {
     const int seg_of[6] = {S_STRETCH, S_BEND, S_LINKER, S_MOTOR, S_BRANCH, S_BOUNDARY};
     for (int r = 0; r <= R; ++r) {
         rc[r] = (int)table.size();
-        for (int q = 0; q < 6; ++q) rs[q * (R + 1) + r] = ff.seg[q] + off[seg_of[q]][r] / kBlock;
-        re[r] = off[S_EXCL][r] / kExclBlock;
+        for (int q = 0; q < 6; ++q) rs[q * (R + 1) + r] = ff.seg[q] + off[seg_of[q]][r] / B;
+        re[r] = off[S_EXCL][r] / X;
         rp[r] = off[S_EXCL][r];
         if (r == R) break;
-        for (int p0 = pb.base[r]; p0 < pb.base[r + 1]; p0 += 256)
-            table.push_back(make_int4(r, p0, p0 + 256 < pb.base[r + 1] ? p0 + 256 : pb.base[r + 1], 0));
+        for (int p0 = pb.base[r]; p0 < pb.base[r + 1]; p0 += P)
+            table.push_back(make_int4(r, p0, p0 + P < pb.base[r + 1] ? p0 + P : pb.base[r + 1], 0));
     }
     pb.n_chain_blocks = (int)table.size();
     // replica of every position, bonded block and excluded-volume block
-    std::vector<int> rb(nb), rbb(ff.seg[6] > 0 ? ff.seg[6] : 1, 0), rbe(tot[S_EXCL] / kExclBlock + 1, 0);
+    std::vector<int> rb(nb), rbb(ff.seg[6] > 0 ? ff.seg[6] : 1, 0), rbe(tot[S_EXCL] / X + 1, 0);
     for (int r = 0; r < R; ++r) {
         for (int p = pb.base[r]; p < pb.base[r + 1]; ++p) rb[p] = r;
         for (int q = 0; q < 6; ++q)
@@ -285,6 +289,7 @@ medyan_status pack_batch(PackedBatch& pb, const std::vector<medyan_mech*>& h) {
     e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_status(e);
     pb.gen = gen;
+    pb.repack = false;
     return MEDYAN_OK;
 }
 

@@ -37,6 +37,12 @@ struct PackedBatch {
     DevBuf<double2> boundary_p;
     DeviceFF ff{};
     ChainDev ch{};
+    // launch shapes of the packed layout (medyan_batch_set_shapes): records
+    // per bonded block and pairs per excluded-volume block (each replica's
+    // records are padded to whole blocks), chain force threads per block,
+    // positions per chain energy block
+    int bonded_block = kBlock, excl_block = kExclBlock, chain_threads = 256, chain_chunk = 256;
+    bool repack = false;  // shapes changed since the last packing
 
     // per-replica block and row tables
     DevBuf<int4> chain_table;         // chain energy block -> (replica, first, end position)
@@ -78,5 +84,8 @@ medyan_status pack_batch(PackedBatch& pb, const std::vector<medyan_mech*>& h);
 // Runs one batched minimization on the packed arrays (coordinates already in
 // pb.x); results stay on the device (pb.x, pb.fcur, pb.st, pb.eout).
 medyan_status cg_batch_run(PackedBatch& pb, int prec, const medyan_cg_params* p);
+// Mean time (ms) of one packed evaluate (energy and forces of every replica
+// at pb.x) after two warm-up passes; for the autotuner.
+medyan_status cg_batch_time_evaluate(PackedBatch& pb, int prec, int reps, float* ms);
 
 }  // namespace mb

@@ -167,6 +167,29 @@ class ForceFieldManager:
             L.check(st, "medyan_mech_hessian")
         return H
 
+    # -- launch shapes ----------------------------------------------------
+    def get_shapes(self) -> dict:
+        from ._abi import LaunchShapes
+        sh = LaunchShapes()
+        L.check(self.lib.medyan_mech_get_shapes(self.handle, C.byref(sh)), "medyan_mech_get_shapes")
+        return sh.as_dict()
+
+    def set_shapes(self, **shapes) -> None:
+        """Block/tile shapes per potential (medyan_launch_shapes); fields not
+        given keep their current values."""
+        from ._abi import LaunchShapes
+        cur = self.get_shapes()
+        cur.update(shapes)
+        sh = LaunchShapes(**cur)
+        L.check(self.lib.medyan_mech_set_shapes(self.handle, C.byref(sh)), "medyan_mech_set_shapes")
+
+    def autotune(self, reps: int = 10) -> dict:
+        """Times the evaluate pass per candidate shape and keeps the fastest."""
+        from ._abi import LaunchShapes
+        sh = LaunchShapes()
+        L.check(self.lib.medyan_mech_autotune(self.handle, reps, C.byref(sh)), "medyan_mech_autotune")
+        return sh.as_dict()
+
     # -- after a minimization --------------------------------------------
     def force_magnitudes(self):
         """ForceFieldManager::assignallforcemags inputs at the current
@@ -256,6 +279,27 @@ class BatchMinimizer:
         L.check(self.lib.medyan_batch_create(arr, len(self._systems), self.precision, C.byref(self.handle)),
                 "medyan_batch_create")
         self.n = len(self._systems)
+
+    def get_shapes(self) -> dict:
+        from ._abi import BatchShapes
+        sh = BatchShapes()
+        L.check(self.lib.medyan_batch_get_shapes(self.handle, C.byref(sh)), "medyan_batch_get_shapes")
+        return sh.as_dict()
+
+    def set_shapes(self, **shapes) -> None:
+        """Packed-layout shapes (medyan_batch_shapes); fields not given keep their values."""
+        from ._abi import BatchShapes
+        cur = self.get_shapes()
+        cur.update(shapes)
+        L.check(self.lib.medyan_batch_set_shapes(self.handle, C.byref(BatchShapes(**cur))), "medyan_batch_set_shapes")
+
+    def autotune(self, reps: int = 5) -> dict:
+        """Times packed evaluate passes at the replicas' current coordinates per candidate
+        shape and keeps the fastest (set each replica's coordinates first)."""
+        from ._abi import BatchShapes
+        sh = BatchShapes()
+        L.check(self.lib.medyan_batch_autotune(self.handle, reps, C.byref(sh)), "medyan_batch_autotune")
+        return sh.as_dict()
 
     def replica(self, r: int) -> C.c_void_p:
         """The handle of replica r (for set_cylinders / rebuild_neighbors)."""

@@ -48,6 +48,12 @@ PROTOTYPES = {
     "medyan_mech_param_grad": (C.c_int32, [_vp, C.c_int32, _pd, _pd, _pd, C.c_int64]),
     "medyan_mech_hessian": (C.c_int32, [_vp, C.c_float, _pd]),
     "medyan_mech_force_magnitudes": (C.c_int32, [_vp, _pd, _pd, _pd]),
+    "medyan_mech_set_shapes": (C.c_int32, [_vp, _vp]),
+    "medyan_mech_get_shapes": (C.c_int32, [_vp, _vp]),
+    "medyan_mech_autotune": (C.c_int32, [_vp, C.c_int32, _vp]),
+    "medyan_batch_set_shapes": (C.c_int32, [_vp, _vp]),
+    "medyan_batch_get_shapes": (C.c_int32, [_vp, _vp]),
+    "medyan_batch_autotune": (C.c_int32, [_vp, C.c_int32, _vp]),
     "medyan_mech_boundary_load_forces": (C.c_int32, [_vp, _vp, _pd, C.c_int64]),
     "medyan_mech_hvp": (C.c_int32, [_vp, _pd, _pd]),
     "medyan_batch_create": (C.c_int32, [_vp, C.c_int32, C.c_int32, C.POINTER(_vp)]),

@@ -86,3 +86,27 @@ def test_batch_evaluate(gpu_lib, oracle):
         fo = oracle.forces(sv, x)
         assert abs(e[r] - eo) <= 1e-12 * abs(eo)
         assert np.abs(fs[r] - fo).max() <= 1e-12 * np.abs(fo).max()
+
+
+def test_batch_shapes_keep_results(gpu_lib, oracle):
+    # a packed layout of other block shapes is the same computation
+    import ctypes as C
+    reps = replicas(oracle, n=5, seed=13)
+    p = cgp(grad_tol=1e-4, energy_rel_tol=1e-14, energy_call_limit=30)
+    with BatchMinimizer([sv for sv, _ in reps], "fp64") as b:
+        st0, xs0, _, rs0 = b.minimize([x for _, x in reps], p)
+        b.set_shapes(bonded_threads=128, excl_threads=32, chain_threads=512, chain_chunk=1024)
+        assert b.get_shapes() == dict(bonded_threads=128, excl_threads=32, chain_threads=512, chain_chunk=1024)
+        st1, xs1, _, rs1 = b.minimize([x for _, x in reps], p)
+        # the autotuner times packed passes at the replicas' coordinates
+        for r, (_, x) in enumerate(reps):
+            xx = np.ascontiguousarray(x, np.float64)
+            b.lib.medyan_mech_set_coords(b.replica(r), xx.ctypes.data_as(C.POINTER(C.c_double)))
+        chosen = b.autotune(reps=3)
+        assert chosen == b.get_shapes()
+        st2, xs2, _, rs2 = b.minimize([x for _, x in reps], p)
+    for r in range(len(reps)):
+        assert st0[r] == st1[r] == st2[r] == 0
+        assert (rs0[r].num_energy_call, rs0[r].num_force_call) == (rs1[r].num_energy_call, rs1[r].num_force_call) \
+            == (rs2[r].num_energy_call, rs2[r].num_force_call)
+        assert np.abs(xs1[r] - xs0[r]).max() <= 1e-7 and np.abs(xs2[r] - xs0[r]).max() <= 1e-7
