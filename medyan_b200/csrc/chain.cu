@@ -117,78 +117,83 @@ template <class R, int KMAX, bool MOVE>
 __global__ void __launch_bounds__(kThreads, KMAX == 1 ? 4 : 2)
     k_chain_energy(const ChainDev ch, const double* __restrict__ x, const double* __restrict__ d,
                    const LambdaSet* __restrict__ lset, double* __restrict__ partial, int nblk_total, int blk_off,
-                   const int4* __restrict__ table) {
+                   const int4* __restrict__ table, int n_table) {
     __shared__ double sm[4 * 32];
     const int n = ch.n_pos;
     const int K = lset ? lset->K : 1;
     const int lane = threadIdx.x & 31;
-    // grid-stride over all positions, or (table) this block's chunk
-    // [table.y, table.z) of one replica's positions
-    int lo = 0, hi = n, w0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, ws = (gridDim.x * blockDim.x) >> 5;
-    if (table) {
-        const int4 t = table[blockIdx.x];
-        if (ch.act && !ch.act[t.x]) return;  // replica not in this pass
-        lo = t.y;
-        hi = t.z;
-        w0 = threadIdx.x >> 5;
-        ws = blockDim.x >> 5;
-    }
-    double acc[KMAX][2];
-#pragma unroll
-    for (int k = 0; k < KMAX; ++k) acc[k][0] = acc[k][1] = 0.0;
-    for (int w = w0; lo + (long long)w * 32 < hi; w += ws) {
-        const int q = lo + w * 32 + lane;
-        const bool in = q < hi;
-        const int qe = lane == 0 ? q - 1 : q + 1;
-        const V3 c = pos_of(x, n, q), dc = MOVE ? pos_of(d, n, q) : V3{0.0, 0.0, 0.0};
-        V3 ce{0.0, 0.0, 0.0}, de{0.0, 0.0, 0.0};
-        if (lane == 0 || lane == 31) {
-            ce = pos_of(x, n, qe);
-            if (MOVE) de = pos_of(d, n, qe);
+    // grid-stride over all positions (one partial row per block), or (table)
+    // the chunks [table.y, table.z) of one replica's positions, one row per
+    // chunk, walked by a capped grid
+    const int trips = table ? n_table : gridDim.x;
+    for (int row = blockIdx.x; row < trips; row += (table ? gridDim.x : trips)) {
+        int lo = 0, hi = n, w0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, ws = (gridDim.x * blockDim.x) >> 5;
+        if (table) {
+            const int4 t = table[row];
+            if (ch.act && !ch.act[t.x]) continue;  // replica not in this pass
+            lo = t.y;
+            hi = t.z;
+            w0 = threadIdx.x >> 5;
+            ws = blockDim.x >> 5;
         }
-        const unsigned char fl = in ? ch.flags[q] : 0;
-        const double2 lp = in ? ch.link_p[q] : double2{0.0, 0.0};
-        const double2 bp = in ? ch.bend_p[q] : double2{0.0, 0.0};
-        V3 cp = shfl_up3(c), cn = shfl_down3(c);
-        if (lane == 0) cp = ce;
-        if (lane == 31) cn = ce;
-        if (!MOVE) {
-            if (fl & kLink) acc[0][0] += stretch_energy<R>(c, cn, lp.x, lp.y);
-            if (fl & kBend) acc[0][1] += bend_energy<R>(diff<R>(cp, c), diff<R>(c, cn), bp.x, bp.y);
-            continue;
-        }
-        V3 dp = shfl_up3(dc), dn = shfl_down3(dc);
-        if (lane == 0) dp = de;
-        if (lane == 31) dn = de;
-        if (fl) {
-#pragma unroll
-            for (int k = 0; k < KMAX; ++k) {
-                if (k >= K) break;
-                const double lam = lset ? lset->lam[k] : 0.0;
-                const V3 Pc = move3(c, lam, dc), Pn = move3(cn, lam, dn);
-                if (fl & kLink) acc[k][0] += stretch_energy<R>(Pc, Pn, lp.x, lp.y);
-                if (fl & kBend) {
-                    const V3 Pp = move3(cp, lam, dp);
-                    acc[k][1] += bend_energy<R>(diff<R>(Pp, Pc), diff<R>(Pc, Pn), bp.x, bp.y);
+        double acc[KMAX][2];
+    #pragma unroll
+        for (int k = 0; k < KMAX; ++k) acc[k][0] = acc[k][1] = 0.0;
+        for (int w = w0; lo + (long long)w * 32 < hi; w += ws) {
+            const int q = lo + w * 32 + lane;
+            const bool in = q < hi;
+            const int qe = lane == 0 ? q - 1 : q + 1;
+            const V3 c = pos_of(x, n, q), dc = MOVE ? pos_of(d, n, q) : V3{0.0, 0.0, 0.0};
+            V3 ce{0.0, 0.0, 0.0}, de{0.0, 0.0, 0.0};
+            if (lane == 0 || lane == 31) {
+                ce = pos_of(x, n, qe);
+                if (MOVE) de = pos_of(d, n, qe);
+            }
+            const unsigned char fl = in ? ch.flags[q] : 0;
+            const double2 lp = in ? ch.link_p[q] : double2{0.0, 0.0};
+            const double2 bp = in ? ch.bend_p[q] : double2{0.0, 0.0};
+            V3 cp = shfl_up3(c), cn = shfl_down3(c);
+            if (lane == 0) cp = ce;
+            if (lane == 31) cn = ce;
+            if (!MOVE) {
+                if (fl & kLink) acc[0][0] += stretch_energy<R>(c, cn, lp.x, lp.y);
+                if (fl & kBend) acc[0][1] += bend_energy<R>(diff<R>(cp, c), diff<R>(c, cn), bp.x, bp.y);
+                continue;
+            }
+            V3 dp = shfl_up3(dc), dn = shfl_down3(dc);
+            if (lane == 0) dp = de;
+            if (lane == 31) dn = de;
+            if (fl) {
+    #pragma unroll
+                for (int k = 0; k < KMAX; ++k) {
+                    if (k >= K) break;
+                    const double lam = lset ? lset->lam[k] : 0.0;
+                    const V3 Pc = move3(c, lam, dc), Pn = move3(cn, lam, dn);
+                    if (fl & kLink) acc[k][0] += stretch_energy<R>(Pc, Pn, lp.x, lp.y);
+                    if (fl & kBend) {
+                        const V3 Pp = move3(cp, lam, dp);
+                        acc[k][1] += bend_energy<R>(diff<R>(Pp, Pc), diff<R>(Pc, Pn), bp.x, bp.y);
+                    }
                 }
             }
         }
-    }
-#pragma unroll
-    for (int k = 0; k < KMAX; ++k) {
-        if (k >= K) break;
-        double e[2] = {acc[k][0], acc[k][1]};
-        block_sum<2>(e, sm);
-        if (threadIdx.x == 0) {
-            // a plain pass writes its one evaluation to every requested slot
-            for (int kk = k; kk < (MOVE ? k + 1 : K); ++kk) {
-                double* o = partial + ((size_t)kk * nblk_total + blk_off + blockIdx.x) * 4;
-                o[0] = e[0];
-                o[1] = e[1];
-                o[2] = 0.0;
-                o[3] = 0.0;
+    #pragma unroll
+        for (int k = 0; k < KMAX; ++k) {
+            if (k >= K) break;
+            double e[2] = {acc[k][0], acc[k][1]};
+            block_sum<2>(e, sm);
+            if (threadIdx.x == 0) {
+                // a plain pass writes its one evaluation to every requested slot
+                for (int kk = k; kk < (MOVE ? k + 1 : K); ++kk) {
+                    double* o = partial + ((size_t)kk * nblk_total + blk_off + row) * 4;
+                    o[0] = e[0];
+                    o[1] = e[1];
+                    o[2] = 0.0;
+                    o[3] = 0.0;
+                }
             }
         }
+        __syncthreads();  // smem of block_sum is reused by the next trip
     }
 }
 
@@ -230,7 +235,8 @@ void launch_chain_forces(const ChainDev& ch, int prec, const double* x, const Fo
     if (ch.n_pos <= 0) return;
     const int threads = ch.force_threads > 0 ? ch.force_threads : kThreads;
     const int per_block = kWarpOut * (threads / 32);
-    const int g = (ch.n_pos + per_block - 1) / per_block;
+    int g = (ch.n_pos + per_block - 1) / per_block;
+    if (ch.act && g > 2 * kBatchGridCap) g = 2 * kBatchGridCap;  // batched: the warp loop covers the rest
     if (prec == MEDYAN_PREC_MIXED)
         k_chain_forces<float><<<g, threads, 0, s>>>(ch, x, t);
     else
@@ -241,14 +247,15 @@ void launch_chain_energy(const ChainDev& ch, int prec, const double* x, const do
                          double* partial, int nblk_total, int blk_off, cudaStream_t s, const int4* table,
                          int table_blocks) {
     if (ch.n_pos <= 0) return;
-    const int g = table ? table_blocks : chain_blocks(ch);
-    if (g <= 0) return;
+    const int nrows = table ? table_blocks : chain_blocks(ch);
+    if (nrows <= 0) return;
+    const int g = table && nrows > kBatchGridCap ? kBatchGridCap : nrows;
     if (prec == MEDYAN_PREC_MIXED) {
-        if (d) k_chain_energy<float, kMaxLambda, true><<<g, kThreads, 0, s>>>(ch, x, d, lam, partial, nblk_total, blk_off, table);
-        else k_chain_energy<float, 1, false><<<g, kThreads, 0, s>>>(ch, x, d, lam, partial, nblk_total, blk_off, table);
+        if (d) k_chain_energy<float, kMaxLambda, true><<<g, kThreads, 0, s>>>(ch, x, d, lam, partial, nblk_total, blk_off, table, nrows);
+        else k_chain_energy<float, 1, false><<<g, kThreads, 0, s>>>(ch, x, d, lam, partial, nblk_total, blk_off, table, nrows);
     } else {
-        if (d) k_chain_energy<double, kMaxLambda, true><<<g, kThreads, 0, s>>>(ch, x, d, lam, partial, nblk_total, blk_off, table);
-        else k_chain_energy<double, 1, false><<<g, kThreads, 0, s>>>(ch, x, d, lam, partial, nblk_total, blk_off, table);
+        if (d) k_chain_energy<double, kMaxLambda, true><<<g, kThreads, 0, s>>>(ch, x, d, lam, partial, nblk_total, blk_off, table, nrows);
+        else k_chain_energy<double, 1, false><<<g, kThreads, 0, s>>>(ch, x, d, lam, partial, nblk_total, blk_off, table, nrows);
     }
 }
 

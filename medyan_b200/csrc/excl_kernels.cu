@@ -29,46 +29,49 @@ __global__ void __launch_bounds__(kMaxExclThreads) k_excl_energy(const DeviceFF 
                                                             const LambdaSet* __restrict__ lset,
                                                             double* __restrict__ partial, int nblk_total,
                                                             int blk_off, int* __restrict__ fb_count,
-                                                            int2* __restrict__ fb_list, int* __restrict__ bad) {
+                                                            int2* __restrict__ fb_list, int* __restrict__ bad, int n_logical) {
     __shared__ double smem[4 * 32];
-    if (ff.act && !ff.act[ff.rep_excl[blockIdx.x]]) return;  // batched: replica not in this pass
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool move = MOVE;
-    bool valid = i < ff.n_excl;
-    V3 X[4] = {}, D[4] = {};
-    double krs = 0;
-    int4 q = valid ? ff.excl_bs[i] : int4{-1, 0, 0, 0};
-    valid = valid && q.x >= 0;  // -1: padding record
-    if (valid) {
-        krs = ff.excl_krs[i];
-        X[0] = load3(x + q.x); X[1] = load3(x + q.y); X[2] = load3(x + q.z); X[3] = load3(x + q.w);
-        if (move) { D[0] = load3(d + q.x); D[1] = load3(d + q.y); D[2] = load3(d + q.z); D[3] = load3(d + q.w); }
-    }
-    const int K = lset ? lset->K : 1;
-#pragma unroll
-    for (int k = 0; k < kMaxLambda; ++k) {
-        if (k >= K) break;
-        const double lam = lset ? lset->lam[k] : 0.0;
-        double e[1] = {0.0};
+    for (int lb = blockIdx.x; lb < n_logical; lb += gridDim.x) {  // capped grid in batches
+        if (ff.act && !ff.act[ff.rep_excl[lb]]) continue;  // batched: replica not in this pass
+        const int i = lb * blockDim.x + threadIdx.x;
+        const bool move = MOVE;
+        bool valid = i < ff.n_excl;
+        V3 X[4] = {}, D[4] = {};
+        double krs = 0;
+        int4 q = valid ? ff.excl_bs[i] : int4{-1, 0, 0, 0};
+        valid = valid && q.x >= 0;  // -1: padding record
         if (valid) {
-            double U = excl_energy<R>(at(X[0], D[0], lam, move), at(X[1], D[1], lam, move),
-                                      at(X[2], D[2], lam, move), at(X[3], D[3], lam, move), krs);
-            if (excl_energy_bad(U)) {
-                int slot = atomicAdd(fb_count, 1);
-                if (slot < kFallbackCap) fb_list[slot] = make_int2(i, k);
-                else atomicOr(bad + k, 2);
-                U = 0.0;
+            krs = ff.excl_krs[i];
+            X[0] = load3(x + q.x); X[1] = load3(x + q.y); X[2] = load3(x + q.z); X[3] = load3(x + q.w);
+            if (move) { D[0] = load3(d + q.x); D[1] = load3(d + q.y); D[2] = load3(d + q.z); D[3] = load3(d + q.w); }
+        }
+        const int K = lset ? lset->K : 1;
+    #pragma unroll
+        for (int k = 0; k < kMaxLambda; ++k) {
+            if (k >= K) break;
+            const double lam = lset ? lset->lam[k] : 0.0;
+            double e[1] = {0.0};
+            if (valid) {
+                double U = excl_energy<R>(at(X[0], D[0], lam, move), at(X[1], D[1], lam, move),
+                                          at(X[2], D[2], lam, move), at(X[3], D[3], lam, move), krs);
+                if (excl_energy_bad(U)) {
+                    int slot = atomicAdd(fb_count, 1);
+                    if (slot < kFallbackCap) fb_list[slot] = make_int2(i, k);
+                    else atomicOr(bad + k, 2);
+                    U = 0.0;
+                }
+                e[0] = U;
             }
-            e[0] = U;
+            block_sum<1>(e, smem);
+            if (threadIdx.x == 0) {
+                double* o = partial + ((size_t)k * nblk_total + blk_off + lb) * 4;
+                o[0] = e[0];
+                o[1] = 0.0;
+                o[2] = 0.0;
+                o[3] = 0.0;
+            }
         }
-        block_sum<1>(e, smem);
-        if (threadIdx.x == 0) {
-            double* o = partial + ((size_t)k * nblk_total + blk_off + blockIdx.x) * 4;
-            o[0] = e[0];
-            o[1] = 0.0;
-            o[2] = 0.0;
-            o[3] = 0.0;
-        }
+        __syncthreads();  // smem of block_sum is reused by the next trip
     }
 }
 
@@ -80,26 +83,28 @@ __device__ __forceinline__ V3 pos_at(const double* __restrict__ x, const ForceTa
 template <class R>
 __global__ void __launch_bounds__(kMaxExclThreads) k_excl_forces(const DeviceFF ff, const double* __restrict__ x,
                                                             const ForceTarget tgt, int* __restrict__ fb_count,
-                                                            int* __restrict__ fb_list, int* __restrict__ status) {
+                                                            int* __restrict__ fb_list, int* __restrict__ status, int n_logical) {
     if (tgt.skip && *tgt.skip) return;
-    if (ff.act && !ff.act[ff.rep_excl[blockIdx.x]]) return;  // batched: replica not in this pass
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= ff.n_excl) return;
-    double* __restrict__ f = target_force(tgt);
-    const double lam = tgt.lam ? *tgt.lam : 0.0;
-    int4 q = ff.excl_bs[i];
-    if (q.x < 0) return;  // padding record
-    T3<R> fo[4];
-    if (excl_force<R>(pos_at(x, tgt, lam, q.x), pos_at(x, tgt, lam, q.y), pos_at(x, tgt, lam, q.z),
-                      pos_at(x, tgt, lam, q.w), ff.excl_krs[i], fo)) {
-        add_force(f, q.x, fo[0].x, fo[0].y, fo[0].z);
-        add_force(f, q.y, fo[1].x, fo[1].y, fo[1].z);
-        add_force(f, q.z, fo[2].x, fo[2].y, fo[2].z);
-        add_force(f, q.w, fo[3].x, fo[3].y, fo[3].z);
-    } else {
-        int slot = atomicAdd(fb_count, 1);
-        if (slot < kFallbackCap) fb_list[slot] = i;
-        else atomicOr(status, 2);
+    for (int lb = blockIdx.x; lb < n_logical; lb += gridDim.x) {  // capped grid in batches
+        if (ff.act && !ff.act[ff.rep_excl[lb]]) continue;  // batched: replica not in this pass
+        const int i = lb * blockDim.x + threadIdx.x;
+        if (i >= ff.n_excl) continue;
+        double* __restrict__ f = target_force(tgt);
+        const double lam = tgt.lam ? *tgt.lam : 0.0;
+        int4 q = ff.excl_bs[i];
+        if (q.x < 0) continue;  // padding record
+        T3<R> fo[4];
+        if (excl_force<R>(pos_at(x, tgt, lam, q.x), pos_at(x, tgt, lam, q.y), pos_at(x, tgt, lam, q.z),
+                          pos_at(x, tgt, lam, q.w), ff.excl_krs[i], fo)) {
+            add_force(f, q.x, fo[0].x, fo[0].y, fo[0].z);
+            add_force(f, q.y, fo[1].x, fo[1].y, fo[1].z);
+            add_force(f, q.z, fo[2].x, fo[2].y, fo[2].z);
+            add_force(f, q.w, fo[3].x, fo[3].y, fo[3].z);
+        } else {
+            int slot = atomicAdd(fb_count, 1);
+            if (slot < kFallbackCap) fb_list[slot] = i;
+            else atomicOr(status, 2);
+        }
     }
 }
 
@@ -463,109 +468,111 @@ __global__ void __launch_bounds__(kFinishThreads) k_energy_finish_batched(
     __shared__ int fbBad[kMaxLambda];
     __shared__ int2 mine[kFallbackCap];
     __shared__ int nfb;
-    const int r = blockIdx.x;
-    if (ff.act && !ff.act[r]) return;  // replica not in this pass
-    const int K = lset ? lset->K : 1;
-    const int total_blocks = nch + nbb + nbe;
-    if (threadIdx.x == 0) {
-        const int n = min(*fb_count, kFallbackCap);
-        const int p0 = excl_pairs[r], p1 = excl_pairs[r + 1];
-        int m = 0;
-        for (int a = 0; a < n; ++a) {
-            const int2 v = fb_list[a];
-            if (v.x >= p0 && v.x < p1) mine[m++] = v;
-        }
-        // deterministic order: by slot, then pair
-        for (int a = 1; a < m; ++a) {
-            int2 v = mine[a];
-            int b = a - 1;
-            while (b >= 0 && (mine[b].y > v.y || (mine[b].y == v.y && mine[b].x > v.x))) {
-                mine[b + 1] = mine[b];
-                --b;
-            }
-            mine[b + 1] = v;
-        }
-        nfb = m;
-        for (int k = 0; k < kMaxLambda; ++k) {
-            fbE[k] = 0.0;
-            fbBad[k] = bad[k];  // queue overflow marks every replica
-        }
-    }
-    __syncthreads();
-    for (int e = 0; e < nfb; ++e) {
-        const int2 q = mine[e];
-        const int4 bs = ff.excl_bs[q.x];
-        const double lam = lset ? lset->lam[q.y] : 0.0;
-        V3 P[4];
-        const int offs[4] = {bs.x, bs.y, bs.z, bs.w};
-        for (int j = 0; j < 4; ++j) {
-            V3 X = load3(x + offs[j]);
-            P[j] = d ? move3(X, lam, load3(d + offs[j])) : X;
-        }
-        double U = energyN_block(six_of(P[0], P[1], P[2], P[3]), ff.excl_krs[q.x], red);
+    for (int r = blockIdx.x; r < R; r += gridDim.x) {  // capped grid over the replicas
+        if (ff.act && !ff.act[r]) continue;  // replica not in this pass
+        const int K = lset ? lset->K : 1;
+        const int total_blocks = nch + nbb + nbe;
         if (threadIdx.x == 0) {
-            if (excl_energy_bad(U)) fbBad[q.y] |= 1;
-            else fbE[q.y] += U;
+            const int n = min(*fb_count, kFallbackCap);
+            const int p0 = excl_pairs[r], p1 = excl_pairs[r + 1];
+            int m = 0;
+            for (int a = 0; a < n; ++a) {
+                const int2 v = fb_list[a];
+                if (v.x >= p0 && v.x < p1) mine[m++] = v;
+            }
+            // deterministic order: by slot, then pair
+            for (int a = 1; a < m; ++a) {
+                int2 v = mine[a];
+                int b = a - 1;
+                while (b >= 0 && (mine[b].y > v.y || (mine[b].y == v.y && mine[b].x > v.x))) {
+                    mine[b + 1] = mine[b];
+                    --b;
+                }
+                mine[b + 1] = v;
+            }
+            nfb = m;
+            for (int k = 0; k < kMaxLambda; ++k) {
+                fbE[k] = 0.0;
+                fbBad[k] = bad[k];  // queue overflow marks every replica
+            }
         }
         __syncthreads();
-    }
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-    auto range_sum = [&](const double* base, int b0, int b1, int j) {
-        double acc = 0.0;
-        int b = b0 + lane;
-        for (; b + 32 * 7 < b1; b += 32 * 8) {
-            double v[8];
-#pragma unroll
-            for (int u = 0; u < 8; ++u) v[u] = __ldcg(base + (size_t)(b + 32 * u) * 4 + j);
-#pragma unroll
-            for (int u = 0; u < 8; ++u) acc += v[u];
-        }
-        for (; b < b1; b += 32) acc += __ldcg(base + (size_t)b * 4 + j);
-        return acc;
-    };
-    const int R1 = R + 1;
-    for (int combo = warp; combo < K * MEDYAN_FF_COUNT; combo += nwarp) {
-        const int k = combo / MEDYAN_FF_COUNT, slot = combo % MEDYAN_FF_COUNT;
-        int seg = -1, j = 0, cj = -1;
-        switch (slot) {
-            case 0: seg = 0; cj = 0; break;
-            case 1: seg = 1; cj = 1; break;
-            case 2: seg = 2; break;
-            case 3: seg = 3; break;
-            case 4: case 5: case 6: case 7: seg = 4; j = slot - 4; break;
-            case 8: break;
-            default: seg = 5; break;
-        }
-        const double* base = partial + (size_t)k * total_blocks * 4;
-        double sv;
-        if (slot == 8) {
-            sv = range_sum(base, nch + nbb + rows_excl[r], nch + nbb + rows_excl[r + 1], 0);
-        } else {
-            sv = range_sum(base, nch + rows_seg[seg * R1 + r], nch + rows_seg[seg * R1 + r + 1], j);
-            if (cj >= 0) sv += range_sum(base, rows_chain[r], rows_chain[r + 1], cj);
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) sv += __shfl_down_sync(0xffffffffu, sv, o);
-        if (lane == 0) sums[k][slot] = sv;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        for (int k = 0; k < K; ++k) {
-            double* o = out + ((size_t)r * kMaxLambda + k) * (MEDYAN_FF_COUNT + 1);
-            double tot = 0.0;
-            bool inf = false;
-            for (int slot = 0; slot < MEDYAN_FF_COUNT; ++slot) {
-                double v = sums[k][slot];
-                if (slot == MEDYAN_FF_EXCLUDED_VOLUME) {
-                    v += fbE[k];
-                    if (fbBad[k]) v = -1.0;
-                }
-                o[slot] = v;
-                if (v <= -1) inf = true;
-                else tot += v;
+        for (int e = 0; e < nfb; ++e) {
+            const int2 q = mine[e];
+            const int4 bs = ff.excl_bs[q.x];
+            const double lam = lset ? lset->lam[q.y] : 0.0;
+            V3 P[4];
+            const int offs[4] = {bs.x, bs.y, bs.z, bs.w};
+            for (int j = 0; j < 4; ++j) {
+                V3 X = load3(x + offs[j]);
+                P[j] = d ? move3(X, lam, load3(d + offs[j])) : X;
             }
-            o[MEDYAN_FF_COUNT] = inf ? __longlong_as_double(0x7ff0000000000000ULL) : tot;
+            double U = energyN_block(six_of(P[0], P[1], P[2], P[3]), ff.excl_krs[q.x], red);
+            if (threadIdx.x == 0) {
+                if (excl_energy_bad(U)) fbBad[q.y] |= 1;
+                else fbE[q.y] += U;
+            }
+            __syncthreads();
         }
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+        auto range_sum = [&](const double* base, int b0, int b1, int j) {
+            double acc = 0.0;
+            int b = b0 + lane;
+            for (; b + 32 * 7 < b1; b += 32 * 8) {
+                double v[8];
+    #pragma unroll
+                for (int u = 0; u < 8; ++u) v[u] = __ldcg(base + (size_t)(b + 32 * u) * 4 + j);
+    #pragma unroll
+                for (int u = 0; u < 8; ++u) acc += v[u];
+            }
+            for (; b < b1; b += 32) acc += __ldcg(base + (size_t)b * 4 + j);
+            return acc;
+        };
+        const int R1 = R + 1;
+        for (int combo = warp; combo < K * MEDYAN_FF_COUNT; combo += nwarp) {
+            const int k = combo / MEDYAN_FF_COUNT, slot = combo % MEDYAN_FF_COUNT;
+            int seg = -1, j = 0, cj = -1;
+            switch (slot) {
+                case 0: seg = 0; cj = 0; break;
+                case 1: seg = 1; cj = 1; break;
+                case 2: seg = 2; break;
+                case 3: seg = 3; break;
+                case 4: case 5: case 6: case 7: seg = 4; j = slot - 4; break;
+                case 8: break;
+                default: seg = 5; break;
+            }
+            const double* base = partial + (size_t)k * total_blocks * 4;
+            double sv;
+            if (slot == 8) {
+                sv = range_sum(base, nch + nbb + rows_excl[r], nch + nbb + rows_excl[r + 1], 0);
+            } else {
+                sv = range_sum(base, nch + rows_seg[seg * R1 + r], nch + rows_seg[seg * R1 + r + 1], j);
+                if (cj >= 0) sv += range_sum(base, rows_chain[r], rows_chain[r + 1], cj);
+            }
+    #pragma unroll
+            for (int o = 16; o > 0; o >>= 1) sv += __shfl_down_sync(0xffffffffu, sv, o);
+            if (lane == 0) sums[k][slot] = sv;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int k = 0; k < K; ++k) {
+                double* o = out + ((size_t)r * kMaxLambda + k) * (MEDYAN_FF_COUNT + 1);
+                double tot = 0.0;
+                bool inf = false;
+                for (int slot = 0; slot < MEDYAN_FF_COUNT; ++slot) {
+                    double v = sums[k][slot];
+                    if (slot == MEDYAN_FF_EXCLUDED_VOLUME) {
+                        v += fbE[k];
+                        if (fbBad[k]) v = -1.0;
+                    }
+                    o[slot] = v;
+                    if (v <= -1) inf = true;
+                    else tot += v;
+                }
+                o[MEDYAN_FF_COUNT] = inf ? __longlong_as_double(0x7ff0000000000000ULL) : tot;
+            }
+        }
+        __syncthreads();  // shared state is reused by the next replica
     }
 }
 
@@ -579,14 +586,13 @@ void launch_excl_energy(const DeviceFF& ff, int prec, const double* x, const dou
     // FP64 in both precision modes: the analytic integral (differences of
     // arctangents, JJ = -(triple product)^2) loses ~1e-6 relative in float.
     (void)prec;
+    const int g = logical_grid(ff, nbe), off = es.n_blocks_chain + es.n_blocks_bonded;
     if (d)
-        k_excl_energy<double, true><<<nbe, excl_block_of(ff), 0, s>>>(ff, x, d, lam, es.partial, total,
-                                                     es.n_blocks_chain + es.n_blocks_bonded, es.fb_count, es.fb_list,
-                                                     es.bad);
+        k_excl_energy<double, true><<<g, excl_block_of(ff), 0, s>>>(ff, x, d, lam, es.partial, total, off,
+                                                                   es.fb_count, es.fb_list, es.bad, nbe);
     else
-        k_excl_energy<double, false><<<nbe, excl_block_of(ff), 0, s>>>(ff, x, d, lam, es.partial, total,
-                                                     es.n_blocks_chain + es.n_blocks_bonded, es.fb_count, es.fb_list,
-                                                     es.bad);
+        k_excl_energy<double, false><<<g, excl_block_of(ff), 0, s>>>(ff, x, d, lam, es.partial, total, off,
+                                                                    es.fb_count, es.fb_list, es.bad, nbe);
 }
 
 void launch_excl_energy_fallback_and_finish(const DeviceFF& ff, const double* x, const double* d,
@@ -602,7 +608,8 @@ void launch_excl_forces(const DeviceFF& ff, int prec, const double* x, const For
     const int nbe = excl_blocks(ff);
     if (nbe <= 0) return;
     (void)prec;  // FP64 in both modes, as for the energy
-    k_excl_forces<double><<<nbe, excl_block_of(ff), 0, s>>>(ff, x, t, fs.fb_count, fs.fb_list, fs.status);
+    k_excl_forces<double><<<logical_grid(ff, nbe), excl_block_of(ff), 0, s>>>(ff, x, t, fs.fb_count, fs.fb_list,
+                                                                           fs.status, nbe);
     k_excl_force_fallback<<<1, kBlock, 0, s>>>(ff, x, t, fs.fb_count, fs.fb_list, fs.status);
 }
 
@@ -610,7 +617,7 @@ void launch_energy_finish_batched(const DeviceFF& ff, const double* x, const dou
                                   const EnergyScratch& es, const int* rows_chain, const int* rows_seg,
                                   const int* rows_excl, const int* excl_pairs, int R, double* out, cudaStream_t s) {
     if (R <= 0) return;
-    k_energy_finish_batched<<<R, kFinishThreads, 0, s>>>(ff, x, d, lam, es.partial, es.n_blocks_chain,
+    k_energy_finish_batched<<<R < 148 ? R : 148, kFinishThreads, 0, s>>>(ff, x, d, lam, es.partial, es.n_blocks_chain,
                                                          es.n_blocks_bonded, es.n_blocks_excl, rows_chain, rows_seg,
                                                          rows_excl, excl_pairs, R, es.fb_count, es.fb_list, es.bad,
                                                          out);

@@ -181,5 +181,12 @@ inline int excl_block_of(const DeviceFF& ff) { return ff.excl_block > 0 ? ff.exc
 inline int bonded_block_of(const DeviceFF& ff) { return ff.bonded_block > 0 ? ff.bonded_block : kBlock; }
 inline int excl_blocks(const DeviceFF& ff) { return (ff.n_excl + excl_block_of(ff) - 1) / excl_block_of(ff); }
 constexpr int kMaxShapeThreads = 512;  // largest block any tunable kernel is launched with
+// Grid of a kernel over n logical blocks: one block each for a single
+// network; for a batched layout (ff.act set) a capped grid that loops over
+// them, so blocks of replicas outside the pass are skipped in a loop trip
+// instead of being scheduled (the tail of a batch, where few replicas are
+// still minimizing, is launch-bound).
+constexpr int kBatchGridCap = 148 * 4;
+inline int logical_grid(const DeviceFF& ff, int n) { return ff.act && n > kBatchGridCap ? kBatchGridCap : n; }
 
 }  // namespace mb
