@@ -149,6 +149,9 @@ public:
             check(medyan_mech_create(&sys, precision_, &h_), "vectorizeAllForceFields");
             n_beads_ = sys.n_beads;
         }
+        n_linker_ = sys.n_linker;
+        n_motor_ = sys.n_motor;
+        n_branch_ = sys.n_branch;
     }
 
     // Total energy at coord (double[3*n_beads]); +inf when a force field's
@@ -199,6 +202,53 @@ public:
 
     void setCoordinates(const double* coord) { check(medyan_mech_set_coords(handle(), coord), "setCoordinates"); }
 
+    // ForceFieldManager::computeHessian (ForceFieldManager.cpp:354-398): the
+    // dense finite-difference Hessian at coord, row-major ndof x ndof, entries
+    // rounded to float as the reference stores them.
+    std::vector<double> computeHessian(const double* coord, float delta) {
+        setCoordinates(coord);
+        const size_t n = 3 * (size_t)n_beads_;
+        std::vector<double> H(n * n);
+        check(medyan_mech_hessian(handle(), delta, H.data()), "computeHessian");
+        return H;
+    }
+
+    // The values ForceFieldManager::assignallforcemags (ForceFieldManager.cpp:346-351)
+    // hands to the linkers, motors and branch points, at coord.
+    struct ForceMagnitudes {
+        std::vector<double> linkerStretch, motorStretch, branchForce;  // branchForce: 3 per branch point
+    };
+    ForceMagnitudes forceMagnitudes(const double* coord) {
+        setCoordinates(coord);
+        ForceMagnitudes m;
+        m.linkerStretch.resize(n_linker_);
+        m.motorStretch.resize(n_motor_);
+        m.branchForce.resize(3 * (size_t)n_branch_);
+        check(medyan_mech_force_magnitudes(handle(), m.linkerStretch.data(), m.motorStretch.data(),
+                                           m.branchForce.data()),
+              "forceMagnitudes");
+        return m;
+    }
+
+    // BoundaryCylinderRepulsion::computeLoadForces for the given filament tips
+    // (after resetNeighborLists): tip t's loadForcesP / loadForcesM vector is
+    // out[o_t .. o_t + n_mon[t]), o_t the sum of the earlier tips' n_mon.
+    std::vector<double> computeLoadForces(const medyan_load_tips& tips) {
+        int64_t total = 0;
+        for (int t = 0; t < tips.n_tips; ++t) total += tips.n_mon[t];
+        std::vector<double> out((size_t)total);
+        check(medyan_mech_boundary_load_forces(handle(), &tips, out.data(), total), "computeLoadForces");
+        return out;
+    }
+
+    // Block and tile shapes per potential for this network (no reference
+    // counterpart: the reference's kernels run on the CPU).
+    medyan_launch_shapes autotune(int reps = 10) {
+        medyan_launch_shapes s{};
+        check(medyan_mech_autotune(handle(), reps, &s), "autotune");
+        return s;
+    }
+
     int numBeads() const { return n_beads_; }
     medyan_mech* handle() const {
         if (!h_) throw Error(MEDYAN_ERR_INVALID_ARG, "vectorizeAllForceFields was not called");
@@ -209,6 +259,7 @@ private:
     medyan_precision precision_;
     medyan_mech* h_ = nullptr;
     int n_beads_ = 0;
+    int n_linker_ = 0, n_motor_ = 0, n_branch_ = 0;
 };
 
 // CGMethod::minimize over a ForceFieldManager's force fields. The reference

@@ -268,6 +268,25 @@ int run_gpu() {
     CHECK(rel(r.energiesAfter.total, ro.energy_after_total) <= 1e-10);
     CHECK((int)fout.size() == nd);
 
+    // after a minimization: the force magnitudes the chemistry reads
+    {
+        const ForceFieldManager::ForceMagnitudes m = ffm2.forceMagnitudes(xg.data());
+        std::vector<double> lo(s.n_linker), mo(s.n_motor), bo(3 * (size_t)s.n_branch);
+        oracle_force_magnitudes(&s, xg.data(), lo.data(), mo.data(), bo.data());
+        double scale = 0, err = 0;
+        for (int i = 0; i < s.n_linker; ++i) {
+            scale = std::fmax(scale, std::fabs(lo[i]));
+            err = std::fmax(err, std::fabs(m.linkerStretch[i] - lo[i]));
+        }
+        CHECK((int)m.linkerStretch.size() == s.n_linker && err <= 1e-12 * scale + 1e-9);
+    }
+    // the autotuner leaves a handle that still computes the same energy
+    {
+        const medyan_launch_shapes sh = ffm2.autotune(3);
+        CHECK(sh.bonded_threads == 128 || sh.bonded_threads == 256 || sh.bonded_threads == 512);
+        CHECK(rel(ffm2.computeEnergy(xg.data()), oracle_energy(&s, xg.data(), nullptr)) <= 1e-12);
+    }
+
     // an unsupported option is refused, not approximated
     ConjugateGradientParams q = p;
     q.lambdaRunningAverageProbability = 0.5;
