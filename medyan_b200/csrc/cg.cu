@@ -58,7 +58,7 @@ __device__ __forceinline__ double dmax_ref(double a, double b) { return (a < b) 
 __device__ void fill_pass(CGState& s, LambdaSet& L) {
     int k = 0;
     if (s.need_e0) L.lam[k++] = 0.0;
-    const int want = s.ls_first_pass ? max(1, s.last_backtracks + 1) : kMaxLambda;
+    const int want = (s.ls_first_pass && !s.full_passes) ? max(1, s.last_backtracks + 1) : kMaxLambda;
     double lam = s.lam_next;
     int trials = 0;
     while (k < kMaxLambda && trials < want) {
@@ -1193,6 +1193,7 @@ medyan_status cg_batch_run(PackedBatch& pb, int prec, const medyan_cg_params* p)
         c.grad_tol = p->grad_tol;
         c.energy_rel_tol = p->energy_rel_tol;
         c.ls_quad = p->line_search;
+        c.full_passes = 1;
         c.status = MEDYAN_OK;
         c.parity = 1;
         c.grad_inf_norm = __builtin_inf();

@@ -108,6 +108,11 @@ struct CGState {
     double q_ebt;          // its energy (TotalEnergy and newEnergy of the search)
     double q_maxe;         // largest energy of a failed trial after the first
     double q_lq;           // lambda of the pending quadratic pass
+    // batched minimization: every line-search pass offers the full set of
+    // trial step sizes (the batch evaluates the largest set any replica asks
+    // for, so fewer trials save nothing there and cost extra rounds)
+    int full_passes;
+    int pad2;
 };
 
 }  // namespace mb
