@@ -117,6 +117,20 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
+# ------------------------------------------------------------ multi-rank
+def max_over_ranks(t: float, world: int, device: str) -> float:
+    """The largest of every rank's t (each rank runs its own replica; the
+    job's time is the slowest rank's). Every rank calls this the same number
+    of times, in the same order."""
+    if world <= 1:
+        return t
+    import torch
+    import torch.distributed as dist
+    tt = torch.tensor([t], dtype=torch.float64, device=device)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    return float(tt.item())
+
+
 # ---------------------------------------------------------------- our arm
 def run_ours(args, rank: int, world: int) -> dict:
     import ctypes as C
@@ -212,11 +226,7 @@ def run_ours(args, rank: int, world: int) -> dict:
         w1.record(stream)
     L.medyan_mech_synchronize(h)
     t_warm = w0.elapsed_time(w1) / 1e3 / K
-    t_step = sum(t_steps)
-    if world > 1:
-        tt = torch.tensor([t_step], device="cuda")
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        t_step = float(tt.item())
+    t_step = max_over_ranks(sum(t_steps), world, "cuda")
 
     # e2e through the C ABI from pinned host buffers
     xh = torch.from_numpy(x.copy()).pin_memory()
@@ -233,7 +243,7 @@ def run_ours(args, rank: int, world: int) -> dict:
         st = L.medyan_mech_evaluate(h, xptr, C.byref(etot), per, fptr)
         if st not in (0, 3):
             raise RuntimeError(f"medyan_mech_evaluate status {st}")
-    e2e_t = time.perf_counter() - t0
+    e2e_t = max_over_ranks(time.perf_counter() - t0, world, "cuda")
 
     # accuracy of this precision against the FP64 path on the same inputs
     ff64 = make("fp64") if args.precision != "fp64" else ff
