@@ -537,6 +537,10 @@ medyan_status medyan_excl_energy_noalloc(const double* d_coords, int32_t n_beads
 /* Library info                                                              */
 /* ------------------------------------------------------------------------ */
 const char* medyan_status_string(int32_t status);
+/* Name of the CUDA runtime error behind the most recent MEDYAN_ERR_CUDA (or
+   MEDYAN_ERR_NO_DEVICE) any entry point returned on the calling thread, e.g.
+   "cudaErrorInvalidValue"; "" when there was none. */
+const char* medyan_last_cuda_error(void);
 int32_t medyan_abi_version(void);
 
 #ifdef __cplusplus

@@ -37,8 +37,14 @@ namespace medyan_b200 {
 class Error : public std::runtime_error {
 public:
     Error(medyan_status s, const std::string& what)
-        : std::runtime_error(what + ": " + medyan_status_string(s)), status(s) {}
+        : std::runtime_error(what + ": " + medyan_status_string(s) + cuda_detail(s)), status(s) {}
     medyan_status status;
+
+private:
+    static std::string cuda_detail(medyan_status s) {
+        if (s != MEDYAN_ERR_CUDA && s != MEDYAN_ERR_NO_DEVICE) return "";
+        return std::string(" [") + medyan_last_cuda_error() + "]";
+    }
 };
 
 inline void check(medyan_status s, const char* what) {

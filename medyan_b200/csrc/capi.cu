@@ -12,8 +12,13 @@ using namespace mb;
 
 namespace mb {
 
+namespace {
+thread_local cudaError_t t_last_cuda_error = cudaSuccess;
+}
+
 medyan_status cuda_status(cudaError_t e) {
     if (e == cudaSuccess) return MEDYAN_OK;
+    t_last_cuda_error = e;
     if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return MEDYAN_ERR_NO_DEVICE;
     return MEDYAN_ERR_CUDA;
 }
@@ -327,7 +332,7 @@ cudaError_t ensure_pass_graph(medyan_mech* h, int which) {
     cudaError_t e = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return e;
     if (which == kPassBoth)
-        launch_evaluate(h->chain, h->ff, h->prec, h->x.raw(), h->lam_zero.raw(),
+        launch_evaluate(h->chain, h->ff, h->prec, h->x.raw(), nullptr, h->lam_zero.raw(),
                         ForceTarget{h->f.raw(), nullptr, nullptr, nullptr, nullptr, nullptr}, h->es, h->fs, h->stream,
                         &h->fork);
     else if (which == kPassEnergy)
@@ -422,6 +427,10 @@ medyan_mech::~medyan_mech() {
 extern "C" {
 
 int32_t medyan_abi_version(void) { return 1; }
+
+const char* medyan_last_cuda_error(void) {
+    return t_last_cuda_error == cudaSuccess ? "" : cudaGetErrorName(t_last_cuda_error);
+}
 
 const char* medyan_status_string(int32_t s) {
     switch (s) {

@@ -84,12 +84,22 @@ __device__ void begin_line_search(CGState& s, LambdaSet& L) {
     s.q_mode = s.ls_quad && !s.safe_mode;
     s.q_phase = 0;
     s.q_maxe = -__builtin_inf();
+    s.spec_skip = 1;
+    s.spec_valid = 0;
     if (s.grad_inf_norm == 0.0) {  // "return zero if no forces": lambda 0, no energy call
         s.ls_immediate_fail = 1;
         L.K = 0;
         return;
     }
     s.lam_next = dmin_ref(s.lambda_max, s.max_dist / s.grad_inf_norm);
+    // speculative force at the first trial, when the previous line search
+    // took its first trial (read only by the single-network minimizer)
+    if (s.last_backtracks == 0) {
+        s.spec_lam = s.lam_next;
+        s.spec_skip = 0;
+        s.spec_valid = 1;
+        s.spec_status = 0;
+    }
     fill_pass(s, L);
 }
 
@@ -304,8 +314,29 @@ __device__ void ls_decide(CGState& s, LambdaSet& Lr, const double* __restrict__ 
     fill_pass(s, *L);  // undecided: evaluate the next halvings
 }
 
-__global__ void k_ls_decide(CGState* __restrict__ st, LambdaSet* __restrict__ L, const double* __restrict__ out) {
-    ls_decide(*st, *L, out);
+// Single network: the decision, then the speculative force. The first pass
+// of a line search also computed the forces at its first trial step; when
+// the line search ends on a move by exactly that step, those forces (already
+// in the new-force buffer) are the ones the force pass would compute, so it
+// is skipped and their status bits count as its own.
+// It also sets the line-search loop's condition (another round?) and, when
+// the line search ends, the condition of the force pass (its kernels also
+// check force_skip themselves).
+__global__ void k_ls_decide(CGState* __restrict__ st, LambdaSet* __restrict__ L, const double* __restrict__ out,
+                            int* __restrict__ force_status, cudaGraphConditionalHandle h_ls,
+                            cudaGraphConditionalHandle h_force) {
+    CGState& s = *st;
+    ls_decide(s, *L, out);
+    s.spec_skip = 1;  // later passes of this line search compute no forces
+    cudaGraphSetConditional(h_ls, (!s.done && s.ls_active) ? 1u : 0u);
+    if (s.ls_active) return;
+    s.force_skip = s.skip_force;
+    if (s.spec_valid && !s.skip_force && s.lam_move == s.spec_lam) {
+        s.force_skip = 1;
+        *force_status |= s.spec_status;
+    }
+    s.spec_valid = 0;
+    cudaGraphSetConditional(h_force, (s.force_skip || s.done) ? 0u : 1u);
 }
 
 // ----------------------------------------------------------- vector passes
@@ -491,10 +522,14 @@ __global__ void __launch_bounds__(kVecThreads) k_cg_dir(int n3, const double* __
     dir_tail(*st, *L, a, m);
 }
 
+// In the loop graph (cond_iter set) the kernel also sets the iteration
+// loop's condition.
 __global__ void __launch_bounds__(kVecThreads) k_cg_reset_dir(int n3, double* __restrict__ d,
                                                               const double* __restrict__ f0,
                                                               const double* __restrict__ f1,
-                                                              const CGState* __restrict__ st) {
+                                                              const CGState* __restrict__ st, int cond_iter,
+                                                              cudaGraphConditionalHandle h_iter) {
+    if (cond_iter && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(h_iter, st->done ? 0u : 1u);
     if (!st->reset_after_dir) return;
     const double* __restrict__ F = st->parity ? f1 : f0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x)
@@ -547,15 +582,10 @@ __global__ void k_cg_record_final(CGState* __restrict__ st, const double* __rest
     s.num_energy_call++;
 }
 
-// Condition kernels for the graph's WHILE nodes.
-__global__ void k_cond_ls(const CGState* __restrict__ st, cudaGraphConditionalHandle h) {
-    cudaGraphSetConditional(h, (!st->done && st->ls_active) ? 1u : 0u);
-}
+// Arms the line-search WHILE node at the start of an iteration; later rounds
+// are armed by k_ls_decide and the next iteration by k_cg_reset_dir.
 __global__ void k_cond_arm_ls(const CGState* __restrict__ st, cudaGraphConditionalHandle h) {
     cudaGraphSetConditional(h, (!st->done && st->ls_active) ? 1u : 0u);
-}
-__global__ void k_cond_iter(const CGState* __restrict__ st, cudaGraphConditionalHandle h) {
-    cudaGraphSetConditional(h, st->done ? 0u : 1u);
 }
 
 // ------------------------------------------------------------ batched form
@@ -767,7 +797,9 @@ struct CGLaunch {
     double *x, *d, *f0, *f1, *part, *minE;
     CGState* st;
     LambdaSet* L;
-    ForceTarget tgt;
+    ForceTarget tgt;   // the iteration's force pass
+    ForceTarget spec;  // the speculative force of a line search's first pass
+    ForceScratch spec_fs;
 };
 
 CGLaunch make_launch(medyan_mech* h) {
@@ -783,28 +815,48 @@ CGLaunch make_launch(medyan_mech* h) {
     c.minE = h->cg_min_coords.raw();
     c.st = h->cg_state.raw();
     c.L = h->cg_lam.raw();
-    c.tgt = ForceTarget{c.f0, c.f1, &c.st->parity, &c.st->skip_force, c.d, &c.st->lam_move};
+    c.tgt = ForceTarget{c.f0, c.f1, &c.st->parity, &c.st->force_skip, c.d, &c.st->lam_move};
+    c.spec = ForceTarget{c.f0, c.f1, &c.st->parity, &c.st->spec_skip, c.d, &c.st->spec_lam};
+    c.spec_fs = ForceScratch{h->fs.fb_count, h->fs.fb_list, &c.st->spec_status};
     return c;
 }
 
-void enqueue_ls_pass(const CGLaunch& c, cudaStream_t s) {
-    enqueue_energy(c.h, c.x, c.d, c.L, s);
-    k_ls_decide<<<1, 1, 0, s>>>(c.st, c.L, c.h->energy_out.raw());
+// Energies at the pass's trial steps; with them, in the first pass of a line
+// search, the forces at its first trial step.
+void enqueue_ls_pass(const CGLaunch& c, cudaStream_t s, cudaGraphConditionalHandle h_ls,
+                     cudaGraphConditionalHandle h_force) {
+    launch_evaluate(c.h->chain, c.h->ff, c.h->prec, c.x, c.d, c.L, c.spec, c.h->es, c.spec_fs, s, &c.h->fork);
+    k_ls_decide<<<1, 1, 0, s>>>(c.st, c.L, c.h->energy_out.raw(), c.h->fs.status, h_ls, h_force);
 }
 
-void enqueue_step(const CGLaunch& c, cudaStream_t s) {
+void enqueue_force_pass(const CGLaunch& c, cudaStream_t s) {
     launch_forces(c.h->chain, c.h->ff, c.h->prec, c.x, c.tgt, c.h->fs, s, &c.h->fork);
+}
+
+// The move and its dots, the new direction. cond_iter: in the loop graph,
+// where the last kernel sets the iteration condition h_iter.
+void enqueue_move_and_direction(const CGLaunch& c, cudaStream_t s, int cond_iter = 0,
+                                cudaGraphConditionalHandle h_iter = 0) {
     k_cg_dots<<<c.vb, kVecThreads, 0, s>>>(c.n3, c.x, c.d, c.f0, c.f1, c.st, c.part);
     k_cg_dir<<<c.vb, kVecThreads, 0, s>>>(c.n3, c.x, c.d, c.f0, c.f1, c.st, c.part, c.minE, c.L);
-    k_cg_reset_dir<<<c.vb, kVecThreads, 0, s>>>(c.n3, c.d, c.f0, c.f1, c.st);
+    k_cg_reset_dir<<<c.vb, kVecThreads, 0, s>>>(c.n3, c.d, c.f0, c.f1, c.st, cond_iter, h_iter);
 }
 
-// Whole minimization loop as one graph: WHILE(iter) { WHILE(ls) { pass }; step }.
+// The force pass, then the move and the new direction.
+void enqueue_step(const CGLaunch& c, cudaStream_t s) {
+    enqueue_force_pass(c, s);
+    enqueue_move_and_direction(c, s);
+}
+
+// Whole minimization loop as one graph:
+// WHILE(iter) { arm; WHILE(ls) { pass; decide }; IF(force) { force pass }; move, direction }.
+// The IF skips the force pass's launches when the line search ended without
+// a move or on the step whose forces the first pass already computed.
 cudaError_t build_graph(const CGLaunch& c, cudaGraphExec_t* exec) {
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaGraphCreate(&g, 0);
     if (e != cudaSuccess) return e;
-    cudaGraphConditionalHandle h_iter, h_ls;
+    cudaGraphConditionalHandle h_iter, h_ls, h_force;
     e = cudaGraphConditionalHandleCreate(&h_iter, g, 1, cudaGraphCondAssignDefault);
     cudaGraphNode_t n_iter;
     cudaGraphNodeParams p_iter = {};
@@ -821,6 +873,8 @@ cudaError_t build_graph(const CGLaunch& c, cudaGraphExec_t* exec) {
     // iteration body: arm the line-search condition, the line-search loop,
     // then the step kernels and the iteration condition
     if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&h_ls, body, 0, 0);
+    // force pass: runs unless the line search's end says otherwise
+    if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&h_force, body, 1, cudaGraphCondAssignDefault);
     cudaGraphNode_t n_arm = nullptr;
     if (e == cudaSuccess) {
         e = cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed);
@@ -847,18 +901,34 @@ cudaError_t build_graph(const CGLaunch& c, cudaGraphExec_t* exec) {
         cudaGraph_t ls_body = p_ls.conditional.phGraph_out[0];
         e = cudaStreamBeginCaptureToGraph(s, ls_body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed);
         if (e == cudaSuccess) {
-            enqueue_ls_pass(c, s);
-            k_cond_ls<<<1, 1, 0, s>>>(c.st, h_ls);
+            enqueue_ls_pass(c, s, h_ls, h_force);
+            cudaGraph_t tmp;
+            e = cudaStreamEndCapture(s, &tmp);
+        }
+    }
+    cudaGraphNode_t n_force;
+    cudaGraphNodeParams p_force = {};
+    if (e == cudaSuccess) {
+        p_force.type = cudaGraphNodeTypeConditional;
+        p_force.conditional.handle = h_force;
+        p_force.conditional.type = cudaGraphCondTypeIf;
+        p_force.conditional.size = 1;
+        e = cudaGraphAddNode(&n_force, body, &n_ls, 1, &p_force);
+    }
+    if (e == cudaSuccess) {
+        e = cudaStreamBeginCaptureToGraph(s, p_force.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeRelaxed);
+        if (e == cudaSuccess) {
+            enqueue_force_pass(c, s);
             cudaGraph_t tmp;
             e = cudaStreamEndCapture(s, &tmp);
         }
     }
     if (e == cudaSuccess) {
-        const cudaGraphNode_t deps[1] = {n_ls};
+        const cudaGraphNode_t deps[1] = {n_force};
         e = cudaStreamBeginCaptureToGraph(s, body, deps, nullptr, 1, cudaStreamCaptureModeRelaxed);
         if (e == cudaSuccess) {
-            enqueue_step(c, s);
-            k_cond_iter<<<1, 1, 0, s>>>(c.st, h_iter);
+            enqueue_move_and_direction(c, s, 1, h_iter);
             cudaGraph_t tmp;
             e = cudaStreamEndCapture(s, &tmp);
         }
@@ -928,6 +998,8 @@ medyan_status cg_enqueue(medyan_mech* h, const medyan_cg_params* p, const double
     s0.min_e = __builtin_inf();
     s0.lam_move = 0.0;
     s0.skip_force = 0;
+    s0.force_skip = 0;
+    s0.spec_skip = 1;
     s0.move_kind = 0;
     LambdaSet l0{};
     if (n3) std::memcpy(px, coord_in, bytes);

@@ -112,7 +112,14 @@ struct CGState {
     // trial step sizes (the batch evaluates the largest set any replica asks
     // for, so fewer trials save nothing there and cost extra rounds)
     int full_passes;
-    int pad2;
+    // speculative force (single network): the first line-search pass also
+    // computes the forces at the first trial step; when that step is the one
+    // accepted, the iteration's force pass is skipped
+    int spec_skip;         // 1: the speculative force kernels do nothing this pass
+    int spec_valid;        // the speculative force of this line search was computed
+    int force_skip;        // 1: the iteration's force pass does nothing
+    int spec_status;       // force-pass status bits of the speculative force
+    double spec_lam;       // its step (the line search's first trial)
 };
 
 }  // namespace mb

@@ -120,7 +120,7 @@ struct ForceScratch {
 // independent kernels on separate streams joined back into the caller's
 // stream; under stream capture the fork and join become graph edges, so the
 // kernels are parallel branches of the graph.
-constexpr int kForkWays = 8;
+constexpr int kForkWays = 10;
 struct Fork {
     cudaStream_t side[kForkWays];
     cudaEvent_t fork, join[kForkWays];
@@ -134,13 +134,18 @@ void launch_energy(const ChainDev& ch, const DeviceFF& ff, int prec, const doubl
                    const LambdaSet* lam, const EnergyScratch& es, cudaStream_t s, const Fork* fk = nullptr);
 void launch_forces(const ChainDev& ch, const DeviceFF& ff, int prec, const double* x, const ForceTarget& t,
                    const ForceScratch& fs, cudaStream_t s, const Fork* fk = nullptr);
-// Energy (at x, one step size: lam) and forces at x in one pass: the energy
-// producers and the force kernels run side by side (with fk), the energy
-// finish after its producers.
-void launch_evaluate(const ChainDev& ch, const DeviceFF& ff, int prec, const double* x, const LambdaSet* lam,
+// Energy (at x, or x + lam_k d for the step sizes of lam when d is set) and
+// forces (where t says) in one pass: the energy producers and the force
+// kernels run side by side (with fk), the energy finish after its producers.
+void launch_evaluate(const ChainDev& ch, const DeviceFF& ff, int prec, const double* x, const double* d,
+                     const LambdaSet* lam,
                      const ForceTarget& t, const EnergyScratch& es, const ForceScratch& fs, cudaStream_t s,
                      const Fork* fk);
-void launch_chain_forces(const ChainDev& ch, int prec, const double* x, const ForceTarget& t, cudaStream_t s);
+// accumulate: add to the target instead of storing every bead's force (the
+// target was zeroed by launch_force_zero)
+void launch_chain_forces(const ChainDev& ch, int prec, const double* x, const ForceTarget& t, cudaStream_t s,
+                         bool accumulate = false);
+void launch_force_zero(const ChainDev& ch, const ForceTarget& t, cudaStream_t s);
 // table (optional): block b evaluates positions [table[b].y, table[b].z) of one
 // replica (batched layouts), table_blocks blocks; else a grid-stride pass.
 void launch_chain_energy(const ChainDev& ch, int prec, const double* x, const double* d, const LambdaSet* lam,

@@ -24,6 +24,7 @@ _vp = C.c_void_p
 PROTOTYPES = {
     "medyan_abi_version": (C.c_int32, []),
     "medyan_status_string": (C.c_char_p, [C.c_int32]),
+    "medyan_last_cuda_error": (C.c_char_p, []),
     "medyan_mech_create": (C.c_int32, [_vp, C.c_int32, C.POINTER(_vp)]),
     "medyan_mech_update": (C.c_int32, [_vp, _vp]),
     "medyan_mech_destroy": (C.c_int32, [_vp]),
@@ -70,7 +71,10 @@ _lib = None
 class MedyanError(RuntimeError):
     def __init__(self, status: int, what: str):
         self.status = status
-        super().__init__(f"{what}: {STATUS_NAMES.get(status, 'unknown')} (status {status})")
+        msg = f"{what}: {STATUS_NAMES.get(status, 'unknown')} (status {status})"
+        if status in (5, 8) and _lib is not None:  # the CUDA error behind it
+            msg += f" [{(_lib.medyan_last_cuda_error() or b'').decode()}]"
+        super().__init__(msg)
 
 
 def load() -> C.CDLL:

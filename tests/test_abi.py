@@ -69,3 +69,6 @@ def test_errors_without_device_are_reported_not_faked():
     with pytest.raises(lib.MedyanError) as e:
         ff.vectorize_all_force_fields(sv)
     assert e.value.status in (5, 8)
+    # the CUDA error behind the status is named, in the message too
+    name = lib.load().medyan_last_cuda_error().decode()
+    assert name.startswith("cudaError") and name in str(e.value)
