@@ -22,10 +22,7 @@
 // shuffles, so there is no shared memory and no block barrier. The force
 // kernel evaluates each link and bend once and writes each bead's force with
 // a plain store; every bead is written, so the pass also initializes the
-// force array for the potentials that add atomically afterwards (batched
-// layouts). A single network zeroes the array first and the chain kernel
-// adds (one coalesced atomic per component), so it runs alongside the other
-// force kernels instead of ahead of them. The energy
+// force array for the potentials that add atomically afterwards. The energy
 // kernel evaluates the link and bend owned by each position at up to
 // kMaxLambda step sizes from one read of x and d.
 #include <algorithm>
@@ -70,7 +67,7 @@ __device__ __forceinline__ V3 pos_of(const double* __restrict__ x, int n, int q)
 // centred at q once, and lanes 1..30 sum the five terms acting on their
 // position from their neighbours by shuffles. No shared memory, no block
 // barriers; every position is written exactly once.
-template <class R, bool ACC>
+template <class R>
 __global__ void __launch_bounds__(kMaxShapeThreads) k_chain_forces(const ChainDev ch, const double* __restrict__ x,
                                                            const ForceTarget tgt) {
     if (tgt.skip && *tgt.skip) return;
@@ -103,28 +100,11 @@ __global__ void __launch_bounds__(kMaxShapeThreads) k_chain_forces(const ChainDe
         if (lane >= 1 && lane <= kWarpOut && in && (!ch.act || ch.act[ch.rep[q]])) {
             // link (q-1, q) acts on q; link (q, q+1) reacts on q; bends centred
             // at q-1 (third bead), q (middle), q+1 (first bead); summed in double
-            const double fx = double(Fp.x) - double(F.x) + double(Bp.x) + (double(A.x) - double(B.x)) - double(An.x);
-            const double fy = double(Fp.y) - double(F.y) + double(Bp.y) + (double(A.y) - double(B.y)) - double(An.y);
-            const double fz = double(Fp.z) - double(F.z) + double(Bp.z) + (double(A.z) - double(B.z)) - double(An.z);
-            if (ACC) {
-                atomicAdd(f + 3 * q, fx);
-                atomicAdd(f + 3 * q + 1, fy);
-                atomicAdd(f + 3 * q + 2, fz);
-            } else {
-                f[3 * q] = fx;
-                f[3 * q + 1] = fy;
-                f[3 * q + 2] = fz;
-            }
+            f[3 * q] = double(Fp.x) - double(F.x) + double(Bp.x) + (double(A.x) - double(B.x)) - double(An.x);
+            f[3 * q + 1] = double(Fp.y) - double(F.y) + double(Bp.y) + (double(A.y) - double(B.y)) - double(An.y);
+            f[3 * q + 2] = double(Fp.z) - double(F.z) + double(Bp.z) + (double(A.z) - double(B.z)) - double(An.z);
         }
     }
-}
-
-// Zeroes the target force array (n3 doubles) ahead of a force pass whose
-// kernels all add: the chain kernel then runs alongside the others.
-__global__ void k_force_zero(int n3, const ForceTarget tgt) {
-    if (tgt.skip && *tgt.skip) return;
-    double* __restrict__ f = target_force(tgt);
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x) f[i] = 0.0;
 }
 
 // Energies. Each warp owns 32 consecutive positions and each lane the link
@@ -251,28 +231,16 @@ int chain_blocks(const ChainDev& ch) {
     return b < 1 ? 1 : (b < cap ? b : cap);
 }
 
-void launch_chain_forces(const ChainDev& ch, int prec, const double* x, const ForceTarget& t, cudaStream_t s,
-                         bool accumulate) {
+void launch_chain_forces(const ChainDev& ch, int prec, const double* x, const ForceTarget& t, cudaStream_t s) {
     if (ch.n_pos <= 0) return;
     const int threads = ch.force_threads > 0 ? ch.force_threads : kThreads;
     const int per_block = kWarpOut * (threads / 32);
     int g = (ch.n_pos + per_block - 1) / per_block;
     if (ch.act && g > 2 * kBatchGridCap) g = 2 * kBatchGridCap;  // batched: the warp loop covers the rest
-    if (prec == MEDYAN_PREC_MIXED) {
-        if (accumulate) k_chain_forces<float, true><<<g, threads, 0, s>>>(ch, x, t);
-        else k_chain_forces<float, false><<<g, threads, 0, s>>>(ch, x, t);
-    } else {
-        if (accumulate) k_chain_forces<double, true><<<g, threads, 0, s>>>(ch, x, t);
-        else k_chain_forces<double, false><<<g, threads, 0, s>>>(ch, x, t);
-    }
-}
-
-void launch_force_zero(const ChainDev& ch, const ForceTarget& t, cudaStream_t s) {
-    const int n3 = 3 * ch.n_pos;
-    if (n3 <= 0) return;
-    int g = (n3 + 255) / 256;
-    if (g > 148 * 8) g = 148 * 8;
-    k_force_zero<<<g, 256, 0, s>>>(n3, t);
+    if (prec == MEDYAN_PREC_MIXED)
+        k_chain_forces<float><<<g, threads, 0, s>>>(ch, x, t);
+    else
+        k_chain_forces<double><<<g, threads, 0, s>>>(ch, x, t);
 }
 
 void launch_chain_energy(const ChainDev& ch, int prec, const double* x, const double* d, const LambdaSet* lam,

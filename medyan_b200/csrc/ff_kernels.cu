@@ -366,37 +366,8 @@ void launch_energy(const ChainDev& ch, const DeviceFF& ff, int prec, const doubl
     launch_excl_energy_fallback_and_finish(ff, x, d, lam, es, s);
 }
 
-namespace {
-
-// Single network with side streams: zero the target, then every force kernel
-// adds, all side by side: chain | linker, motor | branching | boundary,
-// filament leftovers | excluded volume (on s). Waits on the fork already
-// recorded on s (after the zero fill) for sides first..first+3.
-void forces_side_by_side(const ChainDev& ch, const DeviceFF& ff, int prec, const double* x, const ForceTarget& t,
-                         const ForceScratch& fs, cudaStream_t s, const Fork* fk, int first) {
-    for (int k = first; k < first + 4; ++k) cudaStreamWaitEvent(fk->side[k], fk->mid, 0);
-    launch_chain_forces(ch, prec, x, t, fk->side[first], true);
-    bonded_forces_group<2, 4>(ff, prec, x, t, fk->side[first + 1]);
-    bonded_forces_group<4, 5>(ff, prec, x, t, fk->side[first + 2]);
-    bonded_forces_group<5, 6>(ff, prec, x, t, fk->side[first + 3]);
-    bonded_forces_group<0, 2>(ff, prec, x, t, fk->side[first + 3]);
-    launch_excl_forces(ff, prec, x, t, fs, s);
-}
-
-}  // namespace
-
 void launch_forces(const ChainDev& ch, const DeviceFF& ff, int prec, const double* x, const ForceTarget& t,
                    const ForceScratch& fs, cudaStream_t s, const Fork* fk) {
-    if (fk && !ch.act) {
-        launch_force_zero(ch, t, s);
-        cudaEventRecord(fk->mid, s);
-        forces_side_by_side(ch, ff, prec, x, t, fs, s, fk, 0);
-        for (int k = 0; k < 4; ++k) {
-            cudaEventRecord(fk->join[k], fk->side[k]);
-            cudaStreamWaitEvent(s, fk->join[k], 0);
-        }
-        return;
-    }
     // the chain pass stores every bead's force; everything after adds, in four
     // branches: excluded volume | linker, motor | branching | boundary,
     // filament leftovers
@@ -424,25 +395,30 @@ void launch_evaluate(const ChainDev& ch, const DeviceFF& ff, int prec, const dou
         return;
     }
     // side 0: excluded-volume energy, then the finish once sides 1-4 are done;
-    // sides 1-4: bonded groups and chain energy; main: the zero fill of the
-    // target, then the excluded-volume forces; sides 5-8: chain and bonded
-    // forces after the zero fill
-    fork_to(fk, s, 5);
+    // sides 1-4: bonded groups and chain energy; main: chain forces, then
+    // the excluded-volume forces; sides 5-7: bonded forces after the chain
+    // forces (which initialize the force array)
+    fork_to(fk, s, kForkWays);
     launch_excl_energy(ff, MEDYAN_PREC_FP64, x, d, lam, es, fk->side[0]);
     bonded_energy_group<2, 4>(ff, x, d, lam, es, fk->side[1]);
     bonded_energy_group<4, 5>(ff, x, d, lam, es, fk->side[2]);
     bonded_energy_group<5, 6>(ff, x, d, lam, es, fk->side[3]);
     bonded_energy_group<0, 2>(ff, x, d, lam, es, fk->side[3]);
     launch_chain_energy(ch, MEDYAN_PREC_FP64, x, d, lam, es.partial, es.total(), 0, fk->side[4], nullptr, 0);
-    launch_force_zero(ch, t, s);
+    launch_chain_forces(ch, prec, x, t, s);
     cudaEventRecord(fk->mid, s);
-    forces_side_by_side(ch, ff, prec, x, t, fs, s, fk, 5);
+    for (int k = 5; k < 8; ++k) cudaStreamWaitEvent(fk->side[k], fk->mid, 0);
+    bonded_forces_group<2, 4>(ff, prec, x, t, fk->side[5]);
+    bonded_forces_group<4, 5>(ff, prec, x, t, fk->side[6]);
+    bonded_forces_group<5, 6>(ff, prec, x, t, fk->side[7]);
+    bonded_forces_group<0, 2>(ff, prec, x, t, fk->side[7]);
+    launch_excl_forces(ff, prec, x, t, fs, s);
     for (int k = 1; k < 5; ++k) {
         cudaEventRecord(fk->join[k], fk->side[k]);
         cudaStreamWaitEvent(fk->side[0], fk->join[k], 0);
     }
     launch_excl_energy_fallback_and_finish(ff, x, d, lam, es, fk->side[0]);
-    for (int k : {0, 5, 6, 7, 8}) {
+    for (int k : {0, 5, 6, 7}) {
         cudaEventRecord(fk->join[k], fk->side[k]);
         cudaStreamWaitEvent(s, fk->join[k], 0);
     }

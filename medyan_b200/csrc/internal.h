@@ -120,7 +120,7 @@ struct ForceScratch {
 // independent kernels on separate streams joined back into the caller's
 // stream; under stream capture the fork and join become graph edges, so the
 // kernels are parallel branches of the graph.
-constexpr int kForkWays = 10;
+constexpr int kForkWays = 8;
 struct Fork {
     cudaStream_t side[kForkWays];
     cudaEvent_t fork, join[kForkWays];
@@ -141,11 +141,7 @@ void launch_evaluate(const ChainDev& ch, const DeviceFF& ff, int prec, const dou
                      const LambdaSet* lam,
                      const ForceTarget& t, const EnergyScratch& es, const ForceScratch& fs, cudaStream_t s,
                      const Fork* fk);
-// accumulate: add to the target instead of storing every bead's force (the
-// target was zeroed by launch_force_zero)
-void launch_chain_forces(const ChainDev& ch, int prec, const double* x, const ForceTarget& t, cudaStream_t s,
-                         bool accumulate = false);
-void launch_force_zero(const ChainDev& ch, const ForceTarget& t, cudaStream_t s);
+void launch_chain_forces(const ChainDev& ch, int prec, const double* x, const ForceTarget& t, cudaStream_t s);
 // table (optional): block b evaluates positions [table[b].y, table[b].z) of one
 // replica (batched layouts), table_blocks blocks; else a grid-stride pass.
 void launch_chain_energy(const ChainDev& ch, int prec, const double* x, const double* d, const LambdaSet* lam,
