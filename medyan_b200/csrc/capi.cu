@@ -383,6 +383,7 @@ medyan_status medyan_mech::init() {
     if (e == cudaSuccess) e = f_fb_list.reserve(kFallbackCap);
     if (e == cudaSuccess) e = force_status.reserve(1);
     if (e == cudaSuccess) e = lam_zero.reserve(1);
+    if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&small), sizeof(*small));
     if (e != cudaSuccess) return cuda_status(e);
     cudaMemsetAsync(x.raw(), 0, sizeof(double) * (n3 ? n3 : 1), stream);
     cudaMemsetAsync(e_fb_count.raw(), 0, sizeof(int), stream);
@@ -411,6 +412,7 @@ medyan_mech::~medyan_mech() {
     if (stream) cudaStreamSynchronize(stream);
     if (cg_graph) cudaGraphExecDestroy(cg_graph);
     if (cg_pinned) cudaFreeHost(cg_pinned);
+    if (small) cudaFreeHost(small);
     for (auto& g : pass_graph)
         if (g) cudaGraphExecDestroy(g);
     destroy_nl(this);
@@ -506,8 +508,8 @@ medyan_status medyan_mech_energy(medyan_mech* h, double* e_total, double* e_per_
     if (!h || !e_total) return MEDYAN_ERR_INVALID_ARG;
     cudaError_t e = launch_pass(h, kPassEnergy);
     if (e != cudaSuccess) return cuda_status(e);
-    double out[MEDYAN_FF_COUNT + 1];
-    e = cudaMemcpyAsync(out, h->energy_out.ptr(), sizeof out, cudaMemcpyDeviceToHost, h->stream);
+    double* out = h->small->energy;
+    e = cudaMemcpyAsync(out, h->energy_out.ptr(), sizeof h->small->energy, cudaMemcpyDeviceToHost, h->stream);
     if (e != cudaSuccess) return cuda_status(e);
     medyan_status st = sync_status(h);
     if (st != MEDYAN_OK) return st;
@@ -521,14 +523,15 @@ medyan_status medyan_mech_forces(medyan_mech* h, double* force_out) {
     if (!h || (!force_out && h->n_beads)) return MEDYAN_ERR_INVALID_ARG;
     cudaError_t e = launch_pass(h, kPassForces);
     if (e != cudaSuccess) return cuda_status(e);
-    int status = 0;
     e = coords_to_host(h, h->f.raw(), force_out, h->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&status, h->force_status.ptr(), sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(&h->small->force_status, h->force_status.ptr(), sizeof(int), cudaMemcpyDeviceToHost,
+                            h->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(h->force_status.ptr(), 0, sizeof(int), h->stream);
     if (e != cudaSuccess) return cuda_status(e);
     medyan_status st = sync_status(h);
     if (st != MEDYAN_OK) return st;
-    return status ? MEDYAN_ERR_NONFINITE : MEDYAN_OK;
+    return h->small->force_status ? MEDYAN_ERR_NONFINITE : MEDYAN_OK;
 }
 
 medyan_status medyan_mech_enqueue_energy(medyan_mech* h) {
@@ -581,18 +584,19 @@ medyan_status medyan_mech_evaluate(medyan_mech* h, const double* coord, double* 
     if (e != cudaSuccess) return cuda_status(e);
     e = launch_pass(h, kPassBoth);
     if (e != cudaSuccess) return cuda_status(e);
-    double out[MEDYAN_FF_COUNT + 1];
-    int status = 0;
-    e = cudaMemcpyAsync(out, h->energy_out.ptr(), sizeof out, cudaMemcpyDeviceToHost, h->stream);
+    double* out = h->small->energy;
+    e = cudaMemcpyAsync(out, h->energy_out.ptr(), sizeof h->small->energy, cudaMemcpyDeviceToHost, h->stream);
     if (e == cudaSuccess) e = coords_to_host(h, h->f.raw(), force_out, h->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&status, h->force_status.ptr(), sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(&h->small->force_status, h->force_status.ptr(), sizeof(int), cudaMemcpyDeviceToHost,
+                            h->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(h->force_status.ptr(), 0, sizeof(int), h->stream);
     if (e != cudaSuccess) return cuda_status(e);
     medyan_status st = sync_status(h);
     if (st != MEDYAN_OK) return st;
     *e_total = out[MEDYAN_FF_COUNT];
     if (e_per_ff) std::memcpy(e_per_ff, out, sizeof(double) * MEDYAN_FF_COUNT);
-    if (status) return MEDYAN_ERR_NONFINITE;
+    if (h->small->force_status) return MEDYAN_ERR_NONFINITE;
     if (std::isinf(out[MEDYAN_FF_COUNT])) return MEDYAN_ERR_NONFINITE;
     return MEDYAN_OK;
 }

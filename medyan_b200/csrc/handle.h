@@ -190,6 +190,12 @@ struct medyan_mech {
     // enqueueing it never waits on the device (batched minimization)
     unsigned char* cg_pinned = nullptr;
     size_t cg_pinned_bytes = 0;
+    // pinned landing area for the per-call results the host reads back
+    // (energies, force status), so their copies are asynchronous
+    struct SmallPinned {
+        double energy[MEDYAN_FF_COUNT + 1];
+        int force_status;
+    }* small = nullptr;
     int cg_graph_prec = -1;
     long long cg_graph_gen = -1;          // ff_gen the graph was captured with
     long long ff_gen = 0;                 // bumped whenever DeviceFF changes
