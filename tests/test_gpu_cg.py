@@ -129,6 +129,24 @@ def test_mixed_precision_matches_fp64_at_convergence(gpu_lib, oracle):
         assert r.grad_inf_norm < 1e-3 or r.energy_rel_change < 1e-16
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_returned_forces_are_those_at_the_returned_coordinates(gpu_lib, oracle, precision):
+    # The first line-search pass of an iteration can also compute the forces
+    # at its first trial step; when the line search takes that step, the
+    # iteration's force pass is skipped. Whichever path each iteration took,
+    # the forces a converged minimization returns are a fresh evaluation's at
+    # its final coordinates, up to the atomics' summation order.
+    sv, x = small_net(oracle, n_fil=30, cyl_per_fil=8, box=1000.0, n_linker=60, seed=11)
+    p = cgp(grad_tol=0.5)
+    with ForceFieldManager(precision) as ff:
+        ff.vectorize_all_force_fields(sv)
+        sg, xg, fg, rg = ff.minimize(x, p)
+        f_fresh = ff.compute_forces(xg)
+    assert sg == 0 and rg.num_iter > 20
+    assert np.abs(fg - f_fresh).max() <= 1e-12 * np.abs(f_fresh).max()
+    assert rg.grad_inf_norm == pytest.approx(np.abs(f_fresh).max(), rel=1e-12)
+
+
 def test_already_converged(gpu_lib, oracle):
     sv, x = small_net(oracle)
     p = cgp(grad_tol=1e12)
