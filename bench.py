@@ -317,13 +317,16 @@ def minimize_extras(net, make) -> dict:
     out = {}
     p = conjugate_gradient_params(grad_tol=1.0, max_dist=1.0, lambda_max=0.01, energy_rel_tol=1e-9)
     x = net.flat_coords()
+    warm = conjugate_gradient_params(grad_tol=1.0, energy_call_limit=3)
     for prec in ("fp64", "mixed"):
         ff = make(prec)
+        ff.minimize(x, warm)  # builds the minimizer's graph outside the timed call
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         st, xm, fm, r = ff.minimize(x, p)
         dt = time.perf_counter() - t0
         out[prec] = {"status": st, "seconds": dt, "minimizations_per_s": 1.0 / dt, "iterations": r.num_iter,
+                     "us_per_iteration": 1e6 * dt / max(r.num_iter, 1),
                      "energy_calls": r.num_energy_call, "force_calls": r.num_force_call,
                      "energy_before": r.energy_before_total, "energy_after": r.energy_after_total,
                      "grad_inf_norm": r.grad_inf_norm, "energy_rel_change": r.energy_rel_change}
