@@ -13,7 +13,9 @@
 //     sequential Armijo loop over them (so the accepted lambda and the energy
 //     call count are the reference's);
 //   force pass at x + lam*d into the force buffer that does not hold the
-//     current force;
+//     current force, unless the first line-search pass already computed
+//     those forces (speculatively, at its first trial step, when the
+//     previous line search took its first trial) and lam is that step;
 //   dots pass: commit x += lam*d, F.F, F.Fprev, max|F|;
 //     its last block computes beta (PR: max(0, (F.F - F.Fprev)/lastF.F));
 //   direction pass: d = F + beta*d (or F), d.F, max|d|; its last block checks
@@ -25,8 +27,9 @@
 // counted as an energy call as in the reference.
 //
 // The iteration runs as a CUDA graph whose loops are conditional WHILE nodes
-// (line-search passes inside, iterations outside), so a whole minimization is
-// one graph launch. The host only reads the result.
+// (line-search passes inside, iterations outside) and whose force pass sits
+// under a conditional IF node, so a whole minimization is one graph launch.
+// The host only reads the result.
 #include <cstring>
 #include <vector>
 

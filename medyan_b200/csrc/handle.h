@@ -78,7 +78,7 @@ struct CGState {
     int last_backtracks;   // halvings of the previous line search
     int k_trials;          // trial slots in the current pass
     // step bookkeeping
-    int skip_force;        // 1: no force pass this iteration
+    int skip_force;        // 1: no move this iteration (no force pass, no dots pass)
     int move_kind;         // 1: line-search step, 2: recovery step
     int dir_mode;          // 0: d = F + beta*d, 1: d = F
     int reset_after_dir;   // d.F <= 0 after the update: reset to d = F
