@@ -499,13 +499,12 @@ medyan_status medyan_batch_autotune(medyan_batch* b, int32_t reps, medyan_batch_
 /* ------------------------------------------------------------------------ */
 /* Excluded-volume energy without device allocation                          */
 /* ------------------------------------------------------------------------ */
-/* No counterpart in the reference. The reference's CylinderExclVolume energy
-   (src/Mechanics/ForceField/Volume/CylinderExclVolRepulsion.cpp) runs inside
-   ForceFieldManager, which this library covers through a handle. Handles
-   allocate device scratch with cudaMalloc. This entry point allocates
-   nothing, for callers that cannot let a library allocate device memory when
-   they need an energy. Examples: an application whose own pool allocator owns
-   the device, or a step loop whose device footprint must stay fixed.
+/* No counterpart in the reference: it has no entry point of this kind.
+   Handles allocate their device scratch with cudaMalloc. This entry point
+   allocates nothing, for callers that cannot let a library allocate device
+   memory when they need an energy. Examples: an application whose own pool
+   allocator owns the device, or a step loop whose device footprint must stay
+   fixed.
 
    Computes the excluded-volume energy of n_pairs cylinder pairs. All array
    pointers are DEVICE pointers on the current device, owned by the caller:
@@ -513,19 +512,24 @@ medyan_status medyan_batch_autotune(medyan_batch* b, int32_t reps, medyan_batch_
      d_excl_beads  int32[4*n_pairs]    coordinate offsets 3*bead, 16-byte aligned
      d_excl_krs    double[n_pairs]     krep * eqLength1 * eqLength2 per pair
    The kernels and the fallback for degenerate pairs are those of
-   medyan_mech_energy's excluded-volume slot, in FP64. The call enqueues on
-   `stream` (a cudaStream_t; NULL = legacy default stream), waits for it and
-   stores the energy in *e_out (host).
+   medyan_mech_energy's excluded-volume slot, in FP64. The call is
+   synchronous: it enqueues on `stream` (a cudaStream_t; NULL = legacy
+   default stream), waits for that stream and stores the energy in *e_out
+   (host).
 
    Scratch lives in a fixed static device array of the library, sized for
    MEDYAN_NOALLOC_MAX_EXCL_PAIRS pairs. Larger n_pairs returns
    MEDYAN_ERR_CAPACITY. Bead offsets outside [0, 3*n_beads) or not multiples
-   of 3 return MEDYAN_ERR_INDEX_RANGE before any energy kernel runs. A
-   non-finite pair energy returns MEDYAN_ERR_NONFINITE.
+   of 3 return MEDYAN_ERR_INDEX_RANGE before any energy kernel runs. When a
+   pair's energy is non-finite (or below -1) even after the quadrature
+   fallback, the call returns MEDYAN_ERR_NONFINITE and *e_out holds -1, the
+   value the reference's force field reports for a bad energy.
 
-   The first call on each device sets up: it looks up the scratch array's
-   address (cudaGetSymbolAddress) with that device current. Make that first
-   call before any stream capture begins. All calls on one device share the
+   Every call looks up the scratch array's device address on the current
+   device (cudaGetSymbolAddress). The first call on each device also fills
+   the fallback's quadrature grids once: make that first call before any
+   stream capture begins. A cudaDeviceReset discards that set-up: do not use
+   the library across a device reset. All calls on one device share the
    scratch: calls that overlap in time (other host threads, other streams)
    race and give wrong results, so serialize them. */
 #define MEDYAN_NOALLOC_MAX_EXCL_PAIRS 262144

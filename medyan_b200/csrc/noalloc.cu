@@ -12,16 +12,20 @@
 // fallback for degenerate pairs and the deterministic finish) with all
 // scratch in one fixed-size static device array of this library.
 //
-// Set-up: the first call on each device (with that device current) looks up
-// the array's device address with cudaGetSymbolAddress and prepares the
-// fallback kernel's shared-memory limit. Make that first call before any
-// stream capture begins on the device.
+// Set-up: every call looks up the array's device address on the current
+// device with cudaGetSymbolAddress (a cheap host query; the address is not
+// cached, so it stays right if the device's context is ever recreated). The
+// first call on each device also fills the quadrature grids of the fallback
+// for degenerate pairs, once; make that first call before any stream capture
+// begins on the device. A cudaDeviceReset discards that one-time set-up along
+// with every handle: do not use the library across a device reset.
+//
+// The call is synchronous: it waits for `stream` before it returns.
 //
 // The scratch array is shared by every call on a device: calls that overlap
 // in time on one device (two host threads, or two streams) race on it and
 // give wrong results. Serialize them.
 #include <cstring>
-#include <mutex>
 
 #include "handle.h"
 
@@ -47,26 +51,15 @@ static_assert(kFallbackCap <= kPartialOff - kFbListOff, "fallback-queue region")
 // About 129 KiB for the maximum of 262144 pairs.
 static __device__ __align__(256) double g_scratch[kScratchDoubles];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_setup_mu;
-double* g_scratch_ptr[kMaxDevices];
-
-// Symbol address of g_scratch on the current device, looked up once.
+// Device address of g_scratch on the current device, looked up on every
+// call; the excluded-volume kernels' one-time set-up runs on first use.
 cudaError_t scratch_on_current_device(double** out) {
-    int dev = -1;
-    cudaError_t e = cudaGetDevice(&dev);
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
     if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-    std::lock_guard<std::mutex> lock(g_setup_mu);
-    if (!g_scratch_ptr[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_scratch);
-        if (e != cudaSuccess) return e;
-        e = init_excl_kernels();
-        if (e != cudaSuccess) return e;
-        g_scratch_ptr[dev] = static_cast<double*>(p);
-    }
-    *out = g_scratch_ptr[dev];
+    e = init_excl_kernels();
+    if (e != cudaSuccess) return e;
+    *out = static_cast<double*>(p);
     return cudaSuccess;
 }
 

@@ -246,4 +246,6 @@ def main(ref_src: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src")
+    default = os.environ.get("MEDYAN_REF_SRC",
+                             os.path.join(os.path.dirname(os.path.dirname(os.path.dirname(HERE))), "reference", "src"))
+    main(sys.argv[1] if len(sys.argv) > 1 else default)

@@ -110,3 +110,37 @@ def test_batch_shapes_keep_results(gpu_lib, oracle):
         assert (rs0[r].num_energy_call, rs0[r].num_force_call) == (rs1[r].num_energy_call, rs1[r].num_force_call) \
             == (rs2[r].num_energy_call, rs2[r].num_force_call)
         assert np.abs(xs1[r] - xs0[r]).max() <= 1e-7 and np.abs(xs2[r] - xs0[r]).max() <= 1e-7
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_full_ensemble_start_state_matches_oracle(gpu_lib, oracle, precision):
+    """The whole 256-replica ensemble of the medium network's composition
+    (200-4,000 cylinders each), neighbor lists built on the device per
+    replica, as the benchmark runs it. A minimization whose gradient
+    tolerance holds at the start coordinates runs one packed energy pass and
+    one packed force pass and moves nothing: its energy_before_total and
+    returned forces are the packed kernels' values at the start coordinates,
+    checked against the oracle on 16 replicas spread over the size range."""
+    from medyan_b200.network import make_batch
+    nets = make_batch(256, 2)
+    xs = [net.flat_coords() for net in nets]
+    with BatchMinimizer([net.system_view() for net in nets], precision) as b:
+        for r, net in enumerate(nets):
+            bp, _ = net.boundary_params()
+            b.rebuild_neighbor_lists(r, xs[r], net.cylinders_view(), net.nl_params(), bp)
+        st, xo, fo, rs = b.minimize(xs, cgp(grad_tol=1e30))
+    tol = 1e-12 if precision == "fp64" else 1e-6
+    order = np.argsort([net.n_beads for net in nets])
+    sample = sorted(set(int(order[i]) for i in np.linspace(0, len(nets) - 1, 16).round().astype(int)))
+    assert len(sample) >= 8
+    for r in sample:
+        assert st[r] == 0 and rs[r].num_iter == 0
+        assert np.array_equal(xo[r], xs[r])
+        stc, extra = oracle.complete(nets[r])
+        assert stc == 0
+        sv = nets[r].system_view(**extra)
+        eo, _ = oracle.energy(sv, xs[r])
+        fref = oracle.forces(sv, xs[r])
+        # energies are FP64 in both precisions
+        assert abs(rs[r].energy_before_total - eo) <= 1e-12 * abs(eo), (r, rs[r].energy_before_total, eo)
+        assert np.abs(fo[r] - fref).max() <= tol * np.abs(fref).max(), r

@@ -89,6 +89,45 @@ def test_workload_networks(gpu_lib, oracle, cfg, precision):
           f"cfg{cfg}/{precision}")
 
 
+@pytest.fixture(scope="module")
+def cfg4(oracle):
+    """The 400k-cylinder network (20,000 filaments x 20 cylinders, 100k
+    linkers, 10k motors, 5k branch points) with the oracle's CPU neighbor
+    list and its energies and forces at the start coordinates."""
+    net = make_workload(4)
+    st, extra = oracle.complete(net)
+    assert st == 0
+    sv = net.system_view(**extra)
+    x = net.flat_coords()
+    eo, pero = oracle.energy(sv, x)
+    return net, extra, sv, x, eo, pero, oracle.forces(sv, x)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_large_network_matches_oracle(gpu_lib, cfg4, precision):
+    """The benchmark network, records from the oracle's vectorization."""
+    net, extra, sv, x, eo, pero, fo = cfg4
+    e, per, f = gpu_eval(sv, x, precision)
+    check(e, per, f, eo, pero, fo, FP64_TOL if precision == "fp64" else MIXED_TOL, f"cfg4/{precision}")
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_large_network_device_neighbor_list(gpu_lib, cfg4, precision):
+    """The benchmark's own path: excluded-volume and boundary records built
+    by the device neighbor list (their order differs from the oracle's, so the
+    sums agree to rounding), evaluated through the evaluate pass."""
+    net, extra, sv, x, eo, pero, fo = cfg4
+    bp, planes = net.boundary_params()
+    with ForceFieldManager(precision) as ff:
+        ff.vectorize_all_force_fields(net.system_view())
+        ff.set_coords(x)
+        ff.set_cylinders(net.cylinders_view(), net.nl_params(), bp)
+        ne, nb = ff.rebuild_neighbor_lists()
+        assert ne == extra["excl_beads"].shape[0] and nb == extra["boundary_beads"].shape[0]
+        e, per, f = ff.evaluate(x)
+    check(e, per, f, eo, pero, fo, FP64_TOL if precision == "fp64" else MIXED_TOL, f"cfg4-nl/{precision}")
+
+
 def test_reference_unit_inputs(gpu_lib):
     from tests.test_oracle_pins import unit_systems
     with open(os.path.join(GOLDEN, "reference_unit_inputs.json")) as fh:

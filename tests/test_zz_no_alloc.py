@@ -55,6 +55,28 @@ def test_matches_handle_path_twice(gpu_lib, oracle, cfg, seed):
         assert abs(got - want) <= REL_TOL * abs(want), (got, want)
 
 
+def test_calls_allocate_no_device_memory(gpu_lib, oracle):
+    """The property the entry point exists for: after one warm-up call (which
+    loads the library's kernels on the device), further calls leave the
+    device's free memory and torch's allocator untouched."""
+    import torch
+
+    net, extra, x, dev = _device_inputs(1, 0, oracle)
+    n_pairs = extra["excl_beads"].shape[0]
+    st, e0 = _noalloc(dev, net.n_beads, n_pairs)
+    assert st == 0
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    alloc0 = torch.cuda.memory_allocated()
+    for _ in range(5):
+        st, e = _noalloc(dev, net.n_beads, n_pairs)
+        assert st == 0 and e == e0
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
+    assert torch.cuda.memory_allocated() == alloc0
+
+
 def test_limits_and_bad_offsets(gpu_lib, oracle):
     net, extra, x, dev = _device_inputs(0, 0, oracle)
     n_pairs = extra["excl_beads"].shape[0]
