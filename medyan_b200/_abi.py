@@ -127,7 +127,7 @@ class MedyanCylinders(C.Structure):
 
 class LaunchShapes(C.Structure):
     _fields_ = [("bonded_threads", C.c_int32), ("excl_threads", C.c_int32), ("chain_threads", C.c_int32),
-                ("chain_energy_blocks_per_sm", C.c_int32)]
+                ("chain_energy_blocks_per_sm", C.c_int32), ("pass_layout", C.c_int32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -1,8 +1,11 @@
 """Builds the CUDA library in-tree: medyan_b200/libmedyan_b200.so (sm_100a).
 
 Each translation unit is compiled by nvcc to an object under medyan_b200/_build/
-and linked into one shared library. excl_kernels.cu is compiled without FMA
-contraction (see the file's header). Run: python -m medyan_b200.build
+and linked into one shared library. Every file is compiled without FMA
+contraction: the excluded-volume formula needs it to round as the reference
+does (see excl_kernels.cu), and a force computed by two different kernels
+(the fused pass, the per-potential kernels of the speculative pass and of
+packed batches) must round the same way in both. Run: python -m medyan_b200.build
 """
 from __future__ import annotations
 
@@ -16,11 +19,11 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libmedyan_b200.so")
 
-SOURCES = ["capi.cu", "ff_kernels.cu", "chain.cu", "excl_kernels.cu", "nl.cu", "cg.cu", "batch.cu", "pbatch.cu", "diff.cu", "hessian.cu", "aux.cu", "tune.cu", "noalloc.cu"]
+SOURCES = ["capi.cu", "ff_kernels.cu", "chain.cu", "excl_kernels.cu", "nl.cu", "cg.cu", "batch.cu", "pbatch.cu", "diff.cu", "hessian.cu", "aux.cu", "tune.cu", "noalloc.cu", "pass.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + os.path.join(ROOT, "include"),
-          "-I" + CSRC, "--expt-relaxed-constexpr"]
-PER_FILE = {"excl_kernels.cu": ["--fmad=false"], "aux.cu": ["--fmad=false"]}
+          "-I" + CSRC, "--expt-relaxed-constexpr", "--fmad=false"]
+PER_FILE: dict[str, list[str]] = {}
 
 
 def nvcc() -> str:

@@ -266,6 +266,17 @@ medyan_status refresh_device_ff(medyan_mech* h) {
     h->es.n_blocks_excl = excl_blocks(ff);
     const size_t need = (size_t)kMaxLambda * (h->es.total() + 1) * 4;
     cudaError_t e = h->partial.reserve(need);
+    {
+        // fused-pass scratch; the group tickets start at zero (stream-ordered
+        // after every pass already enqueued on the handle's stream)
+        const PassGeometry pg = pass_geometry(h->chain, ff);
+        if (e == cudaSuccess) e = h->pass_rows.reserve((size_t)pg.rows * MEDYAN_FF_COUNT);
+        if (e == cudaSuccess) e = h->pass_group_rows.reserve((size_t)pg.groups * MEDYAN_FF_COUNT);
+        if (e == cudaSuccess) e = h->pass_group_ticket.reserve((size_t)pg.groups);
+        if (e == cudaSuccess)
+            e = cudaMemsetAsync(h->pass_group_ticket.raw(), 0, sizeof(unsigned int) * h->pass_group_ticket.cap,
+                                h->stream);
+    }
     if (e != cudaSuccess) return cuda_status(e);
     h->es.partial = h->partial.ptr();
     h->ff_gen++;
@@ -285,8 +296,15 @@ void enqueue_energy(medyan_mech* h, const double* x, const double* d, const Lamb
 }
 
 void enqueue_forces(medyan_mech* h, const double* x, double* f, cudaStream_t s) {
-    launch_forces(h->chain, h->ff, h->prec, x, ForceTarget{f, nullptr, nullptr, nullptr, nullptr, nullptr}, h->fs, s,
-                  &h->fork);
+    enqueue_force_target(h, x, ForceTarget{f, nullptr, nullptr, nullptr, nullptr, nullptr}, h->fs, s);
+}
+
+void enqueue_force_target(medyan_mech* h, const double* x, const ForceTarget& t, const ForceScratch& fs,
+                          cudaStream_t s) {
+    if (h->pass_layout == 0)
+        launch_pass_fused(h->chain, h->ff, h->prec, x, &t, false, nullptr, h->es, fs, h->pass_scratch(), s, &h->fork);
+    else
+        launch_forces(h->chain, h->ff, h->prec, x, t, fs, s, &h->fork);
 }
 
 cudaError_t coords_to_device(medyan_mech* h, const double* host, double* dev, cudaStream_t s) {
@@ -331,9 +349,13 @@ cudaError_t ensure_pass_graph(medyan_mech* h, int which) {
     h->pass_graph[which] = nullptr;
     cudaError_t e = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return e;
-    if (which == kPassBoth)
-        launch_evaluate(h->chain, h->ff, h->prec, h->x.raw(), nullptr, h->lam_zero.raw(),
-                        ForceTarget{h->f.raw(), nullptr, nullptr, nullptr, nullptr, nullptr}, h->es, h->fs, h->stream,
+    const ForceTarget t{h->f.raw(), nullptr, nullptr, nullptr, nullptr, nullptr};
+    if (h->pass_layout == 0)
+        launch_pass_fused(h->chain, h->ff, h->prec, h->x.raw(), which == kPassEnergy ? nullptr : &t,
+                          which != kPassForces, h->lam_zero.raw(), h->es, h->fs, h->pass_scratch(), h->stream,
+                          &h->fork);
+    else if (which == kPassBoth)
+        launch_evaluate(h->chain, h->ff, h->prec, h->x.raw(), nullptr, h->lam_zero.raw(), t, h->es, h->fs, h->stream,
                         &h->fork);
     else if (which == kPassEnergy)
         enqueue_energy(h, h->x.raw(), nullptr, h->lam_zero.raw(), h->stream);
@@ -370,6 +392,7 @@ medyan_status medyan_mech::init() {
     for (int k = 0; k < kForkWays && e == cudaSuccess; ++k)
         e = cudaEventCreateWithFlags(&fork.join[k], cudaEventDisableTiming);
     if (e == cudaSuccess) e = init_excl_kernels();
+    if (e == cudaSuccess) e = init_pass_kernels();
     const size_t n3 = 3 * (size_t)n_beads;
     if (e == cudaSuccess) e = x.reserve(n3);
     if (e == cudaSuccess) e = f.reserve(n3);
@@ -383,6 +406,7 @@ medyan_status medyan_mech::init() {
     if (e == cudaSuccess) e = f_fb_list.reserve(kFallbackCap);
     if (e == cudaSuccess) e = force_status.reserve(1);
     if (e == cudaSuccess) e = lam_zero.reserve(1);
+    if (e == cudaSuccess) e = pass_ticket.reserve(1);
     if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&small), sizeof(*small));
     if (e != cudaSuccess) return cuda_status(e);
     cudaMemsetAsync(x.raw(), 0, sizeof(double) * (n3 ? n3 : 1), stream);
@@ -391,6 +415,7 @@ medyan_status medyan_mech::init() {
     cudaMemsetAsync(e_ticket.raw(), 0, sizeof(unsigned int), stream);
     cudaMemsetAsync(f_fb_count.raw(), 0, sizeof(int), stream);
     cudaMemsetAsync(force_status.raw(), 0, sizeof(int), stream);
+    cudaMemsetAsync(pass_ticket.raw(), 0, sizeof(unsigned int), stream);
     LambdaSet z{};
     z.K = 1;
     e = lam_zero.assign(&z, 1, stream);
@@ -428,7 +453,7 @@ medyan_mech::~medyan_mech() {
 // ---------------------------------------------------------------------------
 extern "C" {
 
-int32_t medyan_abi_version(void) { return 1; }
+int32_t medyan_abi_version(void) { return 2; }
 
 const char* medyan_last_cuda_error(void) {
     return t_last_cuda_error == cudaSuccess ? "" : cudaGetErrorName(t_last_cuda_error);

@@ -833,7 +833,7 @@ void enqueue_ls_pass(const CGLaunch& c, cudaStream_t s, cudaGraphConditionalHand
 }
 
 void enqueue_force_pass(const CGLaunch& c, cudaStream_t s) {
-    launch_forces(c.h->chain, c.h->ff, c.h->prec, c.x, c.tgt, c.h->fs, s, &c.h->fork);
+    enqueue_force_target(c.h, c.x, c.tgt, c.h->fs, s);
 }
 
 // The move and its dots, the new direction. cond_iter: in the loop graph,

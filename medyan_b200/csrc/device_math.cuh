@@ -61,12 +61,19 @@ __device__ __forceinline__ bool are_equal(double a, double b) { return fabs(a - 
 template <class R>
 __device__ __forceinline__ R stdmax(R a, R b) { return (a < b) ? b : a; }
 
+// f[0] += v at device scope without reading the old value back: a reduction
+// (red) rather than an atomic that returns (atomicAdd whose result is unused
+// still waits for the L2's answer), so the thread does not stall on it.
+__device__ __forceinline__ void red_add(double* p, double v) {
+    asm volatile("red.global.add.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");
+}
+
 // Accumulate an R-valued force into the FP64 force array.
 template <class R>
 __device__ __forceinline__ void add_force(double* __restrict__ f, int off, R fx, R fy, R fz) {
-    atomicAdd(f + off, double(fx));
-    atomicAdd(f + off + 1, double(fy));
-    atomicAdd(f + off + 2, double(fz));
+    red_add(f + off, double(fx));
+    red_add(f + off + 1, double(fy));
+    red_add(f + off + 2, double(fz));
 }
 
 // Block-wide sum of NV values per thread into smem-reduced totals held by

@@ -122,16 +122,19 @@ __device__ __forceinline__ bool bad_force(R x) {
     return isinf(x) || isnan(x) || fabs(double(x)) > 1e15;
 }
 
-// Analytic pair forces (:578-882). Returns false when any component is
-// non-finite or above 1e15 (the caller then uses the quadrature fallback).
+// Analytic pair forces (:578-882), regrouped: the mixed-precision mode's
+// form. Returns false when any component is non-finite or above 1e15 (the
+// caller then uses the quadrature fallback).
 //
 // The kernel is bound by FP64 throughput, and division is the costliest FP64
 // operation in the formula. The expression is the reference's, regrouped so
 // that each of the four arctangent blocks (A: a,c,e; E: a,|c1-c4|^2,g;
 // B: b,c,F; F: b,|c3-c2|^2,h) divides once for 1/Q and twice for its two
 // weights, instead of about a dozen times (x/Q, x/Q^2, x/Q^3 become
-// products with 1/Q). Results agree with the reference's order to rounding;
-// the forces are summed with atomics and so are not bitwise in any case.
+// products with 1/Q). Results agree with the reference's order to a few
+// ulps for most pairs, but near-parallel pairs amplify that to ~1e-8
+// relative within the pair: well inside the mixed mode's 1e-6 force
+// tolerance, outside the FP64 mode's 1e-12, which uses excl_force_exact.
 template <class R>
 struct ExclBlockF {
     R iQ, cN, cQ, cd, c1, T;  // 1/Q, the four coefficients, N/Q*ATG
@@ -158,7 +161,7 @@ __device__ __forceinline__ ExclBlockF<R> excl_force_block(R alpha, R beta, R gam
 }
 
 template <class R>
-__device__ __forceinline__ bool excl_force(const V3& c1, V3 c2, const V3& c3, const V3& c4, double kRS,
+__device__ __forceinline__ bool excl_force_fast(const V3& c1, V3 c2, const V3& c3, const V3& c4, double kRS,
                                            T3<R> (&fo)[4]) {
     if (in_plane(c1, c2, c3, c4)) c2 = move_bead2_out_of_plane(c1, c2, c3, 0.01);
     T3<R> r12 = diff<R>(c1, c2), r34 = diff<R>(c3, c4), r31 = diff<R>(c3, c1), r14 = diff<R>(c1, c4),
@@ -228,6 +231,101 @@ __device__ __forceinline__ bool excl_force(const V3& c1, V3 c2, const V3& c3, co
         bad |= bad_force(fo[bi].x) | bad_force(fo[bi].y) | bad_force(fo[bi].z);
     }
     return !bad;
+}
+
+// Analytic pair forces (:578-882) in the reference's expression order: the
+// FP64 mode's form. Near-parallel pairs cancel heavily in the b_ij sums, so
+// only the reference's own order keeps the forces within 1e-12 of it there
+// (on the 400k-cylinder network one pair at cos 0.993 is 3e-8 relative off
+// with any other grouping; the reference's own fast-math build is 1e-9 off).
+// Returns false when any component is non-finite or above 1e15 (the caller
+// then uses the quadrature fallback).
+template <class R>
+__device__ __forceinline__ bool excl_force_exact(const V3& c1, V3 c2, const V3& c3, const V3& c4, double kRS,
+                                           T3<R> (&fo)[4]) {
+    if (in_plane(c1, c2, c3, c4)) c2 = move_bead2_out_of_plane(c1, c2, c3, 0.01);
+    ExclS<R> S;
+    excl_scalars<R>(c1, c2, c3, c4, S);
+    const R a = S.a, b = S.b, c = S.c, d = S.d, e = S.e, F = S.F;
+    const R AA = S.AA, BB = S.BB, CC = S.CC, DD = S.DD, EE = S.EE, FF = S.FF, GG = S.GG, HH = S.HH;
+    const R JJ = S.JJ, ATG1 = S.ATG1, ATG2 = S.ATG2, ATG3 = S.ATG3, ATG4 = S.ATG4;
+    const R invJJ = R(1) / JJ;
+    const R sumBlock = CC / AA * ATG1 + GG / EE * ATG2 + DD / BB * ATG3 + HH / FF * ATG4;
+    const R enFactor = R(kRS) * invJJ / R(2);
+    const R A1 = AA * AA / (AA * AA + (a + e) * (a + e));
+    const R A2 = AA * AA / (AA * AA + e * e);
+    const R E1 = EE * EE / (EE * EE + (a + e - d) * (a + e - d));
+    const R E2 = EE * EE / (EE * EE + (e - d) * (e - d));
+    const R B1 = BB * BB / (BB * BB + F * F);
+    const R B2 = BB * BB / (BB * BB + (F - b) * (F - b));
+    const R F1 = FF * FF / (FF * FF + (d + F) * (d + F));
+    const R F2 = FF * FF / (FF * FF + (d + F - b) * (d + F - b));
+    const R bA_C = ATG1 / AA;
+    const R bA_A = -(ATG1 * CC) / (AA * AA) + (-A1 * (a + e) + A2 * e) * CC / (AA * AA * AA);
+    const R bA_e = ((A1 - A2) * CC) / (AA * AA);
+    const R bA_a = (A1 * CC) / (AA * AA);
+    const R bE_G = ATG2 / EE;
+    const R bE_E = -(ATG2 * GG) / (EE * EE) + (-E1 * (a + e - d) + E2 * (e - d)) * GG / (EE * EE * EE);
+    const R bE_emd = ((E1 - E2) * GG) / (EE * EE);
+    const R bE_a = (E1 * GG) / (EE * EE);
+    const R bB_D = ATG3 / BB;
+    const R bB_B = -(ATG3 * DD) / (BB * BB) + (-B1 * F + B2 * (F - b)) * DD / (BB * BB * BB);
+    const R bB_fmb = ((B1 - B2) * DD) / (BB * BB);
+    const R bB_b = (B1 * DD) / (BB * BB);
+    const R bF_H = ATG4 / FF;
+    const R bF_F = -(ATG4 * HH) / (FF * FF) + (-F1 * (d + F) + F2 * (d + F - b)) * HH / (FF * FF * FF);
+    const R bF_dpfmb = ((F1 - F2) * HH) / (FF * FF);
+    const R bF_b = (F1 * HH) / (FF * FF);
+    const R b11 = bA_C * (-2 * F) + bA_A * (c / AA) + bA_a * 2 + bE_G * (2 * (F - b)) + bE_E * ((b + c - 2 * F) / EE) +
+                  bE_a * 2 + bF_H * (-2 * b) + bF_F * (b / FF);
+    const R b12 = bA_C * e + bE_G * (2 * d - e) + bE_E * ((e - d) / EE) + bE_emd * (-1) + bB_D * (-F) +
+                  bF_H * (2 * d + F) + bF_F * (-(d + F) / FF) + bF_dpfmb;
+    const R b13 = bA_C * d + bA_A * (-e / AA) + bA_e + bE_G * (-d) + bE_E * (-(e - d) / EE) + bE_emd + bB_D * b +
+                  bF_H * (-b) + bF_F * (b / FF);
+    const R b21 = b12;
+    const R b22 = bE_G * (-2 * a) + bE_E * (a / EE) + bB_D * (2 * e) + bB_B * (c / BB) + bB_fmb * (-2) + bB_b * 2 +
+                  bF_H * (-2 * (a + e)) + bF_F * ((a + c + 2 * e) / FF) + bF_dpfmb * (-2) + bF_b * 2;
+    const R b23 = bA_C * (-a) + bE_G * a + bE_E * (-a / EE) + bB_D * (-d) + bB_B * (-F / BB) + bB_fmb + bF_H * d +
+                  bF_F * (-(d + F) / FF) + bF_dpfmb;
+    const R b31 = b13;
+    const R b32 = b23;
+    const R b33 = bA_A * (a / AA) + bE_E * (a / EE) + bB_B * (b / BB) + bF_F * (b / FF);
+    const R J11 = 2 * (-b * c + F * F), J12 = 2 * (c * d - e * F), J13 = 2 * (b * e - d * F);
+    const R J21 = 2 * (c * d - e * F), J22 = 2 * (-a * c + e * e), J23 = 2 * (-d * e + a * F);
+    const R J31 = 2 * (b * e - d * F), J32 = 2 * (-d * e + a * F), J33 = 2 * (d * d - a * b);
+    const R q = -invJJ * sumBlock;
+    R dv[4][3];
+    dv[0][0] = enFactor * (q * (J31 - J11) + (b31 - b11));
+    dv[0][1] = enFactor * (q * (J32 - J12) + (b32 - b12));
+    dv[0][2] = enFactor * (q * (J33 - J13) + (b33 - b13));
+    dv[1][0] = enFactor * (q * (J11) + (b11));
+    dv[1][1] = enFactor * (q * (J12) + (b12));
+    dv[1][2] = enFactor * (q * (J13) + (b13));
+    dv[2][0] = enFactor * (q * (-J31 - J21) + (-b31 - b21));
+    dv[2][1] = enFactor * (q * (-J32 - J22) + (-b32 - b22));
+    dv[2][2] = enFactor * (q * (-J33 - J23) + (-b33 - b23));
+    dv[3][0] = enFactor * (q * (J21) + (b21));
+    dv[3][1] = enFactor * (q * (J22) + (b22));
+    dv[3][2] = enFactor * (q * (J23) + (b23));
+    const T3<R> u = diff<R>(c1, c2), v = diff<R>(c3, c4), w = diff<R>(c3, c1);
+    bool bad = false;
+#pragma unroll
+    for (int bi = 0; bi < 4; ++bi) {
+        fo[bi].x = -(dv[bi][0] * u.x + dv[bi][1] * v.x + dv[bi][2] * w.x);
+        fo[bi].y = -(dv[bi][0] * u.y + dv[bi][1] * v.y + dv[bi][2] * w.y);
+        fo[bi].z = -(dv[bi][0] * u.z + dv[bi][1] * v.z + dv[bi][2] * w.z);
+        bad |= bad_force(fo[bi].x) | bad_force(fo[bi].y) | bad_force(fo[bi].z);
+    }
+    return !bad;
+}
+
+// The form each precision mode uses: FP64 the reference's order, mixed the
+// regrouped one.
+template <bool EXACT>
+__device__ __forceinline__ bool excl_force(const V3& c1, const V3& c2, const V3& c3, const V3& c4, double kRS,
+                                           T3<double> (&fo)[4]) {
+    if constexpr (EXACT) return excl_force_exact<double>(c1, c2, c3, c4, kRS, fo);
+    else return excl_force_fast<double>(c1, c2, c3, c4, kRS, fo);
 }
 
 }  // namespace mb

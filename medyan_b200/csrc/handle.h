@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "internal.h"
+#include "pass.h"
 
 namespace mb {
 
@@ -140,6 +141,13 @@ struct medyan_mech {
     mb::DeviceFF ff{};
     mb::EnergyScratch es{};
     mb::ForceScratch fs{};
+    // fused passes (pass.cu): layout choice, energy rows and arrival ticket
+    int pass_layout = 1;                  // 0 fused, 1 one kernel per potential group
+    mb::DevBuf<double> pass_rows, pass_group_rows;
+    mb::DevBuf<unsigned int> pass_group_ticket, pass_ticket;
+    mb::PassScratch pass_scratch() const {
+        return mb::PassScratch{pass_rows.raw(), pass_group_rows.raw(), pass_group_ticket.raw(), pass_ticket.raw()};
+    }
 
     // internal bead order (chain.cu), fixed at create: internal position p
     // holds the caller's bead order_host[p]; pos_host is the inverse.
@@ -216,6 +224,10 @@ medyan_status refresh_device_ff(medyan_mech* h);
 medyan_status sync_status(medyan_mech* h);
 void enqueue_energy(medyan_mech* h, const double* x, const double* d, const LambdaSet* lam, cudaStream_t s);
 void enqueue_forces(medyan_mech* h, const double* x, double* f, cudaStream_t s);
+// The handle's force pass into target t (the minimizer's force pass), in
+// the handle's pass layout.
+void enqueue_force_target(medyan_mech* h, const double* x, const ForceTarget& t, const ForceScratch& fs,
+                          cudaStream_t s);
 // Energy (kPassEnergy), forces (kPassForces) or both at h->x into h->es.out /
 // h->f, launched as the handle's graph for that pass (rebuilt when the force
 // fields change).

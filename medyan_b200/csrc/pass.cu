@@ -1,0 +1,671 @@
+// pass.cu — fused single-network passes: the energy and/or the forces of
+// every force field at one set of positions, in one zero fill and three
+// kernels that run side by side.
+//
+//   k_pass_zero    zeroes the force target (force passes only);
+//   k_pass_main    filament chains (warp tiles of 30 consecutive beads, as in
+//                  chain.cu) and the generic records of filament leftovers,
+//                  linkers, motors and boundary terms;
+//   k_pass_branch  branch points (their four potentials need more registers
+//                  than the rest, so they get their own kernel);
+//   k_pass_excl    cylinder excluded volume (FP64 in both precision modes).
+//
+// Every contribution to a bead's force is added atomically into the zeroed
+// target, so the three kernels have no order among themselves and the graph
+// runs them concurrently: the FP64-heavy excluded-volume pairs overlap the
+// bandwidth-bound chain tiles and the gather-bound linker records instead of
+// following them. Energy and force of an interaction come from one read of
+// its record and its beads' positions.
+//
+// Energies: each block writes one row of per-force-field sums (fixed
+// reduction tree), and takes a ticket shared by all three kernels. The block
+// that takes the last ticket, whichever kernel it belongs to, sums the rows
+// in row order (deterministic for a given grid), runs the quadrature
+// fallbacks (energyN / forceN) for the pairs the analytic formulas rejected,
+// applies ForceFieldManager::computeEnergy's rule (a force field at or below
+// -1 makes the total +inf, ForceFieldManager.cpp:137-176) and resets the
+// ticket and the queues. No block waits for another: the last one to finish
+// does the finishing work.
+//
+// Built with --fmad=false (the excluded-volume formula and the quadrature
+// fallbacks round as the reference's code does).
+#include "handle.h"
+#include "potentials.cuh"
+#include "excl.cuh"
+#include "quadrature.cuh"
+#include "pass.h"
+
+#include <mutex>
+
+namespace mb {
+
+namespace {
+
+constexpr int kSlots = MEDYAN_FF_COUNT;
+constexpr int kWarpOut = 30;  // forces written per warp tile: lanes 1..30 of 32 centres
+constexpr unsigned char kLink = 1, kBend = 2;
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kZeroThreads = 256;
+// 64 registers (80 for energy and forces together): the chain tiles and the
+// linker gathers want occupancy
+constexpr int kMainBlocksPerSM = 4;
+constexpr int kExclThreadsMax = 128;
+
+__device__ __forceinline__ V3 shfl_up3(const V3& v) {
+    return V3{__shfl_up_sync(kFull, v.x, 1), __shfl_up_sync(kFull, v.y, 1), __shfl_up_sync(kFull, v.z, 1)};
+}
+__device__ __forceinline__ V3 shfl_down3(const V3& v) {
+    return V3{__shfl_down_sync(kFull, v.x, 1), __shfl_down_sync(kFull, v.y, 1), __shfl_down_sync(kFull, v.z, 1)};
+}
+template <class R>
+__device__ __forceinline__ T3<R> shfl_up3(const T3<R>& v) {
+    return T3<R>{__shfl_up_sync(kFull, v.x, 1), __shfl_up_sync(kFull, v.y, 1), __shfl_up_sync(kFull, v.z, 1)};
+}
+template <class R>
+__device__ __forceinline__ T3<R> shfl_down3(const T3<R>& v) {
+    return T3<R>{__shfl_down_sync(kFull, v.x, 1), __shfl_down_sync(kFull, v.y, 1), __shfl_down_sync(kFull, v.z, 1)};
+}
+
+// Positions of a pass: x, or x + lam*d rounded as calcCoordLineSearch.
+struct Pos {
+    const double* __restrict__ x;
+    const double* __restrict__ d;
+    double lam;
+    __device__ __forceinline__ V3 operator()(int o) const {
+        const V3 p = load3(x + o);
+        return d ? move3(p, lam, load3(d + o)) : p;
+    }
+};
+
+__device__ __forceinline__ Pos pos_of(const PassArgs& a) { return Pos{a.x, a.t.d, a.t.lam ? *a.t.lam : 0.0}; }
+
+// ------------------------------------------------------------ finish
+// Energy rows: each kernel's blocks hold a few per-thread sums, mapped to
+// force-field slots by the kernel kind (0 main: filament stretching and
+// bending, linker, motor, boundary; 1 branch: the four branching slots;
+// 2 excluded volume).
+constexpr int kMainVals = 5, kBranchVals = 4, kExclVals = 1;
+template <int KIND>
+__device__ constexpr int slot_of(int j) {
+    return KIND == 0 ? (j == 4 ? MEDYAN_FF_BOUNDARY : j)
+                     : (KIND == 1 ? MEDYAN_FF_BRANCHING_STRETCHING + j : MEDYAN_FF_EXCLUDED_VOLUME);
+}
+
+// Energy rows are summed by a fixed tree over arrival tickets. Row r belongs
+// to group r / kGroup; the block that completes a group (its group ticket)
+// sums the group's rows with one warp (lane j holds row kGroup*g + j, then a
+// fixed shuffle tree) into a group row, and takes the pass ticket; the block
+// that completes the last group sums the group rows the same way and
+// finishes. Which blocks do this varies from pass to pass; the order of every
+// addition does not.
+constexpr int kGroup = kPassGroup;
+
+// Sum over lanes of v (lane j's value), fixed tree; valid in lane 0.
+__device__ __forceinline__ double warp_tree(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(kFull, v, o);
+    return v;
+}
+
+// Runs the queued fallbacks and writes the results from the group rows;
+// called by the block that completes the last group (all its threads).
+template <bool E, bool F>
+__device__ __noinline__ void pass_finish(const PassArgs& a) {
+    __shared__ double red[6 * 32];
+    __shared__ double sums[kSlots];
+    __shared__ double fbE;
+    __shared__ int nfb;
+    const Pos P = pos_of(a);
+    if constexpr (E) {
+        if (threadIdx.x < 32) {
+            const int ng = (a.n_rows + kGroup - 1) / kGroup;
+            for (int s = 0; s < kSlots; ++s) {
+                double v = 0.0;
+                for (int g = threadIdx.x; g < ng; g += 32) v += __ldcg(a.group_rows + (size_t)s * a.n_groups + g);
+                v = warp_tree(v);
+                if (threadIdx.x == 0) sums[s] = v;
+            }
+        }
+        if (threadIdx.x == 0) {
+            // queued pairs in pair order (the queue fills in arrival order)
+            const int n = min(__ldcg(a.e_fb_count), kFallbackCap);
+            for (int i = 1; i < n; ++i) {
+                const int2 q = __ldcg(a.e_fb_list + i);
+                int j = i - 1;
+                while (j >= 0 && __ldcg(a.e_fb_list + j).x > q.x) {
+                    a.e_fb_list[j + 1] = __ldcg(a.e_fb_list + j);
+                    --j;
+                }
+                a.e_fb_list[j + 1] = q;
+            }
+            nfb = n;
+            fbE = 0.0;
+        }
+        __syncthreads();
+        for (int q = 0; q < nfb; ++q) {
+            const int i = __ldcg(a.e_fb_list + q).x;
+            const int4 bs = a.ff.excl_bs[i];
+            const double U = energyN_block(six_of(P(bs.x), P(bs.y), P(bs.z), P(bs.w)), a.ff.excl_krs[i], red);
+            if (threadIdx.x == 0) {
+                if (excl_energy_bad(U)) atomicOr(a.e_bad, 1);
+                else fbE += U;
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            double v[kSlots];
+#pragma unroll
+            for (int s = 0; s < kSlots; ++s) v[s] = sums[s];
+            double tot = 0.0;
+            bool inf = false;
+            v[MEDYAN_FF_EXCLUDED_VOLUME] += fbE;
+            if (__ldcg(a.e_bad)) v[MEDYAN_FF_EXCLUDED_VOLUME] = -1.0;
+#pragma unroll
+            for (int s = 0; s < kSlots; ++s) {
+                if (v[s] <= -1) inf = true;
+                else tot += v[s];
+            }
+            const double total = inf ? __longlong_as_double(0x7ff0000000000000ULL) : tot;
+            // a plain pass writes its one evaluation to every requested slot
+            const int K = a.lam_set ? a.lam_set->K : 1;
+            for (int k = 0; k < K; ++k) {
+                double* o = a.out + k * (kSlots + 1);
+#pragma unroll
+                for (int s = 0; s < kSlots; ++s) o[s] = v[s];
+                o[kSlots] = total;
+            }
+            *a.e_fb_count = 0;
+            for (int k = 0; k < kMaxLambda; ++k) a.e_bad[k] = 0;
+        }
+    }
+    if constexpr (F) {
+        double* __restrict__ f = target_force(a.t);
+        const int n = min(__ldcg(a.f_fb_count), kFallbackCap);
+        for (int q = 0; q < n; ++q) {
+            const int i = __ldcg(a.f_fb_list + q);
+            const int4 bs = a.ff.excl_bs[i];
+            const V3 c1 = P(bs.x), c2 = P(bs.y), c3 = P(bs.z), c4 = P(bs.w);
+            double out[4][3];
+            bool ok = forceN_block(c1, c2, c3, c4, a.ff.excl_krs[i], false, red, out);
+            if (!ok) ok = forceN_block(c1, c2, c3, c4, a.ff.excl_krs[i], true, red, out);
+            if (threadIdx.x == 0) {
+                if (ok) {
+                    add_force(f, bs.x, out[0][0], out[0][1], out[0][2]);
+                    add_force(f, bs.y, out[1][0], out[1][1], out[1][2]);
+                    add_force(f, bs.z, out[2][0], out[2][1], out[2][2]);
+                    add_force(f, bs.w, out[3][0], out[3][1], out[3][2]);
+                } else {
+                    atomicOr(a.f_status, 1);
+                }
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) *a.f_fb_count = 0;
+    }
+    if (threadIdx.x == 0) *a.ticket = 0u;
+}
+
+// Writes the block's energy row, takes its group's ticket and, for the block
+// that completes a group, sums the group and takes the pass ticket; the
+// block that completes the last group finishes the pass.
+template <int KIND, bool E, bool F, int NV>
+__device__ __forceinline__ void block_done(const PassArgs& a, double (&acc)[NV], int row, bool queued) {
+    __shared__ double smem[NV * 32];
+    __shared__ int state;  // 0 not last in its group, 1 completed its group, 2 completed the pass
+    if constexpr (E) {
+        block_sum<NV>(acc, smem);
+        if (threadIdx.x == 0) {
+            // slot-major rows: rows[slot * n_rows + row]
+#pragma unroll
+            for (int s = 0; s < kSlots; ++s) {
+                double v = 0.0;
+#pragma unroll
+                for (int j = 0; j < NV; ++j)
+                    if (slot_of<KIND>(j) == s) v = acc[j];
+                a.rows[(size_t)s * a.n_rows + row] = v;
+            }
+        }
+    }
+    // the row (thread 0) and any fallback-queue entry (the threads that
+    // queued) are visible device-wide before the tickets are taken; the force
+    // additions need no fence: the finishing block only adds to them
+    if (queued || threadIdx.x == 0) __threadfence();
+    __syncthreads();
+    const int g = row / kGroup;
+    if (threadIdx.x == 0) {
+        const int gsize = min(kGroup, a.n_rows - kGroup * g);
+        state = atomicAdd(a.group_ticket + g, 1u) == (unsigned)gsize - 1 ? 1 : 0;
+    }
+    __syncthreads();
+    if (state == 0) return;
+    __threadfence();
+    if constexpr (E) {
+        if (threadIdx.x < 32) {
+            const int r = kGroup * g + threadIdx.x;
+            const bool in = r < a.n_rows;
+            double v[kSlots];
+#pragma unroll
+            for (int s = 0; s < kSlots; ++s) v[s] = in ? __ldcg(a.rows + (size_t)s * a.n_rows + r) : 0.0;
+#pragma unroll
+            for (int s = 0; s < kSlots; ++s) {
+                const double t = warp_tree(v[s]);
+                if (threadIdx.x == 0) a.group_rows[(size_t)s * a.n_groups + g] = t;
+            }
+        }
+    }
+    if (threadIdx.x == 0) {
+        a.group_ticket[g] = 0u;
+        __threadfence();
+        const int ng = (a.n_rows + kGroup - 1) / kGroup;
+        state = atomicAdd(a.ticket, 1u) == (unsigned)ng - 1 ? 2 : 1;
+    }
+    __syncthreads();
+    if (state != 2) return;
+    __threadfence();
+    pass_finish<E, F>(a);
+}
+
+// ------------------------------------------------------------ main kernel
+// One warp tile of the chains: lanes hold centres q = 30w-1 .. 30w+30; the
+// link (q, q+1) and the bend centred at q are evaluated once, and lanes
+// 1..30 add the five terms acting on their bead and own their link's and
+// bend's energy.
+template <class R, bool E, bool F>
+__device__ __forceinline__ void chain_tile(const PassArgs& a, const Pos& P, double* __restrict__ f, int w,
+                                           double (&acc)[4]) {
+    const ChainDev& ch = a.ch;
+    const int n = ch.n_pos;
+    const int lane = threadIdx.x & 31;
+    const int q = w * kWarpOut - 1 + lane;
+    const bool in = q >= 0 && q < n;
+    const int qe = lane == 0 ? q - 1 : q + 1;  // the halo position of lanes 0 and 31
+    V3 c{0.0, 0.0, 0.0}, ce{0.0, 0.0, 0.0};
+    if (in) c = P(3 * q);
+    if ((lane == 0 || lane == 31) && qe >= 0 && qe < n) ce = P(3 * qe);
+    const unsigned char fl = in ? ch.flags[q] : 0;
+    const double2 lp = in ? ch.link_p[q] : double2{0.0, 0.0};
+    const double2 bp = in ? ch.bend_p[q] : double2{0.0, 0.0};
+    V3 cprev = shfl_up3(c), cnext = shfl_down3(c);
+    if (lane == 0) cprev = ce;
+    if (lane == 31) cnext = ce;
+    const bool own = lane >= 1 && lane <= kWarpOut && in;
+    if constexpr (F) {
+        T3<R> Fl{0, 0, 0}, A{0, 0, 0}, B{0, 0, 0};
+        if (fl & kLink) Fl = stretch_force<R>(c, cnext, lp.x, lp.y);
+        if (fl & kBend) bend_force<R>(diff<R>(cprev, c), diff<R>(c, cnext), bp.x, bp.y, A, B);
+        const T3<R> Fp = shfl_up3(Fl), Bp = shfl_up3(B), An = shfl_down3(A);
+        if (own) {
+            // link (q-1, q) acts on q; link (q, q+1) reacts on q; bends centred
+            // at q-1 (third bead), q (middle), q+1 (first bead); summed in double
+            const double fx = double(Fp.x) - double(Fl.x) + double(Bp.x) + (double(A.x) - double(B.x)) - double(An.x);
+            const double fy = double(Fp.y) - double(Fl.y) + double(Bp.y) + (double(A.y) - double(B.y)) - double(An.y);
+            const double fz = double(Fp.z) - double(Fl.z) + double(Bp.z) + (double(A.z) - double(B.z)) - double(An.z);
+            red_add(f + 3 * q, fx);
+            red_add(f + 3 * q + 1, fy);
+            red_add(f + 3 * q + 2, fz);
+        }
+    }
+    if constexpr (E) {
+        if (own) {
+            if (fl & kLink) acc[0] += stretch_energy<double>(c, cnext, lp.x, lp.y);
+            if (fl & kBend) acc[1] += bend_energy<double>(diff<double>(cprev, c), diff<double>(c, cnext), bp.x, bp.y);
+        }
+    }
+}
+
+// Record i of bonded segment s (0 leftover stretch, 1 leftover bend, 2
+// linker, 3 motor, 5 boundary): energy into acc[0], forces added to f.
+template <class R, bool E, bool F>
+__device__ __forceinline__ void bonded_record(const DeviceFF& ff, const Pos& P, double* __restrict__ f, int s, int i,
+                                              double (&acc)[4]) {
+    switch (s) {
+        case 0:
+            if (i < ff.n_stretch) {
+                const int2 q = ff.stretch_bs[i];
+                const double2 p = ff.stretch_p[i];
+                const V3 c1 = P(q.x), c2 = P(q.y);
+                if constexpr (E) acc[0] += stretch_energy<double>(c1, c2, p.x, p.y);
+                if constexpr (F) {
+                    const T3<R> Fs = stretch_force<R>(c1, c2, p.x, p.y);
+                    add_force(f, q.y, Fs.x, Fs.y, Fs.z);
+                    add_force(f, q.x, -Fs.x, -Fs.y, -Fs.z);
+                }
+            }
+            break;
+        case 1:
+            if (i < ff.n_bend) {
+                const int4 q = ff.bend_bs[i];
+                const double2 p = ff.bend_p[i];
+                const V3 c1 = P(q.x), c2 = P(q.y), c3 = P(q.z);
+                if constexpr (E) acc[0] += bend_energy<double>(diff<double>(c1, c2), diff<double>(c2, c3), p.x, p.y);
+                if constexpr (F) {
+                    T3<R> Fr1, Fr2;
+                    bend_force<R>(diff<R>(c1, c2), diff<R>(c2, c3), p.x, p.y, Fr1, Fr2);
+                    add_force(f, q.x, -Fr1.x, -Fr1.y, -Fr1.z);
+                    add_force(f, q.y, Fr1.x - Fr2.x, Fr1.y - Fr2.y, Fr1.z - Fr2.z);
+                    add_force(f, q.z, Fr2.x, Fr2.y, Fr2.z);
+                }
+            }
+            break;
+        case 2:
+        case 3: {
+            const int n = s == 2 ? ff.n_linker : ff.n_motor;
+            if (i < n) {
+                const int4 q = s == 2 ? ff.linker_bs[i] : ff.motor_bs[i];
+                const double4 p = s == 2 ? ff.linker_p[i] : ff.motor_p[i];
+                const V3 c1 = P(q.x), c2 = P(q.y), c3 = P(q.z), c4 = P(q.w);
+                if constexpr (E) acc[0] += spring_energy<double>(c1, c2, c3, c4, p.x, p.y, p.z, p.w);
+                if constexpr (F) {
+                    const T3<R> Fl = spring_force<R>(c1, c2, c3, c4, p.x, p.y, p.z, p.w);
+                    const R a1 = R(1) - R(p.z), a2 = R(p.z), b1 = R(1) - R(p.w), b2 = R(p.w);
+                    add_force(f, q.x, -Fl.x * a1, -Fl.y * a1, -Fl.z * a1);
+                    add_force(f, q.y, -Fl.x * a2, -Fl.y * a2, -Fl.z * a2);
+                    add_force(f, q.z, Fl.x * b1, Fl.y * b1, Fl.z * b1);
+                    add_force(f, q.w, Fl.x * b2, Fl.y * b2, Fl.z * b2);
+                }
+            }
+            break;
+        }
+        default:
+            if (i < ff.n_boundary) {
+                const int o = ff.boundary_bs[i];
+                const double2 p = ff.boundary_p[i];
+                const double4 pl = ff.planes[ff.boundary_plane[i]];
+                const V3 c = P(o);
+                if constexpr (E) acc[0] += boundary_energy<double>(pl, c, p.x, p.y);
+                if constexpr (F) {
+                    const R f0 = boundary_force_mag<R>(pl, c, p.x, p.y);
+                    add_force(f, o, f0 * R(pl.x), f0 * R(pl.y), f0 * R(pl.z));
+                }
+            }
+            break;
+    }
+}
+
+// Units of the main kernel: [0, nch) chain units (one warp tile per warp),
+// then bonded chunks of blockDim records (a.seg[k] is the first chunk of
+// leftover stretch, leftover bend, linker, motor, boundary). A fixed grid
+// walks them, so each block's energy row covers a fixed set of units.
+template <class R, bool E, bool F>
+__global__ void __launch_bounds__(kPassThreads, (E && F) ? kMainBlocksPerSM - 1 : kMainBlocksPerSM)
+    k_pass_main(const __grid_constant__ PassArgs a) {
+    if (F && a.t.skip && *a.t.skip) return;
+    double* __restrict__ f = F ? target_force(a.t) : nullptr;
+    const Pos P = pos_of(a);
+    double acc[kMainVals] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    const DeviceFF& ff = a.ff;
+    const int units = a.nch + a.nb_main;
+    for (int u = blockIdx.x; u < units; u += gridDim.x) {
+        if (u < a.nch) {
+            const int w = u * (blockDim.x >> 5) + (threadIdx.x >> 5);
+            double ca[4] = {0.0, 0.0, 0.0, 0.0};
+            if ((long long)w * kWarpOut < a.ch.n_pos) chain_tile<R, E, F>(a, P, f, w, ca);
+            acc[0] += ca[0];
+            acc[1] += ca[1];
+        } else {
+            const int b = u - a.nch;
+            int k = 0;
+#pragma unroll
+            for (int j = 1; j < 5; ++j) k += b >= a.seg[j] ? 1 : 0;
+            const int i = (b - a.seg[k]) * blockDim.x + threadIdx.x;
+            double e[4] = {0.0, 0.0, 0.0, 0.0};
+            bonded_record<R, E, F>(ff, P, f, k == 4 ? 5 : k, i, e);
+            // acc: 0 stretching, 1 bending, 2 linker, 3 motor, 4 boundary
+#pragma unroll
+            for (int j = 0; j < kMainVals; ++j)
+                if (j == k) acc[j] += e[0];
+        }
+    }
+    block_done<0, E, F>(a, acc, a.row_main + blockIdx.x, false);
+}
+
+// ------------------------------------------------------------ branch points
+template <class R, bool E, bool F>
+__global__ void __launch_bounds__(kPassThreads) k_pass_branch(const __grid_constant__ PassArgs a) {
+    if (F && a.t.skip && *a.t.skip) return;
+    double* __restrict__ f = F ? target_force(a.t) : nullptr;
+    const Pos P = pos_of(a);
+    const DeviceFF& ff = a.ff;
+    double acc[kBranchVals] = {0.0, 0.0, 0.0, 0.0};
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < ff.n_branch) {
+        const int4 q = ff.branch_bs[i];
+        const double4 pa = ff.branch_pa[i], pb = ff.branch_pb[i];
+        const V3 c1 = P(q.x), c2 = P(q.y), c3 = P(q.z), c4 = P(q.w);
+        const int m = ff.branch_mask;
+        if constexpr (E) {
+            if (m & 1) acc[0] += branch_stretch_energy<double>(c1, c2, c3, pa.y, pa.z, pa.x);
+            if (m & 2) acc[1] += bend_energy<double>(diff<double>(c1, c2), diff<double>(c3, c4), pa.w, pb.x);
+            if (m & 4) acc[2] += branch_dihedral_energy<double>(c1, c2, c3, c4, pb.y, pa.x);
+            if (m & 8) acc[3] += branch_position_energy<double>(c1, c2, c3, pb.z, pa.x);
+        }
+        if constexpr (F) {
+            T3<R> F1{0, 0, 0}, F2{0, 0, 0}, F3{0, 0, 0}, F4{0, 0, 0};
+            if (m & 1) {
+                const T3<R> g = branch_stretch_force<R>(c1, c2, c3, pa.y, pa.z, pa.x);
+                const R pm1 = R(pa.x) - R(1), pp = R(pa.x);
+                F1.x += -g.x * pm1; F1.y += -g.y * pm1; F1.z += -g.z * pm1;
+                F2.x += g.x * pp; F2.y += g.y * pp; F2.z += g.z * pp;
+                F3.x += -g.x; F3.y += -g.y; F3.z += -g.z;
+            }
+            if (m & 2) {
+                T3<R> Fr1, Fr2;
+                bend_force<R>(diff<R>(c1, c2), diff<R>(c3, c4), pa.w, pb.x, Fr1, Fr2);
+                F1.x += -Fr1.x; F1.y += -Fr1.y; F1.z += -Fr1.z;
+                F2.x += Fr1.x; F2.y += Fr1.y; F2.z += Fr1.z;
+                F3.x += -Fr2.x; F3.y += -Fr2.y; F3.z += -Fr2.z;
+                F4.x += Fr2.x; F4.y += Fr2.y; F4.z += Fr2.z;
+            }
+            if (m & 4) {
+                T3<R> L1, L2, L3, L4;
+                branch_dihedral_force<R>(c1, c2, c3, c4, pb.y, pa.x, L1, L2, L3, L4);
+                F1.x += L1.x; F1.y += L1.y; F1.z += L1.z;
+                F2.x += L2.x; F2.y += L2.y; F2.z += L2.z;
+                F3.x += L3.x; F3.y += L3.y; F3.z += L3.z;
+                F4.x += L4.x; F4.y += L4.y; F4.z += L4.z;
+            }
+            if (m & 8) {
+                T3<R> P1, P2, P3;
+                branch_position_force<R>(c1, c2, c3, pb.z, pa.x, P1, P2, P3);
+                F1.x += P1.x; F1.y += P1.y; F1.z += P1.z;
+                F2.x += P2.x; F2.y += P2.y; F2.z += P2.z;
+                F3.x += P3.x; F3.y += P3.y; F3.z += P3.z;
+            }
+            add_force(f, q.x, F1.x, F1.y, F1.z);
+            add_force(f, q.y, F2.x, F2.y, F2.z);
+            add_force(f, q.z, F3.x, F3.y, F3.z);
+            add_force(f, q.w, F4.x, F4.y, F4.z);
+        }
+    }
+    block_done<1, E, F>(a, acc, a.row_branch + blockIdx.x, false);
+}
+
+// ------------------------------------------------------------ excluded volume
+// One pair per thread, FP64. A pair whose analytic energy or forces the
+// reference would reject goes to the fallback queue instead.
+template <bool E, bool F, bool EXACT>
+__global__ void __launch_bounds__(kExclThreadsMax) k_pass_excl(const __grid_constant__ PassArgs a) {
+    if (F && a.t.skip && *a.t.skip) return;
+    double* __restrict__ f = F ? target_force(a.t) : nullptr;
+    const Pos P = pos_of(a);
+    const DeviceFF& ff = a.ff;
+    double acc[kExclVals] = {0.0};
+    bool queued = false;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ff.n_excl; i += gridDim.x * blockDim.x) {
+        const int4 q = ff.excl_bs[i];
+        const double krs = ff.excl_krs[i];
+        const V3 c1 = P(q.x), c2 = P(q.y), c3 = P(q.z), c4 = P(q.w);
+        if constexpr (E) {
+            const double U = excl_energy<double>(c1, c2, c3, c4, krs);
+            if (excl_energy_bad(U)) {
+                const int slot = atomicAdd(a.e_fb_count, 1);
+                if (slot < kFallbackCap) a.e_fb_list[slot] = make_int2(i, 0);
+                else atomicOr(a.e_bad, 2);
+                queued = true;
+            } else {
+                acc[0] += U;
+            }
+        }
+        if constexpr (F) {
+            T3<double> fo[4];
+            if (excl_force<EXACT>(c1, c2, c3, c4, krs, fo)) {
+                add_force(f, q.x, fo[0].x, fo[0].y, fo[0].z);
+                add_force(f, q.y, fo[1].x, fo[1].y, fo[1].z);
+                add_force(f, q.z, fo[2].x, fo[2].y, fo[2].z);
+                add_force(f, q.w, fo[3].x, fo[3].y, fo[3].z);
+            } else {
+                const int slot = atomicAdd(a.f_fb_count, 1);
+                if (slot < kFallbackCap) a.f_fb_list[slot] = i;
+                else atomicOr(a.f_status, 2);
+                queued = true;
+            }
+        }
+    }
+    block_done<2, E, F>(a, acc, a.row_excl + blockIdx.x, queued);
+}
+
+// ------------------------------------------------------------ zero fill
+__global__ void __launch_bounds__(kZeroThreads) k_pass_zero(const ForceTarget t, int n3) {
+    if (t.skip && *t.skip) return;
+    double* __restrict__ f = target_force(t);
+    // cudaMalloc'd buffers are 256-byte aligned: pairs of doubles, then the odd tail
+    double2* __restrict__ f2 = reinterpret_cast<double2*>(f);
+    const int n2 = n3 >> 1;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n2; i += gridDim.x * blockDim.x) f2[i] = double2{0.0, 0.0};
+    if ((n3 & 1) && blockIdx.x == 0 && threadIdx.x == 0) f[n3 - 1] = 0.0;
+}
+
+template <class R, bool E, bool F>
+void launch_kernels(const PassArgs& a, const PassGeometry& g, int prec, cudaStream_t s_main, cudaStream_t s_branch,
+                    cudaStream_t s_excl) {
+    // the excluded-volume pairs first: their FP64 chains are the longest, and
+    // their blocks should be resident before the main kernel's fill the SMs
+    if (g.excl_blocks > 0) {
+        if (prec == MEDYAN_PREC_FP64)
+            k_pass_excl<E, F, true><<<g.excl_blocks, g.excl_threads, 0, s_excl>>>(a);
+        else
+            k_pass_excl<E, F, false><<<g.excl_blocks, g.excl_threads, 0, s_excl>>>(a);
+    }
+    if (g.branch_blocks > 0) k_pass_branch<R, E, F><<<g.branch_blocks, g.threads, 0, s_branch>>>(a);
+    k_pass_main<R, E, F><<<g.main_blocks, g.threads, 0, s_main>>>(a);
+}
+
+}  // namespace
+
+namespace {
+int g_num_sms = 148;  // SMs of the device (set at init; B200: 148)
+}  // namespace
+
+PassGeometry pass_geometry(const ChainDev& ch, const DeviceFF& ff) {
+    PassGeometry g{};
+    g.threads = kPassThreads;
+    g.excl_threads = excl_block_of(ff) > 128 ? 128 : excl_block_of(ff);
+    const int tiles = (ch.n_pos + kWarpOut - 1) / kWarpOut;
+    const int warps = g.threads / 32;
+    g.nch = (tiles + warps - 1) / warps;
+    const int counts[5] = {ff.n_stretch, ff.n_bend, ff.n_linker, ff.n_motor, ff.n_boundary};
+    g.seg[0] = 0;
+    for (int k = 0; k < 5; ++k) g.seg[k + 1] = g.seg[k] + (counts[k] + g.threads - 1) / g.threads;
+    g.nb_main = g.seg[5];
+    // fixed grids that walk the units (one block at least: it can finish the pass)
+    const int units = g.nch + g.nb_main;
+    // a resident grid that walks the units: one block per unit measured
+    // slower (each block's end, a fence and two tickets, holds its SM slot)
+    const int cap = g_num_sms * kMainBlocksPerSM;
+    g.main_blocks = units < 1 ? 1 : (units < cap ? units : cap);
+    g.branch_blocks = (ff.n_branch + g.threads - 1) / g.threads;
+    const int eb = (ff.n_excl + g.excl_threads - 1) / g.excl_threads;
+    const int ecap = g_num_sms * 32;
+    g.excl_blocks = eb < ecap ? eb : ecap;
+    g.rows = g.main_blocks + g.branch_blocks + g.excl_blocks;
+    g.groups = (g.rows + kGroup - 1) / kGroup;
+    return g;
+}
+
+void launch_pass_fused(const ChainDev& ch, const DeviceFF& ff, int prec, const double* x, const ForceTarget* t,
+                       bool energy, const LambdaSet* lam_set, const EnergyScratch& es, const ForceScratch& fs,
+                       const PassScratch& ps, cudaStream_t s, const Fork* fk) {
+    const PassGeometry g = pass_geometry(ch, ff);
+    PassArgs a{};
+    a.ch = ch;
+    a.ff = ff;
+    a.x = x;
+    if (t) a.t = *t;
+    a.rows = ps.rows;
+    a.group_rows = ps.group_rows;
+    a.group_ticket = ps.group_ticket;
+    a.ticket = ps.ticket;
+    a.n_rows = g.rows;
+    a.n_groups = g.groups;
+    a.row_main = 0;
+    a.row_branch = g.main_blocks;
+    a.row_excl = g.main_blocks + g.branch_blocks;
+    a.nch = g.nch;
+    a.nb_main = g.nb_main;
+    for (int k = 0; k < 6; ++k) a.seg[k] = g.seg[k];
+    a.out = es.out;
+    a.lam_set = lam_set;
+    a.e_fb_count = es.fb_count;
+    a.e_fb_list = es.fb_list;
+    a.e_bad = es.bad;
+    a.f_fb_count = fs.fb_count;
+    a.f_fb_list = fs.fb_list;
+    a.f_status = fs.status;
+    const bool force = t != nullptr;
+    if (force) {
+        const int n3 = 3 * ch.n_pos;
+        int zb = (n3 / 2 + kZeroThreads - 1) / kZeroThreads;
+        zb = zb < 1 ? 1 : (zb > 148 * 8 ? 148 * 8 : zb);
+        if (n3 > 0) k_pass_zero<<<zb, kZeroThreads, 0, s>>>(*t, n3);
+    }
+    cudaStream_t sb = s, se = s;
+    if (fk) {
+        cudaEventRecord(fk->fork, s);
+        cudaStreamWaitEvent(fk->side[0], fk->fork, 0);
+        cudaStreamWaitEvent(fk->side[1], fk->fork, 0);
+        sb = fk->side[0];
+        se = fk->side[1];
+    }
+    const bool mixed = prec == MEDYAN_PREC_MIXED;
+    if (energy && force) {
+        if (mixed) launch_kernels<float, true, true>(a, g, prec, s, sb, se);
+        else launch_kernels<double, true, true>(a, g, prec, s, sb, se);
+    } else if (force) {
+        if (mixed) launch_kernels<float, false, true>(a, g, prec, s, sb, se);
+        else launch_kernels<double, false, true>(a, g, prec, s, sb, se);
+    } else {
+        launch_kernels<double, true, false>(a, g, prec, s, sb, se);
+    }
+    if (fk) {
+        for (int k = 0; k < 2; ++k) {
+            cudaEventRecord(fk->join[k], fk->side[k]);
+            cudaStreamWaitEvent(s, fk->join[k], 0);
+        }
+    }
+}
+
+cudaError_t init_pass_kernels() {
+    static std::mutex mu;
+    static bool filled[64];
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(mu);
+    if (filled[dev]) return cudaSuccess;
+    int sms = 0;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    if (sms > 0) g_num_sms = sms;
+    cudaStream_t s = nullptr;
+    e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return e;
+    k_fill_quadrature_grids<<<1, 1, 0, s>>>();
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+    if (e == cudaSuccess) filled[dev] = true;
+    return e;
+}
+
+}  // namespace mb

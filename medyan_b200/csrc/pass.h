@@ -1,0 +1,71 @@
+// pass.h — fused single-network passes (pass.cu): launch geometry, scratch
+// and the argument block the pass kernels share.
+#pragma once
+
+#include "internal.h"
+
+namespace mb {
+
+// Device scratch of the fused passes, owned by the handle: one energy row per
+// block of the pass's kernels and one per group of kPassGroup rows, a ticket
+// per group and the pass ticket (all tickets zero between passes; the blocks
+// that complete them reset them).
+constexpr int kPassGroup = 32;
+struct PassScratch {
+    double* rows;             // [MEDYAN_FF_COUNT][rows], slot-major
+    double* group_rows;       // [MEDYAN_FF_COUNT][groups]
+    unsigned* group_ticket;   // [groups]
+    unsigned* ticket;
+};
+
+constexpr int kPassThreads = 256;  // threads per block of the main and branch kernels
+
+// Blocks and threads of one fused pass over a network.
+struct PassGeometry {
+    int threads;        // threads per block of the main and branch kernels (= records per bonded block)
+    int seg[6];         // first bonded block of leftover stretch, leftover bend, linker, motor, boundary; end
+    int excl_threads;   // pairs per excluded-volume block
+    int nch;            // chain blocks of the main kernel (threads/32 warp tiles of 30 beads each)
+    int nb_main;        // bonded blocks of the main kernel (segments 0-3 and 5)
+    int main_blocks, branch_blocks, excl_blocks;
+    int rows;           // energy rows = blocks of all three kernels
+    int groups;         // rows / kPassGroup, rounded up
+};
+
+struct PassArgs {
+    ChainDev ch;
+    DeviceFF ff;
+    const double* x;
+    ForceTarget t;            // force target and the positions (x, or x + (*lam) d) of both outputs
+    double* rows;
+    double* group_rows;
+    unsigned* group_ticket;
+    unsigned* ticket;
+    int n_rows, n_groups, row_main, row_branch, row_excl;
+    int nch, nb_main;
+    int seg[6];               // PassGeometry::seg
+    double* out;              // [kMaxLambda][MEDYAN_FF_COUNT + 1] energies
+    const LambdaSet* lam_set; // result copied to slots [0, K) (null: slot 0)
+    int* e_fb_count;
+    int2* e_fb_list;
+    int* e_bad;
+    int* f_fb_count;
+    int* f_fb_list;
+    int* f_status;
+};
+
+PassGeometry pass_geometry(const ChainDev& ch, const DeviceFF& ff);
+
+// Energy (energy = true) and/or forces (t set) of a single network's force
+// fields at t's positions (x when t is null or t->d is null). The energy lands
+// in es.out; the forces in target_force(*t), overwritten. Single networks
+// only (ff.act == null). With fk the three kernels run on parallel branches.
+void launch_pass_fused(const ChainDev& ch, const DeviceFF& ff, int prec, const double* x, const ForceTarget* t,
+                       bool energy, const LambdaSet* lam_set, const EnergyScratch& es, const ForceScratch& fs,
+                       const PassScratch& ps, cudaStream_t s, const Fork* fk);
+
+// Fills pass.cu's quadrature grids, once per device (the current one); call
+// before any stream capture.
+cudaError_t init_pass_kernels();
+
+}  // namespace mb

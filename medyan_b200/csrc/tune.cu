@@ -2,7 +2,8 @@
 //
 // The tunable shapes are the records (threads) per block of the bonded and
 // excluded-volume kernels, the threads per block of the chain force kernel,
-// and the fixed grid of the chain energy kernel. The autotuner times the
+// the fixed grid of the chain energy kernel, and the pass layout (fused
+// kernels or one kernel per potential group). The autotuner times the
 // handle's evaluate pass (energy and forces, one CUDA graph) for each
 // candidate of one field at a time, keeps the fastest, and moves to the next
 // field (coordinate descent from the current shapes).
@@ -14,11 +15,13 @@ using namespace mb;
 
 namespace {
 
-bool allowed(int v, const int (&set)[3]) { return v == set[0] || v == set[1] || v == set[2]; }
+constexpr int kNone = -1;
+bool allowed(int v, const int (&set)[3]) { return v != kNone && (v == set[0] || v == set[1] || v == set[2]); }
 constexpr int kBonded[3] = {128, 256, 512};
 constexpr int kExcl[3] = {32, 64, 128};
 constexpr int kChain[3] = {128, 256, 512};
 constexpr int kEnergyBps[3] = {2, 4, 8};
+constexpr int kLayout[3] = {0, 1, kNone};
 
 medyan_launch_shapes current(const medyan_mech* h) {
     medyan_launch_shapes s{};
@@ -26,6 +29,7 @@ medyan_launch_shapes current(const medyan_mech* h) {
     s.excl_threads = excl_block_of(h->ff);
     s.chain_threads = h->chain.force_threads > 0 ? h->chain.force_threads : 256;
     s.chain_energy_blocks_per_sm = h->chain.energy_blocks_per_sm > 0 ? h->chain.energy_blocks_per_sm : 4;
+    s.pass_layout = h->pass_layout;
     return s;
 }
 
@@ -57,7 +61,8 @@ extern "C" {
 medyan_status medyan_mech_set_shapes(medyan_mech* h, const medyan_launch_shapes* s) {
     if (!h || !s) return MEDYAN_ERR_INVALID_ARG;
     if (!allowed(s->bonded_threads, kBonded) || !allowed(s->excl_threads, kExcl) ||
-        !allowed(s->chain_threads, kChain) || !allowed(s->chain_energy_blocks_per_sm, kEnergyBps))
+        !allowed(s->chain_threads, kChain) || !allowed(s->chain_energy_blocks_per_sm, kEnergyBps) ||
+        !allowed(s->pass_layout, kLayout))
         return MEDYAN_ERR_INVALID_ARG;
     cudaError_t e = cudaSetDevice(h->device);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);  // no pass may still read the old tables
@@ -66,6 +71,7 @@ medyan_status medyan_mech_set_shapes(medyan_mech* h, const medyan_launch_shapes*
     h->ff.excl_block = s->excl_threads;
     h->chain.force_threads = s->chain_threads;
     h->chain.energy_blocks_per_sm = s->chain_energy_blocks_per_sm;
+    h->pass_layout = s->pass_layout;
     return refresh_device_ff(h);
 }
 
@@ -81,15 +87,16 @@ medyan_status medyan_mech_autotune(medyan_mech* h, int32_t reps, medyan_launch_s
     medyan_status st = medyan_mech_set_shapes(h, &best);
     float best_ms = 0.0f;
     if (st == MEDYAN_OK) st = time_evaluate(h, reps, &best_ms);
-    int32_t* fields[4] = {&best.bonded_threads, &best.excl_threads, &best.chain_threads,
+    // the layout first: the other fields' best values depend on it
+    int32_t* fields[5] = {&best.pass_layout, &best.bonded_threads, &best.excl_threads, &best.chain_threads,
                           &best.chain_energy_blocks_per_sm};
-    const int* sets[4] = {kBonded, kExcl, kChain, kEnergyBps};
-    for (int f = 0; f < 4 && st == MEDYAN_OK; ++f) {
+    const int* sets[5] = {kLayout, kBonded, kExcl, kChain, kEnergyBps};
+    for (int f = 0; f < 5 && st == MEDYAN_OK; ++f) {
         const int keep = *fields[f];
         for (int c = 0; c < 3 && st == MEDYAN_OK; ++c) {
-            if (sets[f][c] == keep) continue;
+            if (sets[f][c] == keep || sets[f][c] == kNone) continue;
             medyan_launch_shapes trial = best;
-            int32_t* tf[4] = {&trial.bonded_threads, &trial.excl_threads, &trial.chain_threads,
+            int32_t* tf[5] = {&trial.pass_layout, &trial.bonded_threads, &trial.excl_threads, &trial.chain_threads,
                               &trial.chain_energy_blocks_per_sm};
             *tf[f] = sets[f][c];
             st = medyan_mech_set_shapes(h, &trial);

@@ -26,7 +26,7 @@ def test_library_exports_every_header_symbol():
     assert len(declared) >= 15
     missing = [s for s in declared if not hasattr(L, s)]
     assert not missing, missing
-    assert L.medyan_abi_version() == 1
+    assert L.medyan_abi_version() == 2
     assert L.medyan_status_string(6) == b"cylinder outside the neighbor-list grid"
 
 

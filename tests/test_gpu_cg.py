@@ -50,6 +50,22 @@ def test_short_run_matches_oracle(gpu_lib, oracle, method):
     assert errs[0] <= 1e-7 and errs[1] <= 1e-10 and errs[2] <= 1e-12 and errs[3] <= 1e-7, errs
 
 
+def test_fused_force_pass_short_run(gpu_lib, oracle):
+    """The minimizer with the fused pass layout (its force pass: zero fill,
+    then the chain/bonded, branching and excluded-volume kernels side by side)
+    takes the oracle's iterations and calls."""
+    sv, x = small_net(oracle)
+    p = cgp(grad_tol=1e-4, energy_rel_tol=1e-14, energy_call_limit=40)
+    so, xo, fo, ro = oracle.minimize(sv, x, p)
+    with ForceFieldManager("fp64") as ff:
+        ff.vectorize_all_force_fields(sv)
+        ff.set_shapes(pass_layout=0)
+        sg, xg, fg, rg = ff.minimize(x, p)
+    assert sg == so == 0
+    assert (rg.num_energy_call, rg.num_force_call, rg.num_iter) == (ro.num_energy_call, ro.num_force_call, ro.num_iter)
+    assert np.abs(xg - xo).max() <= 1e-7
+
+
 def test_converges_like_oracle(gpu_lib, oracle):
     sv, x = small_net(oracle)
     p = cgp(grad_tol=1.0)
@@ -135,7 +151,10 @@ def test_returned_forces_are_those_at_the_returned_coordinates(gpu_lib, oracle, 
     # at its first trial step; when the line search takes that step, the
     # iteration's force pass is skipped. Whichever path each iteration took,
     # the forces a converged minimization returns are a fresh evaluation's at
-    # its final coordinates, up to the atomics' summation order.
+    # its final coordinates, up to the atomics' summation order. At a minimum
+    # a bead's net force is a small difference of terms hundreds of times
+    # larger (excluded-volume repulsion against filament tension), so the
+    # order of the atomic sums shows at ~1e-12 of the net max|F|.
     sv, x = small_net(oracle, n_fil=30, cyl_per_fil=8, box=1000.0, n_linker=60, seed=11)
     p = cgp(grad_tol=0.5)
     with ForceFieldManager(precision) as ff:
@@ -143,8 +162,8 @@ def test_returned_forces_are_those_at_the_returned_coordinates(gpu_lib, oracle, 
         sg, xg, fg, rg = ff.minimize(x, p)
         f_fresh = ff.compute_forces(xg)
     assert sg == 0 and rg.num_iter > 20
-    assert np.abs(fg - f_fresh).max() <= 1e-12 * np.abs(f_fresh).max()
-    assert rg.grad_inf_norm == pytest.approx(np.abs(f_fresh).max(), rel=1e-12)
+    assert np.abs(fg - f_fresh).max() <= 1e-10 * np.abs(f_fresh).max()
+    assert rg.grad_inf_norm == pytest.approx(np.abs(f_fresh).max(), rel=1e-10)
 
 
 def test_already_converged(gpu_lib, oracle):
