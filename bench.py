@@ -10,8 +10,12 @@ from the device neighbor list (54 nm cutoff).
 
 value: steps/s with coordinates resident in HBM, L2 flushed (256 MiB write)
 before every timed step, device time from CUDA events on the library's stream.
-e2e: the same step through the C ABI (medyan_mech_evaluate) from pinned host
-buffers: coordinates in, energy and forces out, copies inside the timed region.
+e2e: the same step through the C ABI from page-locked host buffers:
+coordinates in, energies and forces out, every step's copies inside the timed
+region. The steps go through medyan_mech_evaluate_async, which overlaps one
+step's inbound copy with the previous step's pass and outbound copy (two
+staging slots); e2e.sync is the synchronous medyan_mech_evaluate, one step at
+a time.
 
 --impl reference times the reference's own compiled CPU kernels
 (oracle/_ref/libmedyan_ref.so, one thread: the reference is single-threaded)
@@ -228,22 +232,41 @@ def run_ours(args, rank: int, world: int) -> dict:
     t_warm = w0.elapsed_time(w1) / 1e3 / K
     t_step = max_over_ranks(sum(t_steps), world, "cuda")
 
-    # e2e through the C ABI from pinned host buffers
-    xh = torch.from_numpy(x.copy()).pin_memory()
-    fh = torch.empty_like(xh).pin_memory()
-    xptr = C.cast(xh.data_ptr(), C.POINTER(C.c_double))
-    fptr = C.cast(fh.data_ptr(), C.POINTER(C.c_double))
+    # e2e through the C ABI from page-locked host buffers: each step's own
+    # coordinates in, its energies and forces out (the asynchronous entry,
+    # two steps in flight), and the synchronous entry for comparison
+    pd = C.POINTER(C.c_double)
+    xh = [torch.from_numpy(x.copy()).pin_memory() for _ in range(2)]
+    fh = [torch.empty_like(xh[0]).pin_memory() for _ in range(2)]
+    eh = [torch.empty(11, dtype=torch.float64).pin_memory() for _ in range(2)]
+
+    def e2e_async(n):
+        for i in range(n):
+            st = L.medyan_mech_evaluate_async(h, C.cast(xh[i % 2].data_ptr(), pd), C.cast(fh[i % 2].data_ptr(), pd),
+                                              C.cast(eh[i % 2].data_ptr(), pd))
+            if st != 0:
+                raise RuntimeError(f"medyan_mech_evaluate_async status {st}")
+        st = L.medyan_mech_wait(h)
+        if st not in (0, 3):
+            raise RuntimeError(f"medyan_mech_wait status {st}")
+
+    e2e_async(4)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e2e_async(K)
+    e2e_t = max_over_ranks(time.perf_counter() - t0, world, "cuda")
     etot = C.c_double()
     per = (C.c_double * 10)()
+    xptr = C.cast(xh[0].data_ptr(), pd)
+    fptr = C.cast(fh[0].data_ptr(), pd)
     for _ in range(2):
         L.medyan_mech_evaluate(h, xptr, C.byref(etot), per, fptr)
-    torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(K):
         st = L.medyan_mech_evaluate(h, xptr, C.byref(etot), per, fptr)
         if st not in (0, 3):
             raise RuntimeError(f"medyan_mech_evaluate status {st}")
-    e2e_t = max_over_ranks(time.perf_counter() - t0, world, "cuda")
+    e2e_sync_t = max_over_ranks(time.perf_counter() - t0, world, "cuda")
 
     # accuracy of this precision against the FP64 path on the same inputs
     ff64 = make("fp64") if args.precision != "fp64" else ff
@@ -251,6 +274,17 @@ def run_ours(args, rank: int, world: int) -> dict:
     e_, per_, f_ = ff.evaluate(x)
     rel_force_err = float(np.abs(f_ - f64).max() / np.abs(f64).max())
     rel_energy_err = float(abs(e_ - e64) / abs(e64))
+    # the FP64 arm: the same steps, same protocol, on the FP64 handle
+    fp64_arm = None
+    if ff64 is not ff:
+        L64, h64 = ff64.lib, ff64.handle
+        s64 = torch.cuda.ExternalStream(L64.medyan_mech_stream(h64))
+        t64 = timed_passes(L64.medyan_mech_enqueue_evaluate, h64, L64, s64, flush, K, max(args.warmup, 3))
+        f64t = timed_passes(L64.medyan_mech_enqueue_forces, h64, L64, s64, flush, K, 3)
+        t64_step = max_over_ranks(sum(t64), world, "cuda")
+        fp64_arm = {"value": world * K / t64_step, "unit": "force-evals/s", "ms_per_step": 1e3 * t64_step / K,
+                    "force_pass_alone_ms": 1e3 * sum(f64t) / K, "launch_shapes": ff64.tuned_shapes,
+                    "l2": "flushed (256 MiB write) before each timed step"}
 
     result = {
         "metric": METRIC,
@@ -270,12 +304,16 @@ def run_ours(args, rank: int, world: int) -> dict:
                    "interactions": counts, "l2": "flushed (256 MiB write) before each timed step",
                    "step": "total energy + forces of all force fields", "parallelism": f"replicas x{world}"},
         "e2e": {"value": world * K / e2e_t, "unit": "force-evals/s", "h2d_bytes_per_step": 8 * x.size,
-                "d2h_bytes_per_step": 8 * x.size + 8 * 11},
+                "d2h_bytes_per_step": 8 * x.size + 8 * 11,
+                "api": "medyan_mech_evaluate_async + medyan_mech_wait (two steps in flight)",
+                "sync": {"value": world * K / e2e_sync_t, "unit": "force-evals/s",
+                         "api": "medyan_mech_evaluate, one step at a time"}},
         # kernel nodes of the evaluate pass graph each timed step launches
         "gpu_launches": K * L.medyan_mech_pass_kernel_count(h, 2),
         "clocks": clocks.summary(),
         "wall_s_timed_region": wall,
         "accuracy_vs_fp64": {"rel_force_err": rel_force_err, "rel_energy_err": rel_energy_err},
+        "fp64": fp64_arm,
         "breakdown_ms": {"force_pass_alone": 1e3 * sum(t_force) / K, "energy_pass_alone": 1e3 * sum(t_energy) / K,
                          "step_l2_warm": 1e3 * t_warm},
     }
@@ -290,6 +328,26 @@ def run_ours(args, rank: int, world: int) -> dict:
     for f in {id(ff): ff, id(ff64): ff64}.values():
         f.close()
     return result
+
+
+def timed_passes(fn, h, L, stream, flush, K: int, warmup: int) -> list:
+    """K passes of fn(h), each after a 256 MiB L2 flush, timed with CUDA
+    events on the handle's stream; seconds per pass."""
+    import torch
+    for _ in range(warmup):
+        fn(h)
+    if L.medyan_mech_synchronize(h) != 0:
+        raise RuntimeError("pass reported an error")
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    with torch.cuda.stream(stream):
+        for i in range(K):
+            flush.zero_()
+            ev[i][0].record(stream)
+            fn(h)
+            ev[i][1].record(stream)
+    L.medyan_mech_synchronize(h)
+    torch.cuda.synchronize()
+    return [a.elapsed_time(b) / 1e3 for a, b in ev]
 
 
 def roofline(achieved_gbs: float, nbytes: int) -> dict:

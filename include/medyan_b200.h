@@ -202,6 +202,43 @@ medyan_status medyan_mech_enqueue_forces(medyan_mech* h);
    medyan_mech_evaluate runs), the two sets of kernels side by side. */
 medyan_status medyan_mech_enqueue_evaluate(medyan_mech* h);
 medyan_status medyan_mech_synchronize(medyan_mech* h);
+
+/* Deterministic force sums (no counterpart in the reference, whose CPU loops
+   add in a fixed order). Forces are normally summed with floating-point
+   atomic additions, whose order varies from run to run, so a force's last
+   bits, and with them a long minimization's trajectory, are not
+   reproducible. With on = 1 every force contribution is rounded to a 64-bit
+   integer count of 2^-32 pN and summed with integer additions, which give
+   the same bits in any order; the sums are converted back to double at the
+   end of each force pass. Forces then differ from the floating-point sums by
+   at most about 1e-9 pN per bead, and a contribution of 2^24 pN (1.7e7 pN)
+   or more is out of range: the call reports MEDYAN_ERR_NONFINITE. Energies
+   are deterministic in both modes. Applies to the standalone passes, the
+   evaluate entry points and the minimizer (not to packed batches, the
+   Hessian or the Hessian-vector product). on = 0 restores the default. */
+medyan_status medyan_mech_set_deterministic(medyan_mech* h, int32_t on);
+
+/* Asynchronous medyan_mech_evaluate, for a caller that evaluates many
+   coordinate sets back to back (no counterpart in the reference, whose
+   evaluation is a synchronous CPU call). Enqueues the host-to-device copy of
+   coord on its own stream, the evaluate pass on the handle's stream and the
+   device-to-host copies of the forces and energies on a third stream, and
+   returns without waiting. Consecutive calls alternate between two staging
+   slots, so the inbound copy of one call overlaps the pass and the outbound
+   copy of the previous one.
+     coord      double[3*n_beads] host, caller's bead order
+     force_out  double[3*n_beads] host
+     e_out      double[MEDYAN_FF_COUNT + 1] host: per force field, then the
+                total (+inf when a force field is at or below -1, as
+                medyan_mech_evaluate reports with MEDYAN_ERR_NONFINITE)
+   All three must stay valid and untouched until medyan_mech_wait returns;
+   the copies overlap only when they are page-locked (cudaHostAlloc,
+   cudaHostRegister). Call medyan_mech_wait before any other entry point on
+   the handle reads the results. */
+medyan_status medyan_mech_evaluate_async(medyan_mech* h, const double* coord, double* force_out, double* e_out);
+/* Waits for every asynchronous evaluation enqueued on the handle. Returns
+   MEDYAN_ERR_NONFINITE when the quadrature fallback failed in any of them. */
+medyan_status medyan_mech_wait(medyan_mech* h);
 /* The handle's cudaStream_t, for event timing or stream ordering. */
 void* medyan_mech_stream(medyan_mech* h);
 /* Kernel launches in one standalone pass (which: 0 energy, 1 forces, 2 both)

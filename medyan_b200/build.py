@@ -19,7 +19,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libmedyan_b200.so")
 
-SOURCES = ["capi.cu", "ff_kernels.cu", "chain.cu", "excl_kernels.cu", "nl.cu", "cg.cu", "batch.cu", "pbatch.cu", "diff.cu", "hessian.cu", "aux.cu", "tune.cu", "noalloc.cu", "pass.cu"]
+SOURCES = ["capi.cu", "ff_kernels.cu", "chain.cu", "excl_kernels.cu", "nl.cu", "cg.cu", "batch.cu", "pbatch.cu", "diff.cu", "hessian.cu", "aux.cu", "tune.cu", "noalloc.cu", "pass.cu", "async.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + os.path.join(ROOT, "include"),
           "-I" + CSRC, "--expt-relaxed-constexpr", "--fmad=false"]

@@ -296,7 +296,8 @@ void enqueue_energy(medyan_mech* h, const double* x, const double* d, const Lamb
 }
 
 void enqueue_forces(medyan_mech* h, const double* x, double* f, cudaStream_t s) {
-    enqueue_force_target(h, x, ForceTarget{f, nullptr, nullptr, nullptr, nullptr, nullptr}, h->fs, s);
+    enqueue_force_target(h, x, ForceTarget{f, nullptr, nullptr, nullptr, nullptr, nullptr, h->deterministic, h->fs.status},
+                         h->fs, s);
 }
 
 void enqueue_force_target(medyan_mech* h, const double* x, const ForceTarget& t, const ForceScratch& fs,
@@ -349,7 +350,7 @@ cudaError_t ensure_pass_graph(medyan_mech* h, int which) {
     h->pass_graph[which] = nullptr;
     cudaError_t e = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return e;
-    const ForceTarget t{h->f.raw(), nullptr, nullptr, nullptr, nullptr, nullptr};
+    const ForceTarget t{h->f.raw(), nullptr, nullptr, nullptr, nullptr, nullptr, h->deterministic, h->fs.status};
     if (h->pass_layout == 0)
         launch_pass_fused(h->chain, h->ff, h->prec, h->x.raw(), which == kPassEnergy ? nullptr : &t,
                           which != kPassForces, h->lam_zero.raw(), h->es, h->fs, h->pass_scratch(), h->stream,
@@ -440,6 +441,7 @@ medyan_mech::~medyan_mech() {
     if (small) cudaFreeHost(small);
     for (auto& g : pass_graph)
         if (g) cudaGraphExecDestroy(g);
+    destroy_async(this);
     destroy_nl(this);
     for (auto& sd : fork.side)
         if (sd) cudaStreamDestroy(sd);
@@ -572,6 +574,18 @@ medyan_status medyan_mech_enqueue_forces(medyan_mech* h) {
 medyan_status medyan_mech_enqueue_evaluate(medyan_mech* h) {
     if (!h) return MEDYAN_ERR_INVALID_ARG;
     return cuda_status(launch_pass(h, kPassBoth));
+}
+
+medyan_status medyan_mech_set_deterministic(medyan_mech* h, int32_t on) {
+    if (!h || (on != 0 && on != 1)) return MEDYAN_ERR_INVALID_ARG;
+    cudaError_t e = cudaSetDevice(h->device);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);  // no pass may still write the old way
+    if (e != cudaSuccess) return cuda_status(e);
+    if (h->deterministic != on) {
+        h->deterministic = on;
+        h->ff_gen++;  // recapture the passes and the minimizer's graph
+    }
+    return MEDYAN_OK;
 }
 
 medyan_status medyan_mech_synchronize(medyan_mech* h) {

@@ -818,8 +818,10 @@ CGLaunch make_launch(medyan_mech* h) {
     c.minE = h->cg_min_coords.raw();
     c.st = h->cg_state.raw();
     c.L = h->cg_lam.raw();
-    c.tgt = ForceTarget{c.f0, c.f1, &c.st->parity, &c.st->force_skip, c.d, &c.st->lam_move};
-    c.spec = ForceTarget{c.f0, c.f1, &c.st->parity, &c.st->spec_skip, c.d, &c.st->spec_lam};
+    c.tgt = ForceTarget{c.f0,           c.f1, &c.st->parity, &c.st->force_skip, c.d, &c.st->lam_move,
+                        h->deterministic, h->fs.status};
+    c.spec = ForceTarget{c.f0,           c.f1, &c.st->parity, &c.st->spec_skip, c.d, &c.st->spec_lam,
+                         h->deterministic, &c.st->spec_status};
     c.spec_fs = ForceScratch{h->fs.fb_count, h->fs.fb_list, &c.st->spec_status};
     return c;
 }

@@ -100,9 +100,10 @@ __global__ void __launch_bounds__(kMaxShapeThreads) k_chain_forces(const ChainDe
         if (lane >= 1 && lane <= kWarpOut && in && (!ch.act || ch.act[ch.rep[q]])) {
             // link (q-1, q) acts on q; link (q, q+1) reacts on q; bends centred
             // at q-1 (third bead), q (middle), q+1 (first bead); summed in double
-            f[3 * q] = double(Fp.x) - double(F.x) + double(Bp.x) + (double(A.x) - double(B.x)) - double(An.x);
-            f[3 * q + 1] = double(Fp.y) - double(F.y) + double(Bp.y) + (double(A.y) - double(B.y)) - double(An.y);
-            f[3 * q + 2] = double(Fp.z) - double(F.z) + double(Bp.z) + (double(A.z) - double(B.z)) - double(An.z);
+            target_store(tgt, f, 3 * q,
+                         double(Fp.x) - double(F.x) + double(Bp.x) + (double(A.x) - double(B.x)) - double(An.x),
+                         double(Fp.y) - double(F.y) + double(Bp.y) + (double(A.y) - double(B.y)) - double(An.y),
+                         double(Fp.z) - double(F.z) + double(Bp.z) + (double(A.z) - double(B.z)) - double(An.z));
         }
     }
 }

@@ -97,10 +97,10 @@ __global__ void __launch_bounds__(kMaxExclThreads) k_excl_forces(const DeviceFF 
         T3<double> fo[4];
         if (excl_force<EXACT>(pos_at(x, tgt, lam, q.x), pos_at(x, tgt, lam, q.y), pos_at(x, tgt, lam, q.z),
                           pos_at(x, tgt, lam, q.w), ff.excl_krs[i], fo)) {
-            add_force(f, q.x, fo[0].x, fo[0].y, fo[0].z);
-            add_force(f, q.y, fo[1].x, fo[1].y, fo[1].z);
-            add_force(f, q.z, fo[2].x, fo[2].y, fo[2].z);
-            add_force(f, q.w, fo[3].x, fo[3].y, fo[3].z);
+            target_add(tgt, f, q.x, fo[0].x, fo[0].y, fo[0].z);
+            target_add(tgt, f, q.y, fo[1].x, fo[1].y, fo[1].z);
+            target_add(tgt, f, q.z, fo[2].x, fo[2].y, fo[2].z);
+            target_add(tgt, f, q.w, fo[3].x, fo[3].y, fo[3].z);
         } else {
             int slot = atomicAdd(fb_count, 1);
             if (slot < kFallbackCap) fb_list[slot] = i;
@@ -128,10 +128,10 @@ __global__ void __launch_bounds__(kBlock) k_excl_force_fallback(const DeviceFF f
         if (!ok) ok = forceN_block(c1, c2, c3, c4, ff.excl_krs[i], true, red, out);
         if (threadIdx.x == 0) {
             if (ok) {
-                add_force(f, q.x, out[0][0], out[0][1], out[0][2]);
-                add_force(f, q.y, out[1][0], out[1][1], out[1][2]);
-                add_force(f, q.z, out[2][0], out[2][1], out[2][2]);
-                add_force(f, q.w, out[3][0], out[3][1], out[3][2]);
+                target_add(tgt, f, q.x, out[0][0], out[0][1], out[0][2]);
+                target_add(tgt, f, q.y, out[1][0], out[1][1], out[1][2]);
+                target_add(tgt, f, q.z, out[2][0], out[2][1], out[2][2]);
+                target_add(tgt, f, q.w, out[3][0], out[3][1], out[3][2]);
             } else {
                 atomicOr(status, 1);
             }

@@ -204,8 +204,8 @@ __global__ void __launch_bounds__(kMaxShapeThreads) k_bonded_forces(const Device
                     if (q.x < 0) break;  // padding record
                     double2 p = ff.stretch_p[i];
                     T3<R> F = stretch_force<R>(P(q.x), P(q.y), p.x, p.y);
-                    add_force(f, q.y, F.x, F.y, F.z);
-                    add_force(f, q.x, -F.x, -F.y, -F.z);
+                    target_add(tgt, f, q.y, F.x, F.y, F.z);
+                    target_add(tgt, f, q.x, -F.x, -F.y, -F.z);
                 }
                 break;
             case 1:
@@ -216,9 +216,9 @@ __global__ void __launch_bounds__(kMaxShapeThreads) k_bonded_forces(const Device
                     V3 c1 = P(q.x), c2 = P(q.y), c3 = P(q.z);
                     T3<R> Fr1, Fr2;
                     bend_force<R>(diff<R>(c1, c2), diff<R>(c2, c3), p.x, p.y, Fr1, Fr2);
-                    add_force(f, q.x, -Fr1.x, -Fr1.y, -Fr1.z);
-                    add_force(f, q.y, Fr1.x - Fr2.x, Fr1.y - Fr2.y, Fr1.z - Fr2.z);
-                    add_force(f, q.z, Fr2.x, Fr2.y, Fr2.z);
+                    target_add(tgt, f, q.x, -Fr1.x, -Fr1.y, -Fr1.z);
+                    target_add(tgt, f, q.y, Fr1.x - Fr2.x, Fr1.y - Fr2.y, Fr1.z - Fr2.z);
+                    target_add(tgt, f, q.z, Fr2.x, Fr2.y, Fr2.z);
                 }
                 break;
             case 2:
@@ -230,10 +230,10 @@ __global__ void __launch_bounds__(kMaxShapeThreads) k_bonded_forces(const Device
                     double4 p = s == 2 ? ff.linker_p[i] : ff.motor_p[i];
                     T3<R> Fl = spring_force<R>(P(q.x), P(q.y), P(q.z), P(q.w), p.x, p.y, p.z, p.w);
                     const R a1 = R(1) - R(p.z), a2 = R(p.z), b1 = R(1) - R(p.w), b2 = R(p.w);
-                    add_force(f, q.x, -Fl.x * a1, -Fl.y * a1, -Fl.z * a1);
-                    add_force(f, q.y, -Fl.x * a2, -Fl.y * a2, -Fl.z * a2);
-                    add_force(f, q.z, Fl.x * b1, Fl.y * b1, Fl.z * b1);
-                    add_force(f, q.w, Fl.x * b2, Fl.y * b2, Fl.z * b2);
+                    target_add(tgt, f, q.x, -Fl.x * a1, -Fl.y * a1, -Fl.z * a1);
+                    target_add(tgt, f, q.y, -Fl.x * a2, -Fl.y * a2, -Fl.z * a2);
+                    target_add(tgt, f, q.z, Fl.x * b1, Fl.y * b1, Fl.z * b1);
+                    target_add(tgt, f, q.w, Fl.x * b2, Fl.y * b2, Fl.z * b2);
                 }
                 break;
             }
@@ -274,10 +274,10 @@ __global__ void __launch_bounds__(kMaxShapeThreads) k_bonded_forces(const Device
                         F2.x += P2.x; F2.y += P2.y; F2.z += P2.z;
                         F3.x += P3.x; F3.y += P3.y; F3.z += P3.z;
                     }
-                    add_force(f, q.x, F1.x, F1.y, F1.z);
-                    add_force(f, q.y, F2.x, F2.y, F2.z);
-                    add_force(f, q.z, F3.x, F3.y, F3.z);
-                    add_force(f, q.w, F4.x, F4.y, F4.z);
+                    target_add(tgt, f, q.x, F1.x, F1.y, F1.z);
+                    target_add(tgt, f, q.y, F2.x, F2.y, F2.z);
+                    target_add(tgt, f, q.z, F3.x, F3.y, F3.z);
+                    target_add(tgt, f, q.w, F4.x, F4.y, F4.z);
                 }
                 break;
             default:
@@ -287,7 +287,7 @@ __global__ void __launch_bounds__(kMaxShapeThreads) k_bonded_forces(const Device
                     double2 p = ff.boundary_p[i];
                     double4 pl = ff.planes[ff.boundary_plane[i]];
                     R f0 = boundary_force_mag<R>(pl, P(o), p.x, p.y);
-                    add_force(f, o, f0 * R(pl.x), f0 * R(pl.y), f0 * R(pl.z));
+                    target_add(tgt, f, o, f0 * R(pl.x), f0 * R(pl.y), f0 * R(pl.z));
                 }
                 break;
         }
@@ -297,6 +297,25 @@ __global__ void __launch_bounds__(kMaxShapeThreads) k_bonded_forces(const Device
 }  // namespace
 
 int bonded_blocks(const DeviceFF& ff) { return ff.seg[6]; }
+
+namespace {
+
+// Deterministic mode: the fixed-point sums back to double, in place.
+__global__ void __launch_bounds__(256) k_fixed_to_double(const ForceTarget t, int n3) {
+    if (t.skip && *t.skip) return;
+    double* __restrict__ f = target_force(t);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x)
+        f[i] = double(__double_as_longlong(f[i])) / kFixedScale;
+}
+
+}  // namespace
+
+void launch_fixed_to_double(const ForceTarget& t, int n3, cudaStream_t s) {
+    if (!t.fixed || n3 <= 0) return;
+    int g = (n3 + 255) / 256;
+    g = g > 148 * 8 ? 148 * 8 : g;
+    k_fixed_to_double<<<g, 256, 0, s>>>(t, n3);
+}
 
 namespace {
 
@@ -383,6 +402,7 @@ void launch_forces(const ChainDev& ch, const DeviceFF& ff, int prec, const doubl
     bonded_forces_group<0, 2>(ff, prec, x, t, b[3]);
     launch_excl_forces(ff, prec, x, t, fs, s);
     if (fk) join_from(fk, s, 3);
+    launch_fixed_to_double(t, 3 * ch.n_pos, s);
 }
 
 void launch_evaluate(const ChainDev& ch, const DeviceFF& ff, int prec, const double* x, const double* d,
@@ -422,6 +442,7 @@ void launch_evaluate(const ChainDev& ch, const DeviceFF& ff, int prec, const dou
         cudaEventRecord(fk->join[k], fk->side[k]);
         cudaStreamWaitEvent(s, fk->join[k], 0);
     }
+    launch_fixed_to_double(t, 3 * ch.n_pos, s);
 }
 
 }  // namespace mb

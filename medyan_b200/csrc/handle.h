@@ -16,6 +16,8 @@
 
 namespace mb {
 
+struct medyan_async;  // async.cu
+
 template <class T>
 struct DevBuf {
     T* p = nullptr;
@@ -143,6 +145,7 @@ struct medyan_mech {
     mb::ForceScratch fs{};
     // fused passes (pass.cu): layout choice, energy rows and arrival ticket
     int pass_layout = 1;                  // 0 fused, 1 one kernel per potential group
+    int deterministic = 0;                // 1: fixed-point force sums (ForceTarget::fixed)
     mb::DevBuf<double> pass_rows, pass_group_rows;
     mb::DevBuf<unsigned int> pass_group_ticket, pass_ticket;
     mb::PassScratch pass_scratch() const {
@@ -212,6 +215,10 @@ struct medyan_mech {
     struct NL;
     NL* nl = nullptr;
 
+    // asynchronous evaluations (async.cu): copy streams, staging slots and
+    // their events, created by the first medyan_mech_evaluate_async
+    mb::medyan_async* async = nullptr;
+
     medyan_status init();
     ~medyan_mech();
 };
@@ -242,4 +249,5 @@ medyan_status cg_enqueue(medyan_mech* h, const medyan_cg_params* p, const double
 medyan_status cg_collect(medyan_mech* h, double* coord_out, double* force_out, medyan_min_result* out);
 cudaError_t coords_to_host(medyan_mech* h, const double* dev, double* host, cudaStream_t s);
 void destroy_nl(medyan_mech* h);
+void destroy_async(medyan_mech* h);
 }  // namespace mb

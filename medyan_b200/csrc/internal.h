@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "medyan_b200.h"
+#include "device_math.cuh"
 
 namespace mb {
 
@@ -97,6 +98,13 @@ struct EnergyScratch {
 // standalone path uses f0 at x. The minimizer passes both force buffers and
 // a device-side parity (the new force goes to the buffer not holding the
 // current one), a skip flag, and a move x + (*lam)*d evaluated on the fly.
+//
+// fixed = 1 (deterministic mode): every contribution is rounded to a 64-bit
+// integer count of kFixedUnit pN and summed with integer additions, which
+// give the same bits in any order; the pass ends with a conversion of the
+// sums back to double in place (launch_fixed_to_double). A contribution of
+// kFixedRange pN or more is out of the format's range: it sets bit 2 of
+// *status and is dropped.
 struct ForceTarget {
     double* f0;
     double* f1;
@@ -104,10 +112,55 @@ struct ForceTarget {
     const int* skip;     // nullable: nonzero -> the pass does nothing
     const double* d;     // nullable: positions are x
     const double* lam;   // step along d
+    int fixed;           // 1: deterministic fixed-point accumulation
+    int* status;         // fixed mode: range flag (bit 2)
 };
+
+constexpr double kFixedScale = 4294967296.0;  // counts per pN (2^32: 2.3e-10 pN resolution)
+constexpr double kFixedRange = 16777216.0;    // |contribution| < 2^24 pN: sums of up to 2^7 such fit in 63 bits
 
 __device__ __forceinline__ double* target_force(const ForceTarget& t) {
     return t.parity ? (*t.parity ? t.f0 : t.f1) : t.f0;
+}
+
+// v as a fixed-point count (0 and the range flag when out of range).
+__device__ __forceinline__ long long fixed_of(double v, int* status) {
+    if (!(fabs(v) < kFixedRange)) {
+        if (status) atomicOr(status, 4);
+        return 0;
+    }
+    return __double2ll_rn(v * kFixedScale);
+}
+
+__device__ __forceinline__ void red_add_fixed(double* p, long long v) {
+    asm volatile("red.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Adds a bead's force contribution to the target's buffer f.
+template <class R>
+__device__ __forceinline__ void target_add(const ForceTarget& t, double* __restrict__ f, int off, R fx, R fy, R fz) {
+    if (t.fixed) {
+        red_add_fixed(f + off, fixed_of(double(fx), t.status));
+        red_add_fixed(f + off + 1, fixed_of(double(fy), t.status));
+        red_add_fixed(f + off + 2, fixed_of(double(fz), t.status));
+    } else {
+        add_force(f, off, fx, fy, fz);
+    }
+}
+
+// Stores a bead's whole force (the chain pass, which writes before any
+// addition).
+__device__ __forceinline__ void target_store(const ForceTarget& t, double* __restrict__ f, int off, double fx, double fy,
+                                             double fz) {
+    if (t.fixed) {
+        f[off] = __longlong_as_double(fixed_of(fx, t.status));
+        f[off + 1] = __longlong_as_double(fixed_of(fy, t.status));
+        f[off + 2] = __longlong_as_double(fixed_of(fz, t.status));
+    } else {
+        f[off] = fx;
+        f[off + 1] = fy;
+        f[off + 2] = fz;
+    }
 }
 
 struct ForceScratch {
@@ -142,6 +195,9 @@ void launch_evaluate(const ChainDev& ch, const DeviceFF& ff, int prec, const dou
                      const ForceTarget& t, const EnergyScratch& es, const ForceScratch& fs, cudaStream_t s,
                      const Fork* fk);
 void launch_chain_forces(const ChainDev& ch, int prec, const double* x, const ForceTarget& t, cudaStream_t s);
+// Deterministic mode: the target's fixed-point sums back to double, in place
+// (nothing when t.fixed is 0).
+void launch_fixed_to_double(const ForceTarget& t, int n3, cudaStream_t s);
 // table (optional): block b evaluates positions [table[b].y, table[b].z) of one
 // replica (batched layouts), table_blocks blocks; else a grid-stride pass.
 void launch_chain_energy(const ChainDev& ch, int prec, const double* x, const double* d, const LambdaSet* lam,

@@ -190,10 +190,10 @@ __device__ __noinline__ void pass_finish(const PassArgs& a) {
             if (!ok) ok = forceN_block(c1, c2, c3, c4, a.ff.excl_krs[i], true, red, out);
             if (threadIdx.x == 0) {
                 if (ok) {
-                    add_force(f, bs.x, out[0][0], out[0][1], out[0][2]);
-                    add_force(f, bs.y, out[1][0], out[1][1], out[1][2]);
-                    add_force(f, bs.z, out[2][0], out[2][1], out[2][2]);
-                    add_force(f, bs.w, out[3][0], out[3][1], out[3][2]);
+                    target_add(a.t, f, bs.x, out[0][0], out[0][1], out[0][2]);
+                    target_add(a.t, f, bs.y, out[1][0], out[1][1], out[1][2]);
+                    target_add(a.t, f, bs.z, out[2][0], out[2][1], out[2][2]);
+                    target_add(a.t, f, bs.w, out[3][0], out[3][1], out[3][2]);
                 } else {
                     atomicOr(a.f_status, 1);
                 }
@@ -300,9 +300,7 @@ __device__ __forceinline__ void chain_tile(const PassArgs& a, const Pos& P, doub
             const double fx = double(Fp.x) - double(Fl.x) + double(Bp.x) + (double(A.x) - double(B.x)) - double(An.x);
             const double fy = double(Fp.y) - double(Fl.y) + double(Bp.y) + (double(A.y) - double(B.y)) - double(An.y);
             const double fz = double(Fp.z) - double(Fl.z) + double(Bp.z) + (double(A.z) - double(B.z)) - double(An.z);
-            red_add(f + 3 * q, fx);
-            red_add(f + 3 * q + 1, fy);
-            red_add(f + 3 * q + 2, fz);
+            target_add(a.t, f, 3 * q, fx, fy, fz);
         }
     }
     if constexpr (E) {
@@ -316,8 +314,8 @@ __device__ __forceinline__ void chain_tile(const PassArgs& a, const Pos& P, doub
 // Record i of bonded segment s (0 leftover stretch, 1 leftover bend, 2
 // linker, 3 motor, 5 boundary): energy into acc[0], forces added to f.
 template <class R, bool E, bool F>
-__device__ __forceinline__ void bonded_record(const DeviceFF& ff, const Pos& P, double* __restrict__ f, int s, int i,
-                                              double (&acc)[4]) {
+__device__ __forceinline__ void bonded_record(const DeviceFF& ff, const ForceTarget& t, const Pos& P,
+                                              double* __restrict__ f, int s, int i, double (&acc)[4]) {
     switch (s) {
         case 0:
             if (i < ff.n_stretch) {
@@ -327,8 +325,8 @@ __device__ __forceinline__ void bonded_record(const DeviceFF& ff, const Pos& P, 
                 if constexpr (E) acc[0] += stretch_energy<double>(c1, c2, p.x, p.y);
                 if constexpr (F) {
                     const T3<R> Fs = stretch_force<R>(c1, c2, p.x, p.y);
-                    add_force(f, q.y, Fs.x, Fs.y, Fs.z);
-                    add_force(f, q.x, -Fs.x, -Fs.y, -Fs.z);
+                    target_add(t, f, q.y, Fs.x, Fs.y, Fs.z);
+                    target_add(t, f, q.x, -Fs.x, -Fs.y, -Fs.z);
                 }
             }
             break;
@@ -341,9 +339,9 @@ __device__ __forceinline__ void bonded_record(const DeviceFF& ff, const Pos& P, 
                 if constexpr (F) {
                     T3<R> Fr1, Fr2;
                     bend_force<R>(diff<R>(c1, c2), diff<R>(c2, c3), p.x, p.y, Fr1, Fr2);
-                    add_force(f, q.x, -Fr1.x, -Fr1.y, -Fr1.z);
-                    add_force(f, q.y, Fr1.x - Fr2.x, Fr1.y - Fr2.y, Fr1.z - Fr2.z);
-                    add_force(f, q.z, Fr2.x, Fr2.y, Fr2.z);
+                    target_add(t, f, q.x, -Fr1.x, -Fr1.y, -Fr1.z);
+                    target_add(t, f, q.y, Fr1.x - Fr2.x, Fr1.y - Fr2.y, Fr1.z - Fr2.z);
+                    target_add(t, f, q.z, Fr2.x, Fr2.y, Fr2.z);
                 }
             }
             break;
@@ -358,10 +356,10 @@ __device__ __forceinline__ void bonded_record(const DeviceFF& ff, const Pos& P, 
                 if constexpr (F) {
                     const T3<R> Fl = spring_force<R>(c1, c2, c3, c4, p.x, p.y, p.z, p.w);
                     const R a1 = R(1) - R(p.z), a2 = R(p.z), b1 = R(1) - R(p.w), b2 = R(p.w);
-                    add_force(f, q.x, -Fl.x * a1, -Fl.y * a1, -Fl.z * a1);
-                    add_force(f, q.y, -Fl.x * a2, -Fl.y * a2, -Fl.z * a2);
-                    add_force(f, q.z, Fl.x * b1, Fl.y * b1, Fl.z * b1);
-                    add_force(f, q.w, Fl.x * b2, Fl.y * b2, Fl.z * b2);
+                    target_add(t, f, q.x, -Fl.x * a1, -Fl.y * a1, -Fl.z * a1);
+                    target_add(t, f, q.y, -Fl.x * a2, -Fl.y * a2, -Fl.z * a2);
+                    target_add(t, f, q.z, Fl.x * b1, Fl.y * b1, Fl.z * b1);
+                    target_add(t, f, q.w, Fl.x * b2, Fl.y * b2, Fl.z * b2);
                 }
             }
             break;
@@ -375,7 +373,7 @@ __device__ __forceinline__ void bonded_record(const DeviceFF& ff, const Pos& P, 
                 if constexpr (E) acc[0] += boundary_energy<double>(pl, c, p.x, p.y);
                 if constexpr (F) {
                     const R f0 = boundary_force_mag<R>(pl, c, p.x, p.y);
-                    add_force(f, o, f0 * R(pl.x), f0 * R(pl.y), f0 * R(pl.z));
+                    target_add(t, f, o, f0 * R(pl.x), f0 * R(pl.y), f0 * R(pl.z));
                 }
             }
             break;
@@ -409,7 +407,7 @@ __global__ void __launch_bounds__(kPassThreads, (E && F) ? kMainBlocksPerSM - 1 
             for (int j = 1; j < 5; ++j) k += b >= a.seg[j] ? 1 : 0;
             const int i = (b - a.seg[k]) * blockDim.x + threadIdx.x;
             double e[4] = {0.0, 0.0, 0.0, 0.0};
-            bonded_record<R, E, F>(ff, P, f, k == 4 ? 5 : k, i, e);
+            bonded_record<R, E, F>(ff, a.t, P, f, k == 4 ? 5 : k, i, e);
             // acc: 0 stretching, 1 bending, 2 linker, 3 motor, 4 boundary
 #pragma unroll
             for (int j = 0; j < kMainVals; ++j)
@@ -471,10 +469,10 @@ __global__ void __launch_bounds__(kPassThreads) k_pass_branch(const __grid_const
                 F2.x += P2.x; F2.y += P2.y; F2.z += P2.z;
                 F3.x += P3.x; F3.y += P3.y; F3.z += P3.z;
             }
-            add_force(f, q.x, F1.x, F1.y, F1.z);
-            add_force(f, q.y, F2.x, F2.y, F2.z);
-            add_force(f, q.z, F3.x, F3.y, F3.z);
-            add_force(f, q.w, F4.x, F4.y, F4.z);
+            target_add(a.t, f, q.x, F1.x, F1.y, F1.z);
+            target_add(a.t, f, q.y, F2.x, F2.y, F2.z);
+            target_add(a.t, f, q.z, F3.x, F3.y, F3.z);
+            target_add(a.t, f, q.w, F4.x, F4.y, F4.z);
         }
     }
     block_done<1, E, F>(a, acc, a.row_branch + blockIdx.x, false);
@@ -509,10 +507,10 @@ __global__ void __launch_bounds__(kExclThreadsMax) k_pass_excl(const __grid_cons
         if constexpr (F) {
             T3<double> fo[4];
             if (excl_force<EXACT>(c1, c2, c3, c4, krs, fo)) {
-                add_force(f, q.x, fo[0].x, fo[0].y, fo[0].z);
-                add_force(f, q.y, fo[1].x, fo[1].y, fo[1].z);
-                add_force(f, q.z, fo[2].x, fo[2].y, fo[2].z);
-                add_force(f, q.w, fo[3].x, fo[3].y, fo[3].z);
+                target_add(a.t, f, q.x, fo[0].x, fo[0].y, fo[0].z);
+                target_add(a.t, f, q.y, fo[1].x, fo[1].y, fo[1].z);
+                target_add(a.t, f, q.z, fo[2].x, fo[2].y, fo[2].z);
+                target_add(a.t, f, q.w, fo[3].x, fo[3].y, fo[3].z);
             } else {
                 const int slot = atomicAdd(a.f_fb_count, 1);
                 if (slot < kFallbackCap) a.f_fb_list[slot] = i;
@@ -642,6 +640,7 @@ void launch_pass_fused(const ChainDev& ch, const DeviceFF& ff, int prec, const d
             cudaStreamWaitEvent(s, fk->join[k], 0);
         }
     }
+    if (force) launch_fixed_to_double(*t, 3 * ch.n_pos, s);
 }
 
 cudaError_t init_pass_kernels() {

@@ -125,6 +125,30 @@ class ForceFieldManager:
             L.check(st, "medyan_mech_evaluate")
         return tot.value, per, f
 
+    def set_deterministic(self, on: bool = True) -> None:
+        """Fixed-point force sums: bitwise reproducible forces and minimizations."""
+        L.check(self.lib.medyan_mech_set_deterministic(self.handle, 1 if on else 0), "medyan_mech_set_deterministic")
+
+    def evaluate_many(self, coords):
+        """Energies and forces at each coordinate set of coords (a list of
+        arrays) through the asynchronous double-buffered entry point; returns
+        (energies [n, FF_COUNT + 1], forces list). The host buffers are
+        page-locked so that the copies overlap."""
+        import torch
+        n3 = 3 * self.n_beads
+        xs = [torch.from_numpy(f64(c).copy()).pin_memory() for c in coords]
+        fs = [torch.empty(n3, dtype=torch.float64).pin_memory() for _ in coords]
+        es = torch.empty((len(coords), FF_COUNT + 1), dtype=torch.float64).pin_memory()
+        pd = C.POINTER(C.c_double)
+        for i in range(len(coords)):
+            L.check(self.lib.medyan_mech_evaluate_async(
+                self.handle, C.cast(xs[i].data_ptr(), pd), C.cast(fs[i].data_ptr(), pd),
+                C.cast(es[i].data_ptr(), pd)), "medyan_mech_evaluate_async")
+        st = self.lib.medyan_mech_wait(self.handle)
+        if st not in (0, 3):
+            L.check(st, "medyan_mech_wait")
+        return es.numpy().copy(), [f.numpy().copy() for f in fs]
+
     # -- minimizer ---------------------------------------------------------
     def minimize(self, coord, params: CGParams):
         """CGMethod::minimize on the device. Returns (status, coord, force, MinResult)."""
