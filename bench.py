@@ -150,17 +150,21 @@ def run_ours(args, rank: int, world: int) -> dict:
     x = net.flat_coords()
     bp, planes = net.boundary_params()
 
-    def make(prec):
+    def make_for(nw, prec):
+        bpn, _ = nw.boundary_params()
         ff = ForceFieldManager(prec)
-        ff.vectorize_all_force_fields(net.system_view())
-        ff.set_coords(x)
-        ff.set_cylinders(net.cylinders_view(), net.nl_params(), bp)
+        ff.vectorize_all_force_fields(nw.system_view())
+        ff.set_coords(nw.flat_coords())
+        ff.set_cylinders(nw.cylinders_view(), nw.nl_params(), bpn)
         ff.rebuild_neighbor_lists()
         ff.lib.medyan_mech_synchronize(ff.handle)
         # block and tile shapes per potential for this network (autotuner,
         # at setup, outside every timed region)
         ff.tuned_shapes = ff.autotune(reps=10)
         return ff
+
+    def make(prec):
+        return make_for(net, prec)
 
     ff = make(args.precision)
     L, h = ff.lib, ff.handle
@@ -322,9 +326,22 @@ def run_ours(args, rank: int, world: int) -> dict:
     result["roofline"] = roofline(fb / t_f / 1e9, fb)
     result["algorithmic_bytes"] = abytes
 
+    # neighbor-list rebuild on the device (host call, coordinates resident)
+    ff.rebuild_neighbor_lists()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(5):
+        ff.rebuild_neighbor_lists()
+    torch.cuda.synchronize()
+    result["nl_rebuild"] = {"rebuilds_per_s": 5 / (time.perf_counter() - t0),
+                            "timed": "medyan_mech_rebuild_neighbors (binning, pair search, re-vectorization of the "
+                                     "excluded-volume and boundary records), host call to return"}
     if not args.no_minimize and rank == 0:
         result["minimization"] = minimize_extras(net, make)
         result["batched_ensemble"] = batch_extras()
+        result["medium_network"] = medium_network_extras(make_for)
+    if rank == 0:
+        result["cpu_extras"] = cpu_extras(net, result.get("minimization"))
     for f in {id(ff): ff, id(ff64): ff64}.values():
         f.close()
     return result
@@ -367,31 +384,133 @@ def roofline(achieved_gbs: float, nbytes: int) -> dict:
 
 
 def minimize_extras(net, make) -> dict:
-    """One timed minimization (gradTol 1 pN, reference example CG params) per
-    precision on the same network: minimizations/s and the final-energy match."""
+    """Minimization of the benchmark network per precision with the
+    reference's criteria (gradTol 1 pN, or |dE|/|E| < 1e-9: whichever comes
+    first, CGMethod.hpp:1431) and the reference example's MAXDISTANCE and
+    LAMBDAMAX. Each timed run rebuilds the neighbor list at the start
+    coordinates first (the workload rebuilds it per minimization). With
+    deterministic force sums a run is bitwise reproducible, so one run per
+    precision is the number (a second is checked identical); three runs with
+    floating-point atomic sums show the spread that summation order alone
+    gives a trajectory."""
+    import numpy as np
     import torch
 
     from medyan_b200.forcefield import conjugate_gradient_params
-    out = {}
+    out = {"criteria": "gradTol 1 pN or energyRelTol 1e-9 (first met), maxDist 1 nm, lambdaMax 0.01",
+           "timed": "neighbor-list rebuild at the start coordinates + minimization"}
     p = conjugate_gradient_params(grad_tol=1.0, max_dist=1.0, lambda_max=0.01, energy_rel_tol=1e-9)
     x = net.flat_coords()
     warm = conjugate_gradient_params(grad_tol=1.0, energy_call_limit=3)
-    for prec in ("fp64", "mixed"):
-        ff = make(prec)
-        ff.minimize(x, warm)  # builds the minimizer's graph outside the timed call
+
+    def run(ff):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
+        ff.set_coords(x)
+        ff.rebuild_neighbor_lists()
         st, xm, fm, r = ff.minimize(x, p)
-        dt = time.perf_counter() - t0
-        out[prec] = {"status": st, "seconds": dt, "minimizations_per_s": 1.0 / dt, "iterations": r.num_iter,
-                     "us_per_iteration": 1e6 * dt / max(r.num_iter, 1),
-                     "energy_calls": r.num_energy_call, "force_calls": r.num_force_call,
-                     "energy_before": r.energy_before_total, "energy_after": r.energy_after_total,
-                     "grad_inf_norm": r.grad_inf_norm, "energy_rel_change": r.energy_rel_change}
+        return time.perf_counter() - t0, st, xm, r
+
+    for prec in ("fp64", "mixed"):
+        ff = make(prec)
+        ff.set_deterministic(True)
+        ff.minimize(x, warm)  # builds the minimizer's graph outside the timed runs
+        (dt, st, xm, r), (dt2, st2, xm2, r2) = run(ff), run(ff)
+        rec = {"status": st, "seconds": dt, "minimizations_per_s": 1.0 / dt, "iterations": r.num_iter,
+               "us_per_iteration": 1e6 * dt / max(r.num_iter, 1), "energy_calls": r.num_energy_call,
+               "force_calls": r.num_force_call, "energy_before": r.energy_before_total,
+               "energy_after": r.energy_after_total, "grad_inf_norm": r.grad_inf_norm,
+               "energy_rel_change": r.energy_rel_change,
+               "second_run_identical": bool(np.array_equal(xm, xm2) and r.num_iter == r2.num_iter),
+               "second_run_seconds": dt2}
+        ff.set_deterministic(False)
+        ff.minimize(x, warm)
+        atomic = [run(ff) for _ in range(3)]
+        ts = [a[0] for a in atomic]
+        rec["atomic_sums"] = {"seconds_median": statistics.median(ts), "seconds_min": min(ts), "seconds_max": max(ts),
+                              "iterations": [a[3].num_iter for a in atomic],
+                              "energy_after": [a[3].energy_after_total for a in atomic],
+                              "grad_inf_norm": [a[3].grad_inf_norm for a in atomic]}
+        out[prec] = rec
         ff.close()
-    if "fp64" in out and "mixed" in out:
-        e64, em = out["fp64"]["energy_after"], out["mixed"]["energy_after"]
-        out["final_energy_rel_diff_mixed_vs_fp64"] = abs(em - e64) / abs(e64)
+    e64, em = out["fp64"]["energy_after"], out["mixed"]["energy_after"]
+    out["final_energy_rel_diff_mixed_vs_fp64"] = abs(em - e64) / abs(e64)
+    ea = out["fp64"]["atomic_sums"]["energy_after"]
+    out["final_energy_rel_spread_fp64_atomic_runs"] = (max(ea) - min(ea)) / abs(e64)
+    return out
+
+
+def cpu_extras(net, gpu_min: dict | None) -> dict:
+    """CPU baselines beside the device numbers, each a bounded sample on one
+    host thread: the reference's own CGMethod (oracle/_ref) on the benchmark
+    network for a fixed number of energy calls (seconds per CG iteration; the
+    minimizations/s estimate scales it by the device FP64 run's iteration
+    count, the same algorithm and criteria), and the neighbor-list rebuild
+    (the oracle's restatement of HybridCylinderCylinderNL, whose reference
+    code is entangled with the simulator's globals and not compiled)."""
+    from medyan_b200.forcefield import conjugate_gradient_params
+    from oracle.oracle import Oracle, Reference
+    out = {}
+    orc = Oracle()
+    st, extra = orc.complete(net)
+    sv = net.system_view(**extra)
+    x = net.flat_coords()
+    if Reference.available():
+        ref, kind = Reference(), "reference"
+    else:
+        ref, kind = orc, "port"
+    p = conjugate_gradient_params(grad_tol=1.0, max_dist=1.0, lambda_max=0.01, energy_rel_tol=1e-9,
+                                  energy_call_limit=120)
+    t0 = time.perf_counter()
+    s, xm, fm, r = ref.minimize(sv, x, p)
+    dt = time.perf_counter() - t0
+    # a run stopped by its call limit reports numIter -1; every iteration
+    # after the first force call makes one more
+    iters = r.num_iter if r.num_iter > 0 else r.num_force_call - 1
+    s_iter = dt / max(iters, 1)
+    rec = {"kind": kind, "cores": 1, "sample": f"{iters} CG iterations ({r.num_energy_call} energy, "
+                                                f"{r.num_force_call} force calls) in {dt:.1f} s",
+           "seconds_per_iteration": s_iter}
+    if gpu_min and "fp64" in gpu_min:
+        n_it = gpu_min["fp64"]["iterations"]
+        rec["minimizations_per_s_estimate"] = 1.0 / (s_iter * n_it)
+        rec["estimate"] = f"1 / (seconds per iteration x {n_it} iterations of the device FP64 run)"
+    out["minimization"] = rec
+    cv = net.cylinders_view()
+    nl = net.nl_params()
+    orc.neighbor_pairs(cv, x, net.n_beads, nl)
+    n, t0 = 0, time.perf_counter()
+    while n < 3:
+        orc.neighbor_pairs(cv, x, net.n_beads, nl)
+        n += 1
+    dt = time.perf_counter() - t0
+    out["nl_rebuild"] = {"kind": "port", "cores": 1, "rebuilds_per_s": n / dt,
+                         "sample": f"{n} rebuilds of the 400k-cylinder list in {dt:.1f} s"}
+    return out
+
+
+def medium_network_extras(make_for) -> dict:
+    """The medium network (2,000 filaments x 20 cylinders, 42k beads, 4k
+    linkers, 500 motors, 400 branch points): force-evals/s on the device in
+    both precisions (same protocol as the headline) and on one host thread
+    with the reference's kernels."""
+    import torch
+
+    from medyan_b200.network import make_workload
+    net = make_workload(1)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    out = {"workload": "cfg1_2000x20_5um", "n_beads": net.n_beads}
+    for prec in ("fp64", "mixed"):
+        ff = make_for(net, prec)
+        L, h = ff.lib, ff.handle
+        s = torch.cuda.ExternalStream(L.medyan_mech_stream(h))
+        t = timed_passes(L.medyan_mech_enqueue_evaluate, h, L, s, flush, 20, 5)
+        out[prec] = {"force_evals_per_s": len(t) / sum(t), "us_per_step": 1e6 * sum(t) / len(t),
+                     "launch_shapes": ff.tuned_shapes}
+        ff.close()
+    rate, n, dt, kind = cpu_reference_rate(net, 3.0)
+    out["cpu"] = {"force_evals_per_s": rate, "kind": kind, "cores": 1,
+                  "sample": f"{n} energy+force evaluations in {dt:.1f} s"}
     return out
 
 
