@@ -415,16 +415,17 @@ typedef struct medyan_launch_shapes {
     int32_t chain_energy_blocks_per_sm; /* fixed grid of the filament-chain energy
                                        kernel, in blocks of 256 per SM: 2, 4, 8 */
     int32_t pass_layout;            /* kernels of the standalone passes and of the
-                                       minimizer's force pass: 0 = fused (a zero
-                                       fill, then three kernels side by side: chains
-                                       with linker, motor, boundary and leftover
-                                       records; branch points; excluded volume;
-                                       energy and force of an interaction from one
-                                       read), 1 = one kernel per potential group
-                                       (chain forces first, the rest after) */
+                                       minimizer's force pass: 0 = fused (forces: a
+                                       zero fill, then three kernels side by side:
+                                       chains with linker, motor, boundary and
+                                       leftover records; branch points; excluded
+                                       volume; energies: the same three kernels
+                                       with the row reduction built in), 1 = one
+                                       kernel per potential group (chain forces
+                                       first, the rest after) */
 } medyan_launch_shapes;
 
-/* The defaults are 256, 64, 256, 4, 1. Setting shapes re-derives the block
+/* The defaults are 256, 64, 256, 4, 0. Setting shapes re-derives the block
    tables and invalidates the handle's captured passes (rebuilt on next use). */
 medyan_status medyan_mech_set_shapes(medyan_mech* h, const medyan_launch_shapes* shapes);
 medyan_status medyan_mech_get_shapes(medyan_mech* h, medyan_launch_shapes* shapes);

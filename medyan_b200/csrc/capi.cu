@@ -273,8 +273,12 @@ medyan_status refresh_device_ff(medyan_mech* h) {
         if (e == cudaSuccess) e = h->pass_rows.reserve((size_t)pg.rows * MEDYAN_FF_COUNT);
         if (e == cudaSuccess) e = h->pass_group_rows.reserve((size_t)pg.groups * MEDYAN_FF_COUNT);
         if (e == cudaSuccess) e = h->pass_group_ticket.reserve((size_t)pg.groups);
+        if (e == cudaSuccess) e = h->pass_fgroup_ticket.reserve((size_t)pg.groups);
         if (e == cudaSuccess)
             e = cudaMemsetAsync(h->pass_group_ticket.raw(), 0, sizeof(unsigned int) * h->pass_group_ticket.cap,
+                                h->stream);
+        if (e == cudaSuccess)
+            e = cudaMemsetAsync(h->pass_fgroup_ticket.raw(), 0, sizeof(unsigned int) * h->pass_fgroup_ticket.cap,
                                 h->stream);
     }
     if (e != cudaSuccess) return cuda_status(e);
@@ -303,7 +307,8 @@ void enqueue_forces(medyan_mech* h, const double* x, double* f, cudaStream_t s) 
 void enqueue_force_target(medyan_mech* h, const double* x, const ForceTarget& t, const ForceScratch& fs,
                           cudaStream_t s) {
     if (h->pass_layout == 0)
-        launch_pass_fused(h->chain, h->ff, h->prec, x, &t, false, nullptr, h->es, fs, h->pass_scratch(), s, &h->fork);
+        launch_pass_fused(h->chain, h->ff, h->prec, x, &t, false, nullptr, h->es, fs, h->pass_scratch(),
+                          h->pass_scratch_forces(), s, &h->fork);
     else
         launch_forces(h->chain, h->ff, h->prec, x, t, fs, s, &h->fork);
 }
@@ -353,8 +358,8 @@ cudaError_t ensure_pass_graph(medyan_mech* h, int which) {
     const ForceTarget t{h->f.raw(), nullptr, nullptr, nullptr, nullptr, nullptr, h->deterministic, h->fs.status};
     if (h->pass_layout == 0)
         launch_pass_fused(h->chain, h->ff, h->prec, h->x.raw(), which == kPassEnergy ? nullptr : &t,
-                          which != kPassForces, h->lam_zero.raw(), h->es, h->fs, h->pass_scratch(), h->stream,
-                          &h->fork);
+                          which != kPassForces, h->lam_zero.raw(), h->es, h->fs, h->pass_scratch(),
+                          h->pass_scratch_forces(), h->stream, &h->fork);
     else if (which == kPassBoth)
         launch_evaluate(h->chain, h->ff, h->prec, h->x.raw(), nullptr, h->lam_zero.raw(), t, h->es, h->fs, h->stream,
                         &h->fork);
@@ -407,7 +412,7 @@ medyan_status medyan_mech::init() {
     if (e == cudaSuccess) e = f_fb_list.reserve(kFallbackCap);
     if (e == cudaSuccess) e = force_status.reserve(1);
     if (e == cudaSuccess) e = lam_zero.reserve(1);
-    if (e == cudaSuccess) e = pass_ticket.reserve(1);
+    if (e == cudaSuccess) e = pass_ticket.reserve(2);
     if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&small), sizeof(*small));
     if (e != cudaSuccess) return cuda_status(e);
     cudaMemsetAsync(x.raw(), 0, sizeof(double) * (n3 ? n3 : 1), stream);
@@ -416,7 +421,7 @@ medyan_status medyan_mech::init() {
     cudaMemsetAsync(e_ticket.raw(), 0, sizeof(unsigned int), stream);
     cudaMemsetAsync(f_fb_count.raw(), 0, sizeof(int), stream);
     cudaMemsetAsync(force_status.raw(), 0, sizeof(int), stream);
-    cudaMemsetAsync(pass_ticket.raw(), 0, sizeof(unsigned int), stream);
+    cudaMemsetAsync(pass_ticket.raw(), 0, 2 * sizeof(unsigned int), stream);
     LambdaSet z{};
     z.K = 1;
     e = lam_zero.assign(&z, 1, stream);

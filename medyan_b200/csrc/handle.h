@@ -144,12 +144,16 @@ struct medyan_mech {
     mb::EnergyScratch es{};
     mb::ForceScratch fs{};
     // fused passes (pass.cu): layout choice, energy rows and arrival ticket
-    int pass_layout = 1;                  // 0 fused, 1 one kernel per potential group
+    int pass_layout = 0;                  // 0 fused, 1 one kernel per potential group
     int deterministic = 0;                // 1: fixed-point force sums (ForceTarget::fixed)
+    // energy side; the force side has its own tickets (its rows are unused)
     mb::DevBuf<double> pass_rows, pass_group_rows;
-    mb::DevBuf<unsigned int> pass_group_ticket, pass_ticket;
+    mb::DevBuf<unsigned int> pass_group_ticket, pass_ticket, pass_fgroup_ticket;
     mb::PassScratch pass_scratch() const {
         return mb::PassScratch{pass_rows.raw(), pass_group_rows.raw(), pass_group_ticket.raw(), pass_ticket.raw()};
+    }
+    mb::PassScratch pass_scratch_forces() const {
+        return mb::PassScratch{nullptr, nullptr, pass_fgroup_ticket.raw(), pass_ticket.raw() + 1};
     }
 
     // internal bead order (chain.cu), fixed at create: internal position p

@@ -414,7 +414,8 @@ __global__ void __launch_bounds__(kPassThreads, (E && F) ? kMainBlocksPerSM - 1 
                 if (j == k) acc[j] += e[0];
         }
     }
-    block_done<0, E, F>(a, acc, a.row_main + blockIdx.x, false);
+    // a force-only pass has no rows here: the main kernel's blocks take no ticket
+    if constexpr (E) block_done<0, E, F>(a, acc, a.row_main + blockIdx.x, false);
 }
 
 // ------------------------------------------------------------ branch points
@@ -475,7 +476,7 @@ __global__ void __launch_bounds__(kPassThreads) k_pass_branch(const __grid_const
             target_add(a.t, f, q.w, F4.x, F4.y, F4.z);
         }
     }
-    block_done<1, E, F>(a, acc, a.row_branch + blockIdx.x, false);
+    if constexpr (E) block_done<1, E, F>(a, acc, a.row_branch + blockIdx.x, false);
 }
 
 // ------------------------------------------------------------ excluded volume
@@ -545,7 +546,7 @@ void launch_kernels(const PassArgs& a, const PassGeometry& g, int prec, cudaStre
             k_pass_excl<E, F, false><<<g.excl_blocks, g.excl_threads, 0, s_excl>>>(a);
     }
     if (g.branch_blocks > 0) k_pass_branch<R, E, F><<<g.branch_blocks, g.threads, 0, s_branch>>>(a);
-    k_pass_main<R, E, F><<<g.main_blocks, g.threads, 0, s_main>>>(a);
+    k_pass_main<R, E, F><<<E ? g.main_blocks : g.main_blocks_forces, g.threads, 0, s_main>>>(a);
 }
 
 }  // namespace
@@ -575,15 +576,21 @@ PassGeometry pass_geometry(const ChainDev& ch, const DeviceFF& ff) {
     const int eb = (ff.n_excl + g.excl_threads - 1) / g.excl_threads;
     const int ecap = g_num_sms * 32;
     g.excl_blocks = eb < ecap ? eb : ecap;
+    // a force-only pass: one unit per block (its main and branch blocks take
+    // no ticket, so a block's end holds nothing up)
+    const int fcap = g_num_sms * 64;
+    g.main_blocks_forces = units < 1 ? 1 : (units < fcap ? units : fcap);
     g.rows = g.main_blocks + g.branch_blocks + g.excl_blocks;
     g.groups = (g.rows + kGroup - 1) / kGroup;
     return g;
 }
 
-void launch_pass_fused(const ChainDev& ch, const DeviceFF& ff, int prec, const double* x, const ForceTarget* t,
-                       bool energy, const LambdaSet* lam_set, const EnergyScratch& es, const ForceScratch& fs,
-                       const PassScratch& ps, cudaStream_t s, const Fork* fk) {
-    const PassGeometry g = pass_geometry(ch, ff);
+namespace {
+
+// The argument block of one energy-only or force-only pass.
+PassArgs pass_args(const ChainDev& ch, const DeviceFF& ff, const PassGeometry& g, const double* x,
+                   const ForceTarget* t, bool energy, const LambdaSet* lam_set, const EnergyScratch& es,
+                   const ForceScratch& fs, const PassScratch& ps) {
     PassArgs a{};
     a.ch = ch;
     a.ff = ff;
@@ -593,11 +600,13 @@ void launch_pass_fused(const ChainDev& ch, const DeviceFF& ff, int prec, const d
     a.group_rows = ps.group_rows;
     a.group_ticket = ps.group_ticket;
     a.ticket = ps.ticket;
-    a.n_rows = g.rows;
-    a.n_groups = g.groups;
+    // the blocks that take tickets: every block of an energy pass; of a
+    // force-only pass the excluded-volume blocks, which own the fallback queue
+    a.n_rows = energy ? g.rows : g.excl_blocks;
+    a.n_groups = (a.n_rows + kGroup - 1) / kGroup;
     a.row_main = 0;
     a.row_branch = g.main_blocks;
-    a.row_excl = g.main_blocks + g.branch_blocks;
+    a.row_excl = energy ? g.main_blocks + g.branch_blocks : 0;
     a.nch = g.nch;
     a.nb_main = g.nb_main;
     for (int k = 0; k < 6; ++k) a.seg[k] = g.seg[k];
@@ -609,33 +618,51 @@ void launch_pass_fused(const ChainDev& ch, const DeviceFF& ff, int prec, const d
     a.f_fb_count = fs.fb_count;
     a.f_fb_list = fs.fb_list;
     a.f_status = fs.status;
+    return a;
+}
+
+}  // namespace
+
+void launch_pass_fused(const ChainDev& ch, const DeviceFF& ff, int prec, const double* x, const ForceTarget* t,
+                       bool energy, const LambdaSet* lam_set, const EnergyScratch& es, const ForceScratch& fs,
+                       const PassScratch& ps, const PassScratch& ps_forces, cudaStream_t s, const Fork* fk) {
+    const PassGeometry g = pass_geometry(ch, ff);
     const bool force = t != nullptr;
+    const bool mixed = prec == MEDYAN_PREC_MIXED;
+    // streams: the force side on s, sides 0-1; the energy side on sides 2-4
+    // (everything on s without a fork)
+    cudaStream_t sf[3] = {s, s, s}, se[3] = {s, s, s};
+    if (fk) {
+        cudaEventRecord(fk->fork, s);
+        for (int k = 0; k < 5; ++k) cudaStreamWaitEvent(fk->side[k], fk->fork, 0);
+        sf[1] = fk->side[0];
+        sf[2] = fk->side[1];
+        se[0] = fk->side[2];
+        se[1] = fk->side[3];
+        se[2] = fk->side[4];
+    }
+    if (energy) {
+        // energy-only kernels (FP64 in both modes), their own tickets
+        const PassArgs a = pass_args(ch, ff, g, x, t, true, lam_set, es, fs, ps);
+        launch_kernels<double, true, false>(a, g, prec, se[0], se[1], se[2]);
+    }
     if (force) {
+        // the zero fill, then the force-only kernels side by side
+        const PassArgs a = pass_args(ch, ff, g, x, t, false, lam_set, es, fs, ps_forces);
         const int n3 = 3 * ch.n_pos;
         int zb = (n3 / 2 + kZeroThreads - 1) / kZeroThreads;
         zb = zb < 1 ? 1 : (zb > 148 * 8 ? 148 * 8 : zb);
         if (n3 > 0) k_pass_zero<<<zb, kZeroThreads, 0, s>>>(*t, n3);
-    }
-    cudaStream_t sb = s, se = s;
-    if (fk) {
-        cudaEventRecord(fk->fork, s);
-        cudaStreamWaitEvent(fk->side[0], fk->fork, 0);
-        cudaStreamWaitEvent(fk->side[1], fk->fork, 0);
-        sb = fk->side[0];
-        se = fk->side[1];
-    }
-    const bool mixed = prec == MEDYAN_PREC_MIXED;
-    if (energy && force) {
-        if (mixed) launch_kernels<float, true, true>(a, g, prec, s, sb, se);
-        else launch_kernels<double, true, true>(a, g, prec, s, sb, se);
-    } else if (force) {
-        if (mixed) launch_kernels<float, false, true>(a, g, prec, s, sb, se);
-        else launch_kernels<double, false, true>(a, g, prec, s, sb, se);
-    } else {
-        launch_kernels<double, true, false>(a, g, prec, s, sb, se);
+        if (fk) {
+            cudaEventRecord(fk->mid, s);
+            cudaStreamWaitEvent(sf[1], fk->mid, 0);
+            cudaStreamWaitEvent(sf[2], fk->mid, 0);
+        }
+        if (mixed) launch_kernels<float, false, true>(a, g, prec, sf[0], sf[1], sf[2]);
+        else launch_kernels<double, false, true>(a, g, prec, sf[0], sf[1], sf[2]);
     }
     if (fk) {
-        for (int k = 0; k < 2; ++k) {
+        for (int k = 0; k < 5; ++k) {
             cudaEventRecord(fk->join[k], fk->side[k]);
             cudaStreamWaitEvent(s, fk->join[k], 0);
         }

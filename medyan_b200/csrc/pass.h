@@ -28,6 +28,7 @@ struct PassGeometry {
     int nch;            // chain blocks of the main kernel (threads/32 warp tiles of 30 beads each)
     int nb_main;        // bonded blocks of the main kernel (segments 0-3 and 5)
     int main_blocks, branch_blocks, excl_blocks;
+    int main_blocks_forces;  // main kernel grid of a force-only pass
     int rows;           // energy rows = blocks of all three kernels
     int groups;         // rows / kPassGroup, rounded up
 };
@@ -59,10 +60,12 @@ PassGeometry pass_geometry(const ChainDev& ch, const DeviceFF& ff);
 // Energy (energy = true) and/or forces (t set) of a single network's force
 // fields at t's positions (x when t is null or t->d is null). The energy lands
 // in es.out; the forces in target_force(*t), overwritten. Single networks
-// only (ff.act == null). With fk the three kernels run on parallel branches.
+// only (ff.act == null). Energies and forces are separate sets of kernels
+// with their own tickets (ps, ps_forces); with fk all of them run on parallel
+// branches.
 void launch_pass_fused(const ChainDev& ch, const DeviceFF& ff, int prec, const double* x, const ForceTarget* t,
                        bool energy, const LambdaSet* lam_set, const EnergyScratch& es, const ForceScratch& fs,
-                       const PassScratch& ps, cudaStream_t s, const Fork* fk);
+                       const PassScratch& ps, const PassScratch& ps_forces, cudaStream_t s, const Fork* fk);
 
 // Fills pass.cu's quadrature grids, once per device (the current one); call
 // before any stream capture.

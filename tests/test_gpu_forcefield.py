@@ -36,7 +36,7 @@ def check(ff_e, ff_per, ff_f, ref_e, ref_per, ref_f, tol, name=""):
         assert err <= tol, (name, err)
 
 
-def gpu_eval(sv, x, precision="fp64", layout=1):
+def gpu_eval(sv, x, precision="fp64", layout=0):
     with ForceFieldManager(precision) as ff:
         ff.vectorize_all_force_fields(sv)
         ff.set_shapes(pass_layout=layout)
@@ -63,7 +63,7 @@ def network_system(nets, tag):
     return SystemView(int(nets[f"{tag}/n_beads"][0]), **arrays), nets[f"{tag}/coord"]
 
 
-# pass layouts: 0 fused kernels, 1 one kernel per potential group (the default)
+# pass layouts: 0 fused kernels (the default), 1 one kernel per potential group
 LAYOUTS = [0, 1]
 
 
@@ -199,12 +199,13 @@ def test_pass_kernel_count(gpu_lib, nets):
         L, h = ff.lib, ff.handle
         ne, nf, nb = (L.medyan_mech_pass_kernel_count(h, w) for w in range(3))
         assert L.medyan_mech_pass_kernel_count(h, 3) == -1
-        assert ne > 0 and nf > 0 and nb == ne + nf
-        # fused layout: the energy pass is the main, branch and
-        # excluded-volume kernels; the force and evaluate passes add the zero fill
-        ff.set_shapes(pass_layout=0)
+        # fused layout (default): the energy pass is the main, branch and
+        # excluded-volume kernels; the force pass adds the zero fill; the
+        # evaluate pass runs both sets side by side
+        assert (ne, nf, nb) == (3, 4, 7)
+        ff.set_shapes(pass_layout=1)
         ne, nf, nb = (L.medyan_mech_pass_kernel_count(h, w) for w in range(3))
-        assert (ne, nf, nb) == (3, 4, 4)
+        assert ne > 0 and nf > 0 and nb == ne + nf
         # building the graphs for the count does not disturb evaluation
         e, per, f = ff.evaluate(x)
         assert np.isfinite(e)
