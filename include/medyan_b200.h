@@ -375,28 +375,37 @@ medyan_status medyan_mech_get_excl_volume(medyan_mech* h, int32_t* beads_out, do
    to every interaction's parameters, at the handle's coordinates, analytic
    and in FP64. With v != NULL (double[3*n_beads], caller's bead order) the
    outputs are instead the derivatives of those gradients along v,
-   d/de [dE/dtheta](x + e v) = v . d2E/(dx dtheta), by a centred difference
-   (step 1e-5 nm in the max-norm of v) — the mixed term an implicit adjoint
-   needs. Outputs are double[n] in the force field's interaction order (the
+   d/de [dE/dtheta](x + e v) = v . d2E/(dx dtheta), in forward mode (the
+   gradient formulas on dual numbers carrying v: exact to rounding) — the
+   mixed term an implicit adjoint needs. Outputs are double[n] in the force field's interaction order (the
    order given at vectorization; for excluded volume and boundary rebuilt on
    the device, the order of medyan_mech_get_excl_volume); either may be NULL.
      MEDYAN_FF_FILAMENT_STRETCHING, _LINKER_STRETCHING, _MOTOR_STRETCHING:
          d_k = dE/dk,      d_p = dE/dl0
      MEDYAN_FF_FILAMENT_BENDING:     d_k = dE/dk,   d_p = dE/dtheta0
+     MEDYAN_FF_BRANCHING_STRETCHING: d_k = dE/dk,   d_p = dE/dl0
+     MEDYAN_FF_BRANCHING_BENDING:    d_k = dE/dk,   d_p = dE/dtheta0
+     MEDYAN_FF_BRANCHING_DIHEDRAL, _BRANCHING_POSITION: d_k = dE/dk; d_p = 0
+                                     (the four branching slots: one entry per
+                                     branch point; zero when that potential is
+                                     off in branch_ff_mask)
      MEDYAN_FF_EXCLUDED_VOLUME:      d_k = dE/dkRS with kRS = krep*L1*L2
                                      (multiply by L1*L2 for dE/dkrep); d_p = 0
      MEDYAN_FF_BOUNDARY:             d_k = dE/dk,   d_p = dE/dscreen_length
    n must equal the force field's interaction count (else
-   MEDYAN_ERR_CAPACITY); the branching slots return MEDYAN_ERR_UNSUPPORTED. */
+   MEDYAN_ERR_CAPACITY). */
 medyan_status medyan_mech_param_grad(medyan_mech* h, int32_t ff, const double* v, double* d_k, double* d_p,
                                      int64_t n);
 
 /* Hessian-vector product hv = (d2E/dx2) v at the handle's coordinates
-   (double[3*n_beads], caller's bead order): a centred difference of the
-   analytic forces along v, -(F(x + e v) - F(x - e v)) / (2 e) with e = 1e-5 nm
-   in the max-norm of v; both sides run through the force kernels with the
-   move applied on the fly. Use an FP64 handle (a mixed handle differences
-   float forces). */
+   (double[3*n_beads], caller's bead order), in forward mode: every force
+   formula of the force pass evaluated on dual numbers carrying v (positions
+   x + e v), hv = -dF/de, exact to rounding and in FP64 whatever the handle's
+   precision. It replaces the reference's finite-difference Hessian columns
+   (ForceFieldManager::computeHessian, ForceFieldManager.cpp:354-489) for
+   products. An excluded-volume pair that the analytic formula rejects (the
+   quadrature fallback's pairs) has no forward-mode derivative: the call
+   returns MEDYAN_ERR_NONFINITE. */
 medyan_status medyan_mech_hvp(medyan_mech* h, const double* v, double* hv);
 
 /* ---- launch shapes and the autotuner (no counterpart in the reference,

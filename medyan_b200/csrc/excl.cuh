@@ -7,6 +7,7 @@
 #pragma once
 
 #include "device_math.cuh"
+#include "dual.cuh"
 
 namespace mb {
 
@@ -21,11 +22,13 @@ template <>
 __device__ __forceinline__ double atan_r<double>(double x) { return atan(x); }
 template <>
 __device__ __forceinline__ float atan_r<float>(float x) { return atanf(x); }
+template <>
+__device__ __forceinline__ Dual atan_r<Dual>(Dual x) { return atan(x); }
 
 // Scalars of the analytic integral, :360-410 / :643-690. Inputs are the four
 // bead positions; all differences are formed in FP64.
-template <class R>
-__device__ __forceinline__ void excl_scalars(const V3& c1, const V3& c2, const V3& c3, const V3& c4, ExclS<R>& s) {
+template <class R, class P3 = V3>
+__device__ __forceinline__ void excl_scalars(const P3& c1, const P3& c2, const P3& c3, const P3& c4, ExclS<R>& s) {
     T3<R> r12 = diff<R>(c1, c2);  // c2 - c1
     T3<R> r34 = diff<R>(c3, c4);  // c4 - c3
     T3<R> r31 = diff<R>(c3, c1);  // c1 - c3
@@ -76,13 +79,16 @@ __device__ __forceinline__ void excl_scalars(const V3& c1, const V3& c2, const V
 }
 
 // Analytic pair energy (:355 and :393-435). kRS = krep*L1*L2.
-template <class R>
-__device__ __forceinline__ double excl_energy(const V3& c1, const V3& c2, const V3& c3, const V3& c4, double kRS) {
+template <class R, class P3 = V3>
+__device__ __forceinline__ R excl_energy_r(const P3& c1, const P3& c2, const P3& c3, const P3& c4, double kRS) {
     ExclS<R> s;
-    excl_scalars<R>(c1, c2, c3, c4, s);
-    R U = R(0.5) * R(kRS) / s.JJ *
-          (s.CC / s.AA * s.ATG1 + s.GG / s.EE * s.ATG2 + s.DD / s.BB * s.ATG3 + s.HH / s.FF * s.ATG4);
-    return double(U);
+    excl_scalars<R, P3>(c1, c2, c3, c4, s);
+    return R(0.5) * R(kRS) / s.JJ *
+           (s.CC / s.AA * s.ATG1 + s.GG / s.EE * s.ATG2 + s.DD / s.BB * s.ATG3 + s.HH / s.FF * s.ATG4);
+}
+template <class R, class P3 = V3>
+__device__ __forceinline__ double excl_energy(const P3& c1, const P3& c2, const P3& c3, const P3& c4, double kRS) {
+    return double(excl_energy_r<R, P3>(c1, c2, c3, c4, kRS));
 }
 
 // The reference accepts an energy unless it is +-inf, NaN or below -1 (:447-449).
@@ -114,6 +120,18 @@ __device__ __forceinline__ V3 move_bead2_out_of_plane(const V3& p1, const V3& p2
     n[1] = n[1] / m;
     n[2] = n[2] / m;
     return V3{p2.x + n[0] * d, p2.y + n[1] * d, p2.z + n[2] * d};
+}
+// Dual positions: the in-plane test on the values, the move on the duals.
+__device__ __forceinline__ V3 value3(const DV3& p) { return V3{p.x.v, p.y.v, p.z.v}; }
+__device__ __forceinline__ bool in_plane(const DV3& p1, const DV3& p2, const DV3& p3, const DV3& p4) {
+    return in_plane(value3(p1), value3(p2), value3(p3), value3(p4));
+}
+__device__ __forceinline__ DV3 move_bead2_out_of_plane(const DV3& p1, const DV3& p2, const DV3& p3, double d) {
+    const DV3 v1 = diff<Dual>(p1, p2), v2 = diff<Dual>(p1, p3);
+    DV3 n{v1.y * v2.z - v1.z * v2.y, v1.z * v2.x - v1.x * v2.z, v1.x * v2.y - v1.y * v2.x};
+    const Dual m = sqrt(n.x * n.x + n.y * n.y + n.z * n.z);
+    n = DV3{n.x / m, n.y / m, n.z / m};
+    return DV3{p2.x + n.x * d, p2.y + n.y * d, p2.z + n.z * d};
 }
 
 // checkNaN_INF (MathFunctions.h:1377-1384).
@@ -240,12 +258,12 @@ __device__ __forceinline__ bool excl_force_fast(const V3& c1, V3 c2, const V3& c
 // with any other grouping; the reference's own fast-math build is 1e-9 off).
 // Returns false when any component is non-finite or above 1e15 (the caller
 // then uses the quadrature fallback).
-template <class R>
-__device__ __forceinline__ bool excl_force_exact(const V3& c1, V3 c2, const V3& c3, const V3& c4, double kRS,
+template <class R, class P3 = V3>
+__device__ __forceinline__ bool excl_force_exact(const P3& c1, P3 c2, const P3& c3, const P3& c4, double kRS,
                                            T3<R> (&fo)[4]) {
     if (in_plane(c1, c2, c3, c4)) c2 = move_bead2_out_of_plane(c1, c2, c3, 0.01);
     ExclS<R> S;
-    excl_scalars<R>(c1, c2, c3, c4, S);
+    excl_scalars<R, P3>(c1, c2, c3, c4, S);
     const R a = S.a, b = S.b, c = S.c, d = S.d, e = S.e, F = S.F;
     const R AA = S.AA, BB = S.BB, CC = S.CC, DD = S.DD, EE = S.EE, FF = S.FF, GG = S.GG, HH = S.HH;
     const R JJ = S.JJ, ATG1 = S.ATG1, ATG2 = S.ATG2, ATG3 = S.ATG3, ATG4 = S.ATG4;

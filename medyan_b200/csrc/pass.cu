@@ -46,9 +46,14 @@ constexpr int kWarpOut = 30;  // forces written per warp tile: lanes 1..30 of 32
 constexpr unsigned char kLink = 1, kBend = 2;
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kZeroThreads = 256;
-// 64 registers (80 for energy and forces together): the chain tiles and the
-// linker gathers want occupancy
+// 64 registers (80 for energy and forces together; 48 for the float forces
+// of the mixed mode, which spill a few bytes there): the chain tiles and the
+// linker gathers are latency-bound and want resident warps
 constexpr int kMainBlocksPerSM = 4;
+template <class R, bool E, bool F>
+constexpr int main_blocks_per_sm() {
+    return (E && F) ? kMainBlocksPerSM - 1 : (!E && sizeof(R) == 4 ? kMainBlocksPerSM + 1 : kMainBlocksPerSM);
+}
 constexpr int kExclThreadsMax = 128;
 
 __device__ __forceinline__ V3 shfl_up3(const V3& v) {
@@ -229,7 +234,7 @@ __device__ __forceinline__ void block_done(const PassArgs& a, double (&acc)[NV],
     // the row (thread 0) and any fallback-queue entry (the threads that
     // queued) are visible device-wide before the tickets are taken; the force
     // additions need no fence: the finishing block only adds to them
-    if (queued || threadIdx.x == 0) __threadfence();
+    if (queued || (E && threadIdx.x == 0)) __threadfence();
     __syncthreads();
     const int g = row / kGroup;
     if (threadIdx.x == 0) {
@@ -385,7 +390,7 @@ __device__ __forceinline__ void bonded_record(const DeviceFF& ff, const ForceTar
 // leftover stretch, leftover bend, linker, motor, boundary). A fixed grid
 // walks them, so each block's energy row covers a fixed set of units.
 template <class R, bool E, bool F>
-__global__ void __launch_bounds__(kPassThreads, (E && F) ? kMainBlocksPerSM - 1 : kMainBlocksPerSM)
+__global__ void __launch_bounds__(kPassThreads, main_blocks_per_sm<R, E, F>())
     k_pass_main(const __grid_constant__ PassArgs a) {
     if (F && a.t.skip && *a.t.skip) return;
     double* __restrict__ f = F ? target_force(a.t) : nullptr;

@@ -4,9 +4,15 @@
 // function evaluates the reference's expressions in the reference's order.
 //
 // Forces are returned per bead (caller accumulates); energies as double.
+//
+// The position type P3 is V3 (FP64 coordinates) everywhere but in the
+// directional derivatives (diff.cu), which pass DV3 positions with R = Dual
+// (dual.cuh): the same formulas then also return their derivative along the
+// direction the positions carry.
 #pragma once
 
 #include "device_math.cuh"
+#include "dual.cuh"
 
 namespace mb {
 
@@ -34,18 +40,24 @@ __device__ __forceinline__ LenDev<float> length_dev<float>(double dx, double dy,
     float dev = float(d2 - l0 * l0) / (dist + float(l0));
     return LenDev<float>{dist, dev};
 }
+// Dual differences (directional derivatives): the FP64 form.
+template <class R>
+__device__ __forceinline__ LenDev<R> length_dev(const Dual& dx, const Dual& dy, const Dual& dz, double l0) {
+    const Dual dist = sqrt(dx * dx + dy * dy + dz * dz);
+    return LenDev<R>{dist, dist - l0};
+}
 
 // ---------------------------------------------------------------------------
 // FilamentStretchingHarmonic, Filament/FilamentStretchingHarmonic.cpp:185-275.
 // ---------------------------------------------------------------------------
-template <class R>
-__device__ __forceinline__ double stretch_energy(const V3& c1, const V3& c2, double k, double l0) {
+template <class R, class P3 = V3>
+__device__ __forceinline__ double stretch_energy(const P3& c1, const P3& c2, double k, double l0) {
     LenDev<R> L = length_dev<R>(c2.x - c1.x, c2.y - c1.y, c2.z - c1.z, l0);
     return double(R(0.5) * R(k) * L.dev * L.dev);
 }
 // Force on c2 (c1 receives the negative).
-template <class R>
-__device__ __forceinline__ T3<R> stretch_force(const V3& c1, const V3& c2, double k, double l0) {
+template <class R, class P3 = V3>
+__device__ __forceinline__ T3<R> stretch_force(const P3& c1, const P3& c2, double k, double l0) {
     LenDev<R> L = length_dev<R>(c2.x - c1.x, c2.y - c1.y, c2.z - c1.z, l0);
     R invL = R(1) / L.dist;
     R f0 = R(k) * L.dev * invL;
@@ -122,20 +134,20 @@ __device__ __forceinline__ void bend_force(const T3<R>& r1, const T3<R>& r2, dou
 // MotorGhostStretchingHarmonic (MotorGhost/...Harmonic.cpp:234-345): a spring
 // between points at fractions p1, p2 along two cylinders. Midpoints in FP64.
 // ---------------------------------------------------------------------------
-template <class R>
-__device__ __forceinline__ double spring_energy(const V3& c1, const V3& c2, const V3& c3, const V3& c4, double k,
+template <class R, class P3 = V3>
+__device__ __forceinline__ double spring_energy(const P3& c1, const P3& c2, const P3& c3, const P3& c4, double k,
                                                 double l0, double p1, double p2) {
-    V3 v1 = midpoint(c1, c2, p1);
-    V3 v2 = midpoint(c3, c4, p2);
+    P3 v1 = midpoint(c1, c2, p1);
+    P3 v2 = midpoint(c3, c4, p2);
     LenDev<R> L = length_dev<R>(v2.x - v1.x, v2.y - v1.y, v2.z - v1.z, l0);
     return double(R(0.5) * R(k) * L.dev * L.dev);
 }
 // Returns Fl; bead forces are -Fl(1-p1), -Fl p1, Fl(1-p2), Fl p2.
-template <class R>
-__device__ __forceinline__ T3<R> spring_force(const V3& c1, const V3& c2, const V3& c3, const V3& c4, double k,
+template <class R, class P3 = V3>
+__device__ __forceinline__ T3<R> spring_force(const P3& c1, const P3& c2, const P3& c3, const P3& c4, double k,
                                               double l0, double p1, double p2) {
-    V3 v1 = midpoint(c1, c2, p1);
-    V3 v2 = midpoint(c3, c4, p2);
+    P3 v1 = midpoint(c1, c2, p1);
+    P3 v2 = midpoint(c3, c4, p2);
     LenDev<R> L = length_dev<R>(v2.x - v1.x, v2.y - v1.y, v2.z - v1.z, l0);
     R invL = R(1) / L.dist;
     R f0 = R(k) * L.dev * invL;
@@ -146,18 +158,18 @@ __device__ __forceinline__ T3<R> spring_force(const V3& c1, const V3& c2, const 
 // ---------------------------------------------------------------------------
 // BranchingStretchingHarmonic, Branching/BranchingStretchingHarmonic.cpp:195-266.
 // ---------------------------------------------------------------------------
-template <class R>
-__device__ __forceinline__ double branch_stretch_energy(const V3& c1, const V3& c2, const V3& c3, double k, double l0,
+template <class R, class P3 = V3>
+__device__ __forceinline__ double branch_stretch_energy(const P3& c1, const P3& c2, const P3& c3, double k, double l0,
                                                         double pos) {
-    V3 v1 = midpoint(c1, c2, pos);
+    P3 v1 = midpoint(c1, c2, pos);
     LenDev<R> L = length_dev<R>(c3.x - v1.x, c3.y - v1.y, c3.z - v1.z, l0);
     return double(R(0.5) * R(k) * L.dev * L.dev);
 }
 // Returns g = f0*r1; bead forces are -g(pos-1), g pos, -g.
-template <class R>
-__device__ __forceinline__ T3<R> branch_stretch_force(const V3& c1, const V3& c2, const V3& c3, double k, double l0,
+template <class R, class P3 = V3>
+__device__ __forceinline__ T3<R> branch_stretch_force(const P3& c1, const P3& c2, const P3& c3, double k, double l0,
                                                       double pos) {
-    V3 v1 = midpoint(c1, c2, pos);
+    P3 v1 = midpoint(c1, c2, pos);
     LenDev<R> L = length_dev<R>(c3.x - v1.x, c3.y - v1.y, c3.z - v1.z, l0);
     R invL = R(1) / L.dist;
     R f0 = R(k) * L.dev * invL;
@@ -166,10 +178,11 @@ __device__ __forceinline__ T3<R> branch_stretch_force(const V3& c1, const V3& c2
 }
 
 // Virtual plus end for a branch at pos == 1 (Branching/BranchingDihedralCosine.cpp:236-243).
-__device__ __forceinline__ double virtual_plus_end(const V3& c1, V3& c2, double pos) {
+template <class P3>
+__device__ __forceinline__ double virtual_plus_end(const P3& c1, P3& c2, double pos) {
     if (are_equal(pos, 1.0)) {
         const double position = 0.5;
-        c2 = V3{(1 / position) * (c2.x - (1 - position) * c1.x), (1 / position) * (c2.y - (1 - position) * c1.y),
+        c2 = P3{(1 / position) * (c2.x - (1 - position) * c1.x), (1 / position) * (c2.y - (1 - position) * c1.y),
                 (1 / position) * (c2.z - (1 - position) * c1.z)};
         return position;
     }
@@ -179,11 +192,11 @@ __device__ __forceinline__ double virtual_plus_end(const V3& c1, V3& c2, double 
 // ---------------------------------------------------------------------------
 // BranchingDihedralCosine::energy, BranchingDihedralCosine.cpp:211-263.
 // ---------------------------------------------------------------------------
-template <class R>
-__device__ __forceinline__ double branch_dihedral_energy(const V3& c1, V3 c2, const V3& c3, const V3& c4, double k,
-                                                         double pos) {
+template <class R, class P3 = V3>
+__device__ __forceinline__ R branch_dihedral_energy_r(const P3& c1, P3 c2, const P3& c3, const P3& c4, double k,
+                                                      double pos) {
     double position = virtual_plus_end(c1, c2, pos);
-    V3 mp = midpoint(c1, c2, position);
+    P3 mp = midpoint(c1, c2, position);
     // vectorProduct(n1, mp, c2, mp, c3) and vectorProduct(n2, c3, c4, mp, c3).
     T3<R> a = diff<R>(mp, c2), b = diff<R>(mp, c3), c = diff<R>(c3, c4);
     T3<R> n1{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
@@ -192,15 +205,20 @@ __device__ __forceinline__ double branch_dihedral_energy(const V3& c1, V3 c2, co
     R m2 = sqrt(n2.x * n2.x + n2.y * n2.y + n2.z * n2.z);
     n1 = T3<R>{n1.x / m1, n1.y / m1, n1.z / m1};
     n2 = T3<R>{n2.x / m2, n2.y / m2, n2.z / m2};
-    return double(R(k) * (R(1) - dot(n1, n2)));
+    return R(k) * (R(1) - dot(n1, n2));
+}
+template <class R, class P3 = V3>
+__device__ __forceinline__ double branch_dihedral_energy(const P3& c1, const P3& c2, const P3& c3, const P3& c4,
+                                                         double k, double pos) {
+    return double(branch_dihedral_energy_r<R, P3>(c1, c2, c3, c4, k, pos));
 }
 
 // BranchingDihedralCosine::forces (LAMMPS form), BranchingDihedralCosine.cpp:268-490.
-template <class R>
-__device__ __forceinline__ void branch_dihedral_force(const V3& c1, V3 c2, const V3& c3, const V3& c4, double k,
+template <class R, class P3 = V3>
+__device__ __forceinline__ void branch_dihedral_force(const P3& c1, P3 c2, const P3& c3, const P3& c4, double k,
                                                       double pos, T3<R>& L1, T3<R>& L2, T3<R>& L3, T3<R>& L4) {
     double position = virtual_plus_end(c1, c2, pos);
-    V3 mp = midpoint(c1, c2, position);
+    P3 mp = midpoint(c1, c2, position);
     T3<R> vb1 = diff<R>(mp, c2), vb2 = diff<R>(mp, c3), vb3 = diff<R>(c3, c4);
     R vb2xm = -vb2.x, vb2ym = -vb2.y, vb2zm = -vb2.z;
     R ax = vb1.y * vb2zm - vb1.z * vb2ym;
@@ -255,10 +273,10 @@ __device__ __forceinline__ void branch_dihedral_force(const V3& c1, V3 c2, const
 // ---------------------------------------------------------------------------
 // BranchingPositionCosine, Branching/BranchingPositionCosine.cpp:190-440.
 // ---------------------------------------------------------------------------
-template <class R>
-__device__ __forceinline__ double branch_position_energy(const V3& c1, V3 c2, const V3& c3, double k, double pos) {
+template <class R, class P3 = V3>
+__device__ __forceinline__ R branch_position_energy_r(const P3& c1, P3 c2, const P3& c3, double k, double pos) {
     double position = virtual_plus_end(c1, c2, pos);
-    V3 mp = midpoint(c1, c2, position);
+    P3 mp = midpoint(c1, c2, position);
     T3<R> a = diff<R>(mp, c2), b = diff<R>(mp, c3);
     R X = sqrt(dot(a, a));
     R D = sqrt(dot(b, b));
@@ -275,13 +293,18 @@ __device__ __forceinline__ double branch_position_energy(const V3& c1, V3 c2, co
     const double posheta = 0.5 * M_PI;
     R sinp = sqrt(stdmax<R>((R(1) - cosp * cosp), R(0)));
     R cospmq = cosp * R(cos(posheta)) + sinp * R(sin(posheta));
-    return double(R(k) * (R(1) - cospmq));
+    return R(k) * (R(1) - cospmq);
 }
-template <class R>
-__device__ __forceinline__ void branch_position_force(const V3& c1, V3 c2, const V3& c3, double k, double pos,
+template <class R, class P3 = V3>
+__device__ __forceinline__ double branch_position_energy(const P3& c1, const P3& c2, const P3& c3, double k,
+                                                         double pos) {
+    return double(branch_position_energy_r<R, P3>(c1, c2, c3, k, pos));
+}
+template <class R, class P3 = V3>
+__device__ __forceinline__ void branch_position_force(const P3& c1, P3 c2, const P3& c3, double k, double pos,
                                                       T3<R>& F1, T3<R>& F2, T3<R>& F3) {
     double position = virtual_plus_end(c1, c2, pos);
-    V3 mp = midpoint(c1, c2, position);
+    P3 mp = midpoint(c1, c2, position);
     T3<R> r1 = diff<R>(mp, c2), r2 = diff<R>(mp, c3);
     R Xsq = dot(r1, r1);
     R Dsq = dot(r2, r2);
@@ -323,15 +346,18 @@ __device__ __forceinline__ void branch_position_force(const V3& c1, V3 c2, const
 __device__ __forceinline__ double plane_distance(const double4& pl, const V3& p) {
     return (pl.x * p.x + pl.y * p.y + pl.z * p.z + pl.w) / sqrt(pl.x * pl.x + pl.y * pl.y + pl.z * pl.z);
 }
-template <class R>
-__device__ __forceinline__ double boundary_energy(const double4& pl, const V3& p, double k, double slen) {
-    double r = plane_distance(pl, p);
+__device__ __forceinline__ Dual plane_distance(const double4& pl, const DV3& p) {
+    return (pl.x * p.x + pl.y * p.y + pl.z * p.z + pl.w) / sqrt(pl.x * pl.x + pl.y * pl.y + pl.z * pl.z);
+}
+template <class R, class P3 = V3>
+__device__ __forceinline__ double boundary_energy(const double4& pl, const P3& p, double k, double slen) {
+    const auto r = plane_distance(pl, p);
     R Rr = R(-r / slen);
     return double(R(k) * exp(Rr));
 }
-template <class R>
-__device__ __forceinline__ R boundary_force_mag(const double4& pl, const V3& p, double k, double slen) {
-    double r = plane_distance(pl, p);
+template <class R, class P3 = V3>
+__device__ __forceinline__ R boundary_force_mag(const double4& pl, const P3& p, double k, double slen) {
+    const auto r = plane_distance(pl, p);
     R Rr = R(-r / slen);
     return R(k) * exp(Rr) / R(slen);
 }
