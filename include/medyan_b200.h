@@ -163,6 +163,14 @@ medyan_status medyan_mech_create(const medyan_system* sys, int32_t precision, me
 /* Replace every force field's arrays after a new vectorization (same handle,
    same bead count). Device buffers grow when needed; none are freed. */
 medyan_status medyan_mech_update(medyan_mech* h, const medyan_system* sys);
+/* Create and update pack the force-field records on the device: the
+   caller's arrays are copied as they are and kernels remap the bead offsets
+   to the library's internal bead order, assign links and bends to filament
+   chains and pack the parameters (the per-record work of the reference's
+   ForceField::vectorize calls, ForceFieldManager.cpp:35-93). With on = 1 the
+   next updates pack with host loops instead: the same records bit for bit,
+   kept to check the device packing against. */
+medyan_status medyan_mech_set_host_packing(medyan_mech* h, int32_t on);
 
 medyan_status medyan_mech_destroy(medyan_mech* h);
 

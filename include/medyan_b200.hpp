@@ -74,7 +74,7 @@ struct ConjugateGradientParams {
     ConjugateGradientDescentSearch descentSearchMethod = ConjugateGradientDescentSearch::polakRibiere;
     double maxDist = 1.0;
     double lambdaMax = 0.01;
-    double lambdaRunningAverageProbability = 0.0;  // only 0 is supported
+    double lambdaRunningAverageProbability = 0.0;  // accepted in [0, 1]; no effect, as in the reference
     std::string lineSearchAlgorithm = "BACKTRACKING";  // BACKTRACKING, or QUADRATIC (any other value, as in the reference)
     double gradTol = 1e-1;
     double energyRelTol = 1e-9;
@@ -255,6 +255,23 @@ public:
         return s;
     }
 
+    // Bitwise reproducible force sums (fixed point; medyan_mech_set_deterministic).
+    void setDeterministic(bool on) { check(medyan_mech_set_deterministic(handle(), on ? 1 : 0), "setDeterministic"); }
+
+    // Many evaluations back to back with the copies overlapped
+    // (medyan_mech_evaluate_async): results land in force[i] and energy[i]
+    // (MEDYAN_FF_COUNT + 1 each) by the time the call returns; page-locked
+    // buffers overlap, pageable ones work.
+    void evaluateMany(const std::vector<const double*>& coord, const std::vector<double*>& force,
+                      const std::vector<double*>& energy) {
+        if (coord.size() != force.size() || coord.size() != energy.size())
+            throw Error(MEDYAN_ERR_INVALID_ARG, "evaluateMany: sizes");
+        for (size_t i = 0; i < coord.size(); ++i)
+            check(medyan_mech_evaluate_async(handle(), coord[i], force[i], energy[i]), "evaluateMany");
+        const medyan_status st = medyan_mech_wait(handle());
+        if (st != MEDYAN_OK && st != MEDYAN_ERR_NONFINITE) check(st, "evaluateMany");
+    }
+
     int numBeads() const { return n_beads_; }
     medyan_mech* handle() const {
         if (!h_) throw Error(MEDYAN_ERR_INVALID_ARG, "vectorizeAllForceFields was not called");
@@ -275,8 +292,14 @@ class CGMethod {
 public:
     static MinimizationResult minimize(const ConjugateGradientParams& p, std::vector<double>& coord,
                                        ForceFieldManager& ffm, std::vector<double>* outForce = nullptr) {
-        if (p.lambdaRunningAverageProbability != 0.0)
-            throw Error(MEDYAN_ERR_UNSUPPORTED, "CGMethod::minimize: running-average lambda");
+        // lambdaRunningAverageProbability changes nothing in the reference:
+        // CGMethod::minimize builds a new LambdaRunningAverageManager in every
+        // iteration (CGMethod.hpp:1316-1317) and records one lambda into it,
+        // and the manager acts only after ten records (LineSearch.hpp:33-42).
+        // Any probability therefore gives the trajectory of 0 (checked on the
+        // reference's compiled CGMethod in tests/test_oracle_pins.py).
+        if (!(p.lambdaRunningAverageProbability >= 0.0 && p.lambdaRunningAverageProbability <= 1.0))
+            throw Error(MEDYAN_ERR_INVALID_ARG, "CGMethod::minimize: lambdaRunningAverageProbability");
         if ((int)coord.size() != 3 * ffm.numBeads()) throw Error(MEDYAN_ERR_INVALID_ARG, "CGMethod::minimize: coord");
         medyan_cg_params cp{};
         cp.method = p.descentSearchMethod == ConjugateGradientDescentSearch::steepest         ? MEDYAN_CG_STEEPEST

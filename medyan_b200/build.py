@@ -19,7 +19,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libmedyan_b200.so")
 
-SOURCES = ["capi.cu", "ff_kernels.cu", "chain.cu", "excl_kernels.cu", "nl.cu", "cg.cu", "batch.cu", "pbatch.cu", "diff.cu", "hessian.cu", "aux.cu", "tune.cu", "noalloc.cu", "pass.cu", "async.cu"]
+SOURCES = ["capi.cu", "ff_kernels.cu", "chain.cu", "excl_kernels.cu", "nl.cu", "cg.cu", "batch.cu", "pbatch.cu", "diff.cu", "hessian.cu", "aux.cu", "tune.cu", "noalloc.cu", "pass.cu", "async.cu", "vectorize.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + os.path.join(ROOT, "include"),
           "-I" + CSRC, "--expt-relaxed-constexpr", "--fmad=false"]
@@ -40,20 +40,32 @@ def _stale(out: str, deps: list[str]) -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build(verbose: bool = False, force: bool = False) -> str:
+def build(verbose: bool = False, force: bool = False, jobs: int | None = None) -> str:
+    """Compiles the stale translation units (in parallel, one nvcc per core)
+    and links the library."""
+    from concurrent.futures import ThreadPoolExecutor
     os.makedirs(BUILD, exist_ok=True)
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
     headers.append(os.path.join(ROOT, "include", "medyan_b200.h"))
-    objs = []
+    objs, cmds = [], []
     for src in SOURCES:
         path = os.path.join(CSRC, src)
         obj = os.path.join(BUILD, src.replace(".cu", ".o"))
         objs.append(obj)
         if force or _stale(obj, [path, *headers, __file__]):
-            cmd = [nvcc(), *ARCH, *COMMON, *PER_FILE.get(src, []), "-c", path, "-o", obj]
-            if verbose:
-                print(" ".join(cmd), flush=True)
-            subprocess.run(cmd, check=True)
+            cmds.append([nvcc(), *ARCH, *COMMON, *PER_FILE.get(src, []), "-c", path, "-o", obj])
+
+    def run(cmd: list[str]) -> None:
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+
+    if cmds:
+        # the longest translation units first
+        cmds.sort(key=lambda c: -os.path.getsize(c[-3]))
+        with ThreadPoolExecutor(max_workers=jobs or min(len(cmds), os.cpu_count() or 1)) as pool:
+            for fut in [pool.submit(run, c) for c in cmds]:
+                fut.result()
     if force or _stale(LIB, objs):
         cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
         if verbose:

@@ -83,7 +83,10 @@ medyan_status validate_system(const medyan_system* s) {
     return MEDYAN_OK;
 }
 
-// Packs the vectorization into the device records of DeviceFF.
+// Packs the vectorization into the device records of DeviceFF with host
+// loops: the same records as upload_system_device (vectorize.cu), which
+// create and update use; kept as the reference for it
+// (medyan_mech_set_host_packing).
 medyan_status upload_system(medyan_mech* h, const medyan_system* s) {
     cudaStream_t st = h->stream;
     std::vector<int2> i2;
@@ -93,7 +96,10 @@ medyan_status upload_system(medyan_mech* h, const medyan_system* s) {
     std::vector<double> d1;
     std::vector<int> ii, pl;
     DeviceFF& ff = h->ff;
+    const int bonded_block = ff.bonded_block, excl_block = ff.excl_block;  // launch shapes survive an update
     ff = DeviceFF{};
+    ff.bonded_block = bonded_block;
+    ff.excl_block = excl_block;
     ff.n_beads = s->n_beads;
     cudaError_t e = cudaSuccess;
 #define UPLOAD(buf, vec)                                                              \
@@ -497,7 +503,7 @@ medyan_status medyan_mech_create(const medyan_system* sys, int32_t precision, me
     h->prec = precision;
     h->n_beads = sys->n_beads;
     medyan_status st = h->init();
-    if (st == MEDYAN_OK) st = upload_system(h, sys);
+    if (st == MEDYAN_OK) st = upload_system_device(h, sys);
     if (st == MEDYAN_OK) st = sync_status(h);
     if (st != MEDYAN_OK) {
         delete h;
@@ -511,9 +517,15 @@ medyan_status medyan_mech_update(medyan_mech* h, const medyan_system* sys) {
     if (!h || !sys || sys->n_beads != h->n_beads) return MEDYAN_ERR_INVALID_ARG;
     medyan_status v = validate_system(sys);
     if (v != MEDYAN_OK) return v;
-    medyan_status st = upload_system(h, sys);
+    medyan_status st = h->host_packing ? upload_system(h, sys) : upload_system_device(h, sys);
     if (st != MEDYAN_OK) return st;
     return sync_status(h);
+}
+
+medyan_status medyan_mech_set_host_packing(medyan_mech* h, int32_t on) {
+    if (!h || (on != 0 && on != 1)) return MEDYAN_ERR_INVALID_ARG;
+    h->host_packing = on;
+    return MEDYAN_OK;
 }
 
 medyan_status medyan_mech_destroy(medyan_mech* h) {

@@ -162,6 +162,9 @@ struct medyan_mech {
     std::vector<int> order_host, pos_host;
     bool identity_order = true;
     mb::DevBuf<int> order;       // device copy of order_host (empty when identity)
+    mb::DevBuf<int> pos_dev;     // device copy of pos_host (device packing)
+    mb::DevBuf<unsigned char> vec_stage;  // the caller's arrays during device packing
+    int host_packing = 0;        // 1: the next update packs records with the host loops
     mb::DevBuf<double> stage;    // 3*n_beads staging for reordered transfers
 
     // filament chains (chain.cu)
@@ -231,6 +234,7 @@ namespace mb {
 medyan_status cuda_status(cudaError_t e);
 medyan_status validate_system(const medyan_system* s);
 medyan_status upload_system(medyan_mech* h, const medyan_system* s);
+medyan_status upload_system_device(medyan_mech* h, const medyan_system* s);
 medyan_status refresh_device_ff(medyan_mech* h);
 medyan_status sync_status(medyan_mech* h);
 void enqueue_energy(medyan_mech* h, const double* x, const double* d, const LambdaSet* lam, cudaStream_t s);

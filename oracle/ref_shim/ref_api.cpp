@@ -182,6 +182,14 @@ void medyan_ref_prepared_forces(void* h, const double* coord, double* force) {
 // moveAlongDirectionLimitingBeadMove_ (src/Controller/MController.h:273-339)
 // for a bead-only system: step = min over all coordinates of
 // maxDist/|dir_i|, then coord += step*dir over the DOF.
+// ConjugateGradientParams::lambdaRunningAverageProbability of the next
+// medyan_ref_cg_minimize calls (0 unless set), to exercise the reference's
+// LambdaRunningAverageManager (Mechanics/Minimizer/LineSearch.hpp:21-48).
+static double g_lambda_avg_probability = 0.0;
+extern "C" void medyan_ref_set_lambda_running_average(double probability) {
+    g_lambda_avg_probability = probability;
+}
+
 int medyan_ref_cg_minimize(const medyan_system* sys, const medyan_cg_params* p, double* coord_io,
                            double* force_out, medyan_min_result* out) {
     RefSystem r(sys);
@@ -202,6 +210,7 @@ int medyan_ref_cg_minimize(const medyan_system* sys, const medyan_cg_params* p, 
     cg.tryToRecoverInLineSearchError = p->try_to_recover != 0;
     cg.lineSearchAlgorithm = p->line_search ? "QUADRATIC" : "BACKTRACKING";
     cg.reportOnCallLimit = true;
+    cg.lambdaRunningAverageProbability = g_lambda_avg_probability;
 
     const auto energyFunc = [&](floatingpoint* c) {
         double e[MEDYAN_FF_COUNT];

@@ -287,16 +287,27 @@ int run_gpu() {
         CHECK(rel(ffm2.computeEnergy(xg.data()), oracle_energy(&s, xg.data(), nullptr)) <= 1e-12);
     }
 
-    // an unsupported option is refused, not approximated
-    ConjugateGradientParams q = p;
-    q.lambdaRunningAverageProbability = 0.5;
-    threw = false;
-    try {
-        CGMethod::minimize(q, xg, ffm2);
-    } catch (const Error& e) {
-        threw = e.status == MEDYAN_ERR_UNSUPPORTED;
+    // lambdaRunningAverageProbability: no effect in the reference (the manager
+    // is rebuilt every iteration), so a run with 0.5 is the run with 0; a value
+    // outside [0, 1] is refused
+    {
+        ffm2.setDeterministic(true);
+        ConjugateGradientParams q = p;
+        std::vector<double> xa = xg, xb = xg;
+        const MinimizationResult ra = CGMethod::minimize(q, xa, ffm2);
+        q.lambdaRunningAverageProbability = 0.5;
+        const MinimizationResult rb = CGMethod::minimize(q, xb, ffm2);
+        CHECK(ra.numIter == rb.numIter && ra.numEnergyCall == rb.numEnergyCall && xa == xb);
+        q.lambdaRunningAverageProbability = 2.0;
+        threw = false;
+        try {
+            CGMethod::minimize(q, xg, ffm2);
+        } catch (const Error& e) {
+            threw = e.status == MEDYAN_ERR_INVALID_ARG;
+        }
+        CHECK(threw);
+        ffm2.setDeterministic(false);
     }
-    CHECK(threw);
     std::printf("adaptor ok: E=%.10g, %lld pairs, %d CG iterations\n", eg, (long long)ne, r.numIter);
     return 0;
 }

@@ -239,3 +239,36 @@ def test_quadratic_reference_defect(oracle, unit):
     st2, x2, f2, r2 = run_cb(Reference(strict=True).lib, "medyan_ref_cg_minimize_cb", cg["n"], p, init, cbs)
     assert st == 0 and r.error_flags == 0
     assert r2.error_flags & 1  # errorLineSearch
+
+
+@pytest.mark.skipif(not Reference.available(strict=True), reason="reference build not present")
+def test_lambda_running_average_is_a_no_op(oracle):
+    """ConjugateGradientParams::lambdaRunningAverageProbability. CGMethod::minimize
+    creates a new LambdaRunningAverageManager in every iteration
+    (Mechanics/Minimizer/CGMethod.hpp:1316-1317) and the line search records
+    into it once (CGMethod.hpp:363-366); the manager's status, which alone
+    lets it cap lambda, changes only when its tenth record arrives
+    (LineSearch.hpp:33-42), so it never does, and no random number is drawn.
+    Any probability gives the trajectory of 0: checked here on the
+    reference's own compiled CGMethod with probability 1."""
+    import ctypes as C
+    from medyan_b200.forcefield import conjugate_gradient_params as cgp
+    from medyan_b200.network import make_workload
+    ref = Reference(strict=True)
+    ref.lib.medyan_ref_set_lambda_running_average.argtypes = [C.c_double]
+    ref.lib.medyan_ref_set_lambda_running_average.restype = None
+    net = make_workload(0, n_fil=12, cyl_per_fil=6, box=700.0, n_linker=16, seed=3)
+    st, extra = oracle.complete(net)
+    sv, x = net.system_view(**extra), net.flat_coords()
+    p = cgp(grad_tol=1.0)
+    runs = []
+    for prob in (0.0, 1.0):
+        ref.lib.medyan_ref_set_lambda_running_average(prob)
+        runs.append(ref.minimize(sv, x, p))
+    ref.lib.medyan_ref_set_lambda_running_average(0.0)
+    (s0, x0, f0, r0), (s1, x1, f1, r1) = runs
+    assert s0 == s1
+    assert (r0.num_iter, r0.num_energy_call, r0.num_force_call) == (r1.num_iter, r1.num_energy_call, r1.num_force_call)
+    # the reference reports no iteration count; one force call per iteration
+    assert r0.num_force_call > 10  # enough line searches that a persistent manager would have acted
+    assert np.array_equal(x0, x1) and r0.energy_after_total == r1.energy_after_total
