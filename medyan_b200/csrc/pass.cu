@@ -46,13 +46,13 @@ constexpr int kWarpOut = 30;  // forces written per warp tile: lanes 1..30 of 32
 constexpr unsigned char kLink = 1, kBend = 2;
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kZeroThreads = 256;
-// 64 registers (80 for energy and forces together; 48 for the float forces
-// of the mixed mode, which spill a few bytes there): the chain tiles and the
-// linker gathers are latency-bound and want resident warps
-constexpr int kMainBlocksPerSM = 4;
-template <class R, bool E, bool F>
+// Resident blocks of the main kernel per SM: 80 registers a thread, room
+// for a chain tile's loads in flight beside the one being computed
+constexpr int kMainBlocksPerSM = 3;
+constexpr int kTilesPerWarp = 4;  // chain tiles per warp in a force-only pass's chain unit
+template <class R, bool E, bool F, bool LS>
 constexpr int main_blocks_per_sm() {
-    return (E && F) ? kMainBlocksPerSM - 1 : (!E && sizeof(R) == 4 ? kMainBlocksPerSM + 1 : kMainBlocksPerSM);
+    return kMainBlocksPerSM;
 }
 constexpr int kExclThreadsMax = 128;
 
@@ -274,30 +274,67 @@ __device__ __forceinline__ void block_done(const PassArgs& a, double (&acc)[NV],
 // One warp tile of the chains: lanes hold centres q = 30w-1 .. 30w+30; the
 // link (q, q+1) and the bend centred at q are evaluated once, and lanes
 // 1..30 add the five terms acting on their bead and own their link's and
-// bend's energy.
-template <class R, bool E, bool F>
-__device__ __forceinline__ void chain_tile(const PassArgs& a, const Pos& P, double* __restrict__ f, int w,
-                                           double (&acc)[4]) {
+// bend's energy. A tile is fetched (loads only) one tile ahead of its
+// computation, so a warp's loads for its next tile are in flight while it
+// computes the current one.
+template <bool LS>
+struct ChainRaw;
+template <>
+struct ChainRaw<false> {
+    V3 c, e;  // the centre's position; lanes 0 and 31: the halo position (q-1, q+1)
+    double2 lp, bp;
+    unsigned fl;
+};
+template <>
+struct ChainRaw<true> {  // positions x + lam*d: x and d of the centre and the halo
+    V3 c, e, cd, ed;
+    double2 lp, bp;
+    unsigned fl;
+};
+
+template <bool LS>
+__device__ __forceinline__ void chain_fetch(const PassArgs& a, const Pos& P, int w, ChainRaw<LS>& r) {
     const ChainDev& ch = a.ch;
     const int n = ch.n_pos;
     const int lane = threadIdx.x & 31;
     const int q = w * kWarpOut - 1 + lane;
     const bool in = q >= 0 && q < n;
     const int qe = lane == 0 ? q - 1 : q + 1;  // the halo position of lanes 0 and 31
-    V3 c{0.0, 0.0, 0.0}, ce{0.0, 0.0, 0.0};
-    if (in) c = P(3 * q);
-    if ((lane == 0 || lane == 31) && qe >= 0 && qe < n) ce = P(3 * qe);
-    const unsigned char fl = in ? ch.flags[q] : 0;
-    const double2 lp = in ? ch.link_p[q] : double2{0.0, 0.0};
-    const double2 bp = in ? ch.bend_p[q] : double2{0.0, 0.0};
+    const bool halo = (lane == 0 || lane == 31) && qe >= 0 && qe < n;
+    r.c = r.e = V3{0.0, 0.0, 0.0};
+    if (in) r.c = load3(P.x + 3 * q);
+    if (halo) r.e = load3(P.x + 3 * qe);
+    if constexpr (LS) {
+        r.cd = r.ed = V3{0.0, 0.0, 0.0};
+        if (in) r.cd = load3(P.d + 3 * q);
+        if (halo) r.ed = load3(P.d + 3 * qe);
+    }
+    r.fl = in ? ch.flags[q] : 0u;
+    r.lp = in ? ch.link_p[q] : double2{0.0, 0.0};
+    r.bp = in ? ch.bend_p[q] : double2{0.0, 0.0};
+}
+
+template <class R, bool E, bool F, bool LS>
+__device__ __forceinline__ void chain_compute(const PassArgs& a, const Pos& P, double* __restrict__ f, int w,
+                                              const ChainRaw<LS>& r, double (&acc)[kMainVals]) {
+    const int n = a.ch.n_pos;
+    const int lane = threadIdx.x & 31;
+    const int q = w * kWarpOut - 1 + lane;
+    const bool in = q >= 0 && q < n;
+    V3 c = r.c, ce = r.e;
+    if constexpr (LS) {
+        c = move3(r.c, P.lam, r.cd);
+        ce = move3(r.e, P.lam, r.ed);
+    }
+    const unsigned fl = r.fl;
     V3 cprev = shfl_up3(c), cnext = shfl_down3(c);
     if (lane == 0) cprev = ce;
     if (lane == 31) cnext = ce;
     const bool own = lane >= 1 && lane <= kWarpOut && in;
     if constexpr (F) {
         T3<R> Fl{0, 0, 0}, A{0, 0, 0}, B{0, 0, 0};
-        if (fl & kLink) Fl = stretch_force<R>(c, cnext, lp.x, lp.y);
-        if (fl & kBend) bend_force<R>(diff<R>(cprev, c), diff<R>(c, cnext), bp.x, bp.y, A, B);
+        if (fl & kLink) Fl = stretch_force<R>(c, cnext, r.lp.x, r.lp.y);
+        if (fl & kBend) bend_force<R>(diff<R>(cprev, c), diff<R>(c, cnext), r.bp.x, r.bp.y, A, B);
         const T3<R> Fp = shfl_up3(Fl), Bp = shfl_up3(B), An = shfl_down3(A);
         if (own) {
             // link (q-1, q) acts on q; link (q, q+1) reacts on q; bends centred
@@ -310,8 +347,8 @@ __device__ __forceinline__ void chain_tile(const PassArgs& a, const Pos& P, doub
     }
     if constexpr (E) {
         if (own) {
-            if (fl & kLink) acc[0] += stretch_energy<double>(c, cnext, lp.x, lp.y);
-            if (fl & kBend) acc[1] += bend_energy<double>(diff<double>(cprev, c), diff<double>(c, cnext), bp.x, bp.y);
+            if (fl & kLink) acc[0] += stretch_energy<double>(c, cnext, r.lp.x, r.lp.y);
+            if (fl & kBend) acc[1] += bend_energy<double>(diff<double>(cprev, c), diff<double>(c, cnext), r.bp.x, r.bp.y);
         }
     }
 }
@@ -385,39 +422,70 @@ __device__ __forceinline__ void bonded_record(const DeviceFF& ff, const ForceTar
     }
 }
 
-// Units of the main kernel: [0, nch) chain units (one warp tile per warp),
-// then bonded chunks of blockDim records (a.seg[k] is the first chunk of
-// leftover stretch, leftover bend, linker, motor, boundary). A fixed grid
-// walks them, so each block's energy row covers a fixed set of units.
+// Bonded chunk b of the main kernel: blockDim records of one segment.
 template <class R, bool E, bool F>
-__global__ void __launch_bounds__(kPassThreads, main_blocks_per_sm<R, E, F>())
+__device__ __forceinline__ void main_chunk(const PassArgs& a, const Pos& P, double* __restrict__ f, int b,
+                                           double (&acc)[kMainVals]) {
+    int k = 0;
+#pragma unroll
+    for (int j = 1; j < 5; ++j) k += b >= a.seg[j] ? 1 : 0;
+    const int i = (b - a.seg[k]) * blockDim.x + threadIdx.x;
+    double e[4] = {0.0, 0.0, 0.0, 0.0};
+    bonded_record<R, E, F>(a.ff, a.t, P, f, k == 4 ? 5 : k, i, e);
+    // acc: 0 stretching, 1 bending, 2 linker, 3 motor, 4 boundary
+#pragma unroll
+    for (int j = 0; j < kMainVals; ++j)
+        if (j == k) acc[j] += e[0];
+}
+
+// The main kernel's grid is resident (a few blocks per SM) and walks its
+// work in two phases: the chain tiles, one warp per tile with the next tile
+// fetched while the current one is computed, then the bonded chunks of
+// blockDim records (a.seg[k] is the first chunk of leftover stretch,
+// leftover bend, linker, motor, boundary). In an energy pass both walks are
+// fixed by the grid, so each block's energy row covers a fixed set of tiles
+// and chunks and the sums are reproducible; a force-only pass takes its
+// tiles and chunks from work counters instead.
+template <class R, bool E, bool F, bool LS>
+__global__ void __launch_bounds__(kPassThreads, main_blocks_per_sm<R, E, F, LS>())
     k_pass_main(const __grid_constant__ PassArgs a) {
     if (F && a.t.skip && *a.t.skip) return;
     double* __restrict__ f = F ? target_force(a.t) : nullptr;
     const Pos P = pos_of(a);
     double acc[kMainVals] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    const DeviceFF& ff = a.ff;
-    const int units = a.nch + a.nb_main;
-    for (int u = blockIdx.x; u < units; u += gridDim.x) {
+    const int tiles = (a.ch.n_pos + kWarpOut - 1) / kWarpOut;
+    if constexpr (F && !E) {
+        // force-only passes: one unit per block, so the hardware hands units
+        // to SMs as they free up (the pass's other kernels hold some SMs at
+        // first). Units [0, a.nch) are chain units, kTilesPerWarp consecutive
+        // tiles per warp, each fetched while the one before is computed;
+        // then one bonded chunk per unit.
+        const int u = blockIdx.x;
         if (u < a.nch) {
-            const int w = u * (blockDim.x >> 5) + (threadIdx.x >> 5);
-            double ca[4] = {0.0, 0.0, 0.0, 0.0};
-            if ((long long)w * kWarpOut < a.ch.n_pos) chain_tile<R, E, F>(a, P, f, w, ca);
-            acc[0] += ca[0];
-            acc[1] += ca[1];
+            const int w0 = (u * (blockDim.x >> 5) + (threadIdx.x >> 5)) * kTilesPerWarp;
+            ChainRaw<LS> cur, nxt;
+            if (w0 < tiles) chain_fetch<LS>(a, P, w0, cur);
+#pragma unroll 1
+            for (int j = 0; j < kTilesPerWarp && w0 + j < tiles; ++j) {
+                const int w = w0 + j;
+                if (j + 1 < kTilesPerWarp && w + 1 < tiles) chain_fetch<LS>(a, P, w + 1, nxt);
+                chain_compute<R, E, F, LS>(a, P, f, w, cur, acc);
+                cur = nxt;
+            }
         } else {
-            const int b = u - a.nch;
-            int k = 0;
-#pragma unroll
-            for (int j = 1; j < 5; ++j) k += b >= a.seg[j] ? 1 : 0;
-            const int i = (b - a.seg[k]) * blockDim.x + threadIdx.x;
-            double e[4] = {0.0, 0.0, 0.0, 0.0};
-            bonded_record<R, E, F>(ff, a.t, P, f, k == 4 ? 5 : k, i, e);
-            // acc: 0 stretching, 1 bending, 2 linker, 3 motor, 4 boundary
-#pragma unroll
-            for (int j = 0; j < kMainVals; ++j)
-                if (j == k) acc[j] += e[0];
+            main_chunk<R, E, F>(a, P, f, u - a.nch, acc);
         }
+    } else {
+        const int warps = gridDim.x * (blockDim.x >> 5);
+        int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+        ChainRaw<LS> cur, nxt;
+        if (w < tiles) chain_fetch<LS>(a, P, w, cur);
+        for (; w < tiles; w += warps) {
+            if (w + warps < tiles) chain_fetch<LS>(a, P, w + warps, nxt);
+            chain_compute<R, E, F, LS>(a, P, f, w, cur, acc);
+            cur = nxt;
+        }
+        for (int b = blockIdx.x; b < a.nb_main; b += gridDim.x) main_chunk<R, E, F>(a, P, f, b, acc);
     }
     // a force-only pass has no rows here: the main kernel's blocks take no ticket
     if constexpr (E) block_done<0, E, F>(a, acc, a.row_main + blockIdx.x, false);
@@ -551,7 +619,11 @@ void launch_kernels(const PassArgs& a, const PassGeometry& g, int prec, cudaStre
             k_pass_excl<E, F, false><<<g.excl_blocks, g.excl_threads, 0, s_excl>>>(a);
     }
     if (g.branch_blocks > 0) k_pass_branch<R, E, F><<<g.branch_blocks, g.threads, 0, s_branch>>>(a);
-    k_pass_main<R, E, F><<<E ? g.main_blocks : g.main_blocks_forces, g.threads, 0, s_main>>>(a);
+    const int mb = E ? g.main_blocks : g.main_blocks_forces;
+    if (a.t.d)
+        k_pass_main<R, E, F, true><<<mb, g.threads, 0, s_main>>>(a);
+    else
+        k_pass_main<R, E, F, false><<<mb, g.threads, 0, s_main>>>(a);
 }
 
 }  // namespace
@@ -581,10 +653,11 @@ PassGeometry pass_geometry(const ChainDev& ch, const DeviceFF& ff) {
     const int eb = (ff.n_excl + g.excl_threads - 1) / g.excl_threads;
     const int ecap = g_num_sms * 32;
     g.excl_blocks = eb < ecap ? eb : ecap;
-    // a force-only pass: one unit per block (its main and branch blocks take
-    // no ticket, so a block's end holds nothing up)
-    const int fcap = g_num_sms * 64;
-    g.main_blocks_forces = units < 1 ? 1 : (units < fcap ? units : fcap);
+    // a force-only pass: one unit per block, chain units of kTilesPerWarp
+    // tiles per warp
+    g.nch_forces = (tiles + warps * kTilesPerWarp - 1) / (warps * kTilesPerWarp);
+    const int funits = g.nch_forces + g.nb_main;
+    g.main_blocks_forces = funits < 1 ? 1 : funits;
     g.rows = g.main_blocks + g.branch_blocks + g.excl_blocks;
     g.groups = (g.rows + kGroup - 1) / kGroup;
     return g;
@@ -612,7 +685,7 @@ PassArgs pass_args(const ChainDev& ch, const DeviceFF& ff, const PassGeometry& g
     a.row_main = 0;
     a.row_branch = g.main_blocks;
     a.row_excl = energy ? g.main_blocks + g.branch_blocks : 0;
-    a.nch = g.nch;
+    a.nch = energy ? g.nch : g.nch_forces;
     a.nb_main = g.nb_main;
     for (int k = 0; k < 6; ++k) a.seg[k] = g.seg[k];
     a.out = es.out;

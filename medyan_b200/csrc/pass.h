@@ -28,7 +28,8 @@ struct PassGeometry {
     int nch;            // chain blocks of the main kernel (threads/32 warp tiles of 30 beads each)
     int nb_main;        // bonded blocks of the main kernel (segments 0-3 and 5)
     int main_blocks, branch_blocks, excl_blocks;
-    int main_blocks_forces;  // main kernel grid of a force-only pass
+    int nch_forces;     // chain units of a force-only pass (kTilesPerWarp tiles per warp)
+    int main_blocks_forces;  // main kernel grid of a force-only pass: one unit per block
     int rows;           // energy rows = blocks of all three kernels
     int groups;         // rows / kPassGroup, rounded up
 };
@@ -43,7 +44,7 @@ struct PassArgs {
     unsigned* group_ticket;
     unsigned* ticket;
     int n_rows, n_groups, row_main, row_branch, row_excl;
-    int nch, nb_main;
+    int nch, nb_main;         // chain units (of this pass's kind), bonded chunks
     int seg[6];               // PassGeometry::seg
     double* out;              // [kMaxLambda][MEDYAN_FF_COUNT + 1] energies
     const LambdaSet* lam_set; // result copied to slots [0, K) (null: slot 0)
