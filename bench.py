@@ -199,7 +199,9 @@ def run_ours(args, rank: int, world: int) -> dict:
             for i in range(K):
                 flush.zero_()
                 ev[i][0].record(stream)
+                torch.cuda.nvtx.range_push("evaluate_step")
                 step()
+                torch.cuda.nvtx.range_pop()
                 ev[i][1].record(stream)
         L.medyan_mech_synchronize(h)
         torch.cuda.synchronize()
@@ -211,15 +213,21 @@ def run_ours(args, rank: int, world: int) -> dict:
         L.medyan_mech_enqueue_energy(h)
     L.medyan_mech_synchronize(h)
     evp = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(K)]
+    # NVTX ranges name the passes for a profiler (ncu --nvtx --nvtx-include "force_pass/")
+    nvtx = torch.cuda.nvtx
     with torch.cuda.stream(stream):
         for i in range(K):
             flush.zero_()
             evp[i][0].record(stream)
+            nvtx.range_push("force_pass")
             L.medyan_mech_enqueue_forces(h)
+            nvtx.range_pop()
             evp[i][1].record(stream)
             flush.zero_()
             evp[i][2].record(stream)
+            nvtx.range_push("energy_pass")
             L.medyan_mech_enqueue_energy(h)
+            nvtx.range_pop()
             evp[i][3].record(stream)
     L.medyan_mech_synchronize(h)
     torch.cuda.synchronize()

@@ -439,7 +439,10 @@ typedef struct medyan_launch_shapes {
                                        volume; energies: the same three kernels
                                        with the row reduction built in), 1 = one
                                        kernel per potential group (chain forces
-                                       first, the rest after) */
+                                       first, the rest after), 2 = fused with
+                                       the filament chains in a kernel of their
+                                       own that stages chain segments through
+                                       shared memory by bulk copies */
 } medyan_launch_shapes;
 
 /* The defaults are 256, 64, 256, 4, 0. Setting shapes re-derives the block

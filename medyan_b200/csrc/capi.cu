@@ -275,11 +275,14 @@ medyan_status refresh_device_ff(medyan_mech* h) {
     {
         // fused-pass scratch; the group tickets start at zero (stream-ordered
         // after every pass already enqueued on the handle's stream)
-        const PassGeometry pg = pass_geometry(h->chain, ff);
-        if (e == cudaSuccess) e = h->pass_rows.reserve((size_t)pg.rows * MEDYAN_FF_COUNT);
-        if (e == cudaSuccess) e = h->pass_group_rows.reserve((size_t)pg.groups * MEDYAN_FF_COUNT);
-        if (e == cudaSuccess) e = h->pass_group_ticket.reserve((size_t)pg.groups);
-        if (e == cudaSuccess) e = h->pass_fgroup_ticket.reserve((size_t)pg.groups);
+        // (sized for both fused layouts, so a change of layout needs no reallocation)
+        const PassGeometry pg = pass_geometry(h->chain, ff, false), ps = pass_geometry(h->chain, ff, true);
+        const int rows = pg.rows > ps.rows ? pg.rows : ps.rows;
+        const int groups = pg.groups > ps.groups ? pg.groups : ps.groups;
+        if (e == cudaSuccess) e = h->pass_rows.reserve((size_t)rows * MEDYAN_FF_COUNT);
+        if (e == cudaSuccess) e = h->pass_group_rows.reserve((size_t)groups * MEDYAN_FF_COUNT);
+        if (e == cudaSuccess) e = h->pass_group_ticket.reserve((size_t)groups);
+        if (e == cudaSuccess) e = h->pass_fgroup_ticket.reserve((size_t)groups);
         if (e == cudaSuccess)
             e = cudaMemsetAsync(h->pass_group_ticket.raw(), 0, sizeof(unsigned int) * h->pass_group_ticket.cap,
                                 h->stream);
@@ -312,9 +315,9 @@ void enqueue_forces(medyan_mech* h, const double* x, double* f, cudaStream_t s) 
 
 void enqueue_force_target(medyan_mech* h, const double* x, const ForceTarget& t, const ForceScratch& fs,
                           cudaStream_t s) {
-    if (h->pass_layout == 0)
+    if (h->pass_layout == 0 || h->pass_layout == 2)
         launch_pass_fused(h->chain, h->ff, h->prec, x, &t, false, nullptr, h->es, fs, h->pass_scratch(),
-                          h->pass_scratch_forces(), s, &h->fork);
+                          h->pass_scratch_forces(), s, &h->fork, h->pass_layout == 2);
     else
         launch_forces(h->chain, h->ff, h->prec, x, t, fs, s, &h->fork);
 }
@@ -362,10 +365,10 @@ cudaError_t ensure_pass_graph(medyan_mech* h, int which) {
     cudaError_t e = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return e;
     const ForceTarget t{h->f.raw(), nullptr, nullptr, nullptr, nullptr, nullptr, h->deterministic, h->fs.status};
-    if (h->pass_layout == 0)
+    if (h->pass_layout == 0 || h->pass_layout == 2)
         launch_pass_fused(h->chain, h->ff, h->prec, h->x.raw(), which == kPassEnergy ? nullptr : &t,
                           which != kPassForces, h->lam_zero.raw(), h->es, h->fs, h->pass_scratch(),
-                          h->pass_scratch_forces(), h->stream, &h->fork);
+                          h->pass_scratch_forces(), h->stream, &h->fork, h->pass_layout == 2);
     else if (which == kPassBoth)
         launch_evaluate(h->chain, h->ff, h->prec, h->x.raw(), nullptr, h->lam_zero.raw(), t, h->es, h->fs, h->stream,
                         &h->fork);

@@ -371,12 +371,14 @@ __device__ __forceinline__ void block_reduce3(double& a, double& b, double& m, d
     __syncthreads();
 }
 
-// Returns true in exactly one block: the last to finish (sums then visible).
+// Returns true in exactly one block: the last to finish. Each block's
+// partials are stored by its thread 0, whose acquire-release ticket publishes
+// them; the last block's threads see every block's partials after the
+// barrier that follows its ticket.
 __device__ __forceinline__ bool last_block(unsigned int* ticket) {
     __shared__ bool last;
-    __threadfence();
     __syncthreads();
-    if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    if (threadIdx.x == 0) last = ticket_add(ticket, 1u) == gridDim.x - 1;
     __syncthreads();
     return last;
 }

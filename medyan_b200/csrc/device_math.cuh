@@ -68,6 +68,23 @@ __device__ __forceinline__ void red_add(double* p, double v) {
     asm volatile("red.global.add.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");
 }
 
+// Arrival tickets of the last-block-done reductions. A block publishes what
+// its thread 0 wrote (a row of partial sums) and learns whether it is the
+// last to arrive with one acquire-release atomic: the release orders the
+// thread's earlier stores before the increment, and the acquire makes every
+// earlier arriver's stores visible to the last one (and, after a block
+// barrier, to its other threads). A sequentially consistent __threadfence()
+// per block costs several microseconds when the memory system is busy, and
+// the finishing block of a pass used to wait on four of them in a row.
+__device__ __forceinline__ unsigned ticket_add(unsigned* p, unsigned v) {
+    unsigned old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+// Release fence for stores of threads other than the one taking the ticket
+// (made before the block barrier that precedes the ticket).
+__device__ __forceinline__ void fence_release() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+
 // Accumulate an R-valued force into the FP64 force array.
 template <class R>
 __device__ __forceinline__ void add_force(double* __restrict__ f, int off, R fx, R fy, R fz) {

@@ -251,13 +251,12 @@ __global__ void __launch_bounds__(kSplitFinishThreads) k_energy_finish(
         finish_rows(ff, partial + (size_t)k * total_blocks * 4, r_lo, r_hi, nch, nbb, wsum, dst);
     }
     if (G > 1) {
-        // last-block-done: publish this block's shares, take a ticket
-        __threadfence();
+        // last-block-done: this block's shares (thread 0's stores) are
+        // published by thread 0's acquire-release ticket
         __syncthreads();
-        if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == (unsigned)G - 1;
+        if (threadIdx.x == 0) last = ticket_add(ticket, 1u) == (unsigned)G - 1;
         __syncthreads();
         if (!last) return;
-        __threadfence();
         if (threadIdx.x < K * MEDYAN_FF_COUNT) {
             const int k = threadIdx.x / MEDYAN_FF_COUNT, slot = threadIdx.x % MEDYAN_FF_COUNT;
             double v = 0.0;

@@ -144,7 +144,7 @@ struct medyan_mech {
     mb::EnergyScratch es{};
     mb::ForceScratch fs{};
     // fused passes (pass.cu): layout choice, energy rows and arrival ticket
-    int pass_layout = 0;                  // 0 fused, 1 one kernel per potential group
+    int pass_layout = 0;                  // 0 fused, 1 one kernel per potential group, 2 fused with streamed chain
     int deterministic = 0;                // 1: fixed-point force sums (ForceTarget::fixed)
     // energy side; the force side has its own tickets (its rows are unused)
     mb::DevBuf<double> pass_rows, pass_group_rows;

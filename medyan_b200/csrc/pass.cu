@@ -122,18 +122,30 @@ __device__ __noinline__ void pass_finish(const PassArgs& a) {
     __shared__ int nfb;
     const Pos P = pos_of(a);
     if constexpr (E) {
-        if (threadIdx.x < 32) {
+        __shared__ int n_queued, bad0;
+        // the queue length and status are fetched while the group rows load
+        if (threadIdx.x == 0) {
+            n_queued = __ldcg(a.e_fb_count);
+            bad0 = __ldcg(a.e_bad);
+        }
+        // warp w sums slots w, w + nwarp, ...: every warp's loads are in
+        // flight at once (ten slots one after another were ten L2 round
+        // trips in a row). Per slot the lanes add their groups in group
+        // order and the warp tree is fixed, whichever warp does it.
+        {
             const int ng = (a.n_rows + kGroup - 1) / kGroup;
-            for (int s = 0; s < kSlots; ++s) {
+            const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
+            for (int s = warp; s < kSlots; s += nwarp) {
                 double v = 0.0;
-                for (int g = threadIdx.x; g < ng; g += 32) v += __ldcg(a.group_rows + (size_t)s * a.n_groups + g);
+                for (int g = lane; g < ng; g += 32) v += __ldcg(a.group_rows + (size_t)s * a.n_groups + g);
                 v = warp_tree(v);
-                if (threadIdx.x == 0) sums[s] = v;
+                if (lane == 0) sums[s] = v;
             }
         }
+        __syncthreads();
         if (threadIdx.x == 0) {
             // queued pairs in pair order (the queue fills in arrival order)
-            const int n = min(__ldcg(a.e_fb_count), kFallbackCap);
+            const int n = min(n_queued, kFallbackCap);
             for (int i = 1; i < n; ++i) {
                 const int2 q = __ldcg(a.e_fb_list + i);
                 int j = i - 1;
@@ -164,7 +176,8 @@ __device__ __noinline__ void pass_finish(const PassArgs& a) {
             double tot = 0.0;
             bool inf = false;
             v[MEDYAN_FF_EXCLUDED_VOLUME] += fbE;
-            if (__ldcg(a.e_bad)) v[MEDYAN_FF_EXCLUDED_VOLUME] = -1.0;
+            // the fallbacks may have flagged a pair: read the status again then
+            if (nfb > 0 ? __ldcg(a.e_bad) : bad0) v[MEDYAN_FF_EXCLUDED_VOLUME] = -1.0;
 #pragma unroll
             for (int s = 0; s < kSlots; ++s) {
                 if (v[s] <= -1) inf = true;
@@ -231,19 +244,19 @@ __device__ __forceinline__ void block_done(const PassArgs& a, double (&acc)[NV],
             }
         }
     }
-    // the row (thread 0) and any fallback-queue entry (the threads that
-    // queued) are visible device-wide before the tickets are taken; the force
-    // additions need no fence: the finishing block only adds to them
-    if (queued || (E && threadIdx.x == 0)) __threadfence();
+    // the row (thread 0's stores) is published by thread 0's ticket; a
+    // fallback-queue entry (stored by the thread that queued it) by that
+    // thread's release fence before the barrier. The force additions need no
+    // ordering: the finishing block only adds to them
+    if (queued) fence_release();
     __syncthreads();
     const int g = row / kGroup;
     if (threadIdx.x == 0) {
         const int gsize = min(kGroup, a.n_rows - kGroup * g);
-        state = atomicAdd(a.group_ticket + g, 1u) == (unsigned)gsize - 1 ? 1 : 0;
+        state = ticket_add(a.group_ticket + g, 1u) == (unsigned)gsize - 1 ? 1 : 0;
     }
     __syncthreads();
     if (state == 0) return;
-    __threadfence();
     if constexpr (E) {
         if (threadIdx.x < 32) {
             const int r = kGroup * g + threadIdx.x;
@@ -259,14 +272,13 @@ __device__ __forceinline__ void block_done(const PassArgs& a, double (&acc)[NV],
         }
     }
     if (threadIdx.x == 0) {
+        // the group row (thread 0's store) is published by the pass ticket
         a.group_ticket[g] = 0u;
-        __threadfence();
         const int ng = (a.n_rows + kGroup - 1) / kGroup;
-        state = atomicAdd(a.ticket, 1u) == (unsigned)ng - 1 ? 2 : 1;
+        state = ticket_add(a.ticket, 1u) == (unsigned)ng - 1 ? 2 : 1;
     }
     __syncthreads();
     if (state != 2) return;
-    __threadfence();
     pass_finish<E, F>(a);
 }
 
@@ -453,7 +465,8 @@ __global__ void __launch_bounds__(kPassThreads, main_blocks_per_sm<R, E, F, LS>(
     double* __restrict__ f = F ? target_force(a.t) : nullptr;
     const Pos P = pos_of(a);
     double acc[kMainVals] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    const int tiles = (a.ch.n_pos + kWarpOut - 1) / kWarpOut;
+    // no chain units: the chain runs in the streamed chain kernel
+    const int tiles = a.nch > 0 ? (a.ch.n_pos + kWarpOut - 1) / kWarpOut : 0;
     if constexpr (F && !E) {
         // force-only passes: one unit per block, so the hardware hands units
         // to SMs as they free up (the pass's other kernels hold some SMs at
@@ -489,6 +502,247 @@ __global__ void __launch_bounds__(kPassThreads, main_blocks_per_sm<R, E, F, LS>(
     }
     // a force-only pass has no rows here: the main kernel's blocks take no ticket
     if constexpr (E) block_done<0, E, F>(a, acc, a.row_main + blockIdx.x, false);
+}
+
+// ------------------------------------------------------------ streamed chain
+// Chain segments staged through shared memory (pass layout 2). Segment s
+// covers output positions [s0, s0 + kChainSeg), s0 = s * kChainSeg, as
+// kChainWarps warp tiles of kWarpOut positions (the warp-tile kernel's
+// tiles, lanes holding centres s0 + 30w - 1 + lane). A tile needs the
+// centres s0-1 .. s0+S and the positions s0-2 .. s0+S+1.
+//
+// Warp-specialized pipeline: a producer warp issues bulk copies
+// (cp.async.bulk, completion counted in bytes on the stage's "full"
+// mbarrier) of the next kChainStages segments' coordinates, link and bend
+// parameters and flags, so a block keeps ~55 KB of loads in flight with no
+// registers held for them. Each consumer warp computes its tile from shared
+// memory on its own (neighbours by warp shuffles, no block barrier) and
+// arrives on the stage's "empty" mbarrier; the producer refills a stage once
+// all consumer warps have arrived. Segments whose windows would start before
+// the arrays or run past their ends are filled by the producer warp with
+// plain loads instead.
+constexpr int kChainWarps = kChainThreads / 32;  // consumer warps (one tile each per segment)
+constexpr int kSegPos = kChainSeg + 4;           // positions s0-2 .. s0+S+1
+constexpr int kSegCen = kChainSeg + 2;           // centres s0-1 .. s0+S
+static_assert(kChainSeg == kChainWarps * kWarpOut, "a segment is one tile per consumer warp");
+static_assert(kChainSeg % 2 == 0, "segment starts must keep the coordinate window 16-byte aligned");
+
+template <bool LS>
+struct ChainStage {
+    double x[3 * kSegPos];             // positions s0-2 .. s0+S+1
+    double d[LS ? 3 * kSegPos : 2];    // their search directions (x + lam d passes)
+    double2 lp[kSegCen];               // (k, l0) of centres s0-1 .. s0+S
+    double2 bp[kSegCen];               // (k, theta0) of the same centres
+    unsigned char fl[kChainSeg + 32];  // flags from (s0-1) rounded down to 16 bytes
+};
+
+// Dynamic shared memory of a chain block with `stages` stages.
+template <bool LS>
+constexpr size_t chain_smem_bytes(int stages = kChainStages) {
+    return stages * sizeof(ChainStage<LS>) + 2 * stages * sizeof(unsigned long long);
+}
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+    asm volatile("{ .reg .b64 st; mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1; }" ::"r"(smem_addr(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
+    asm volatile("{ .reg .b64 st; mbarrier.arrive.shared::cta.b64 st, [%0]; }" ::"r"(smem_addr(bar)) : "memory");
+}
+// Waits for the phase of the given parity to complete; gives up after a
+// bounded number of polls (false).
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
+    const unsigned a = smem_addr(bar);
+    for (int i = 0; i < (1 << 20); ++i) {
+        unsigned done;
+        asm volatile(
+            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+// Bulk copy of `bytes` (a multiple of 16, both addresses 16-byte aligned)
+// from global to shared memory, counted on bar.
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
+// The flag window of the segment at s0: first byte and length, and whether
+// all of the segment's windows lie inside the arrays (bulk copies).
+__device__ __forceinline__ int flag_first(int s0) { return (s0 - 1) & ~15; }
+__device__ __forceinline__ int flag_bytes(int s0) { return ((s0 + kChainSeg + 1 - flag_first(s0)) + 15) & ~15; }
+__device__ __forceinline__ bool seg_inside(int s0, int n) {
+    return s0 >= 2 && s0 + kChainSeg + 2 <= n && flag_first(s0) + flag_bytes(s0) <= n;
+}
+
+// Producer warp: loads segment seg into stage st and completes the stage's
+// full barrier, by bulk copies (lane 0) or by plain loads (all lanes; zeros
+// outside the arrays).
+template <bool LS>
+__device__ __forceinline__ void chain_produce(const PassArgs& a, const double* d, bool bulk, int seg,
+                                              ChainStage<LS>& st, unsigned long long* full) {
+    const int n = a.ch.n_pos;
+    const int s0 = seg * kChainSeg;
+    const int lane = threadIdx.x & 31;
+    if (bulk && seg_inside(s0, n)) {
+        if (lane == 0) {
+            // the stage may last have been written through the generic proxy
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            const unsigned bx = 24u * kSegPos, bp = 16u * kSegCen;
+            const int ff = flag_first(s0);
+            const unsigned bf = (unsigned)flag_bytes(s0);
+            mbar_expect_tx(full, bx * (LS ? 2u : 1u) + 2u * bp + bf);
+            bulk_load(st.x, a.x + 3 * (s0 - 2), bx, full);
+            if constexpr (LS) bulk_load(st.d, d + 3 * (s0 - 2), bx, full);
+            bulk_load(st.lp, a.ch.link_p + (s0 - 1), bp, full);
+            bulk_load(st.bp, a.ch.bend_p + (s0 - 1), bp, full);
+            bulk_load(st.fl, a.ch.flags + ff, bf, full);
+        }
+        return;
+    }
+    for (int i = lane; i < 3 * kSegPos; i += 32) {
+        const int q = s0 - 2 + i / 3;
+        const bool in = q >= 0 && q < n;
+        st.x[i] = in ? __ldg(a.x + 3 * (s0 - 2) + i) : 0.0;
+        if constexpr (LS) st.d[i] = in ? __ldg(d + 3 * (s0 - 2) + i) : 0.0;
+    }
+    const int fo = (s0 - 1) - flag_first(s0);
+    for (int j = lane; j < kSegCen; j += 32) {
+        const int c = s0 - 1 + j;
+        const bool in = c >= 0 && c < n;
+        st.lp[j] = in ? a.ch.link_p[c] : double2{0.0, 0.0};
+        st.bp[j] = in ? a.ch.bend_p[c] : double2{0.0, 0.0};
+        st.fl[fo + j] = in ? a.ch.flags[c] : (unsigned char)0;
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(full);  // release: the consumers see the stores
+}
+
+template <bool LS>
+__device__ __forceinline__ V3 stage_pos(const ChainStage<LS>& st, int p, double lam) {
+    const V3 v{st.x[3 * p], st.x[3 * p + 1], st.x[3 * p + 2]};
+    if constexpr (LS) return move3(v, lam, V3{st.d[3 * p], st.d[3 * p + 1], st.d[3 * p + 2]});
+    return v;
+}
+
+// The grid is resident and walks the segments in a fixed order (blockIdx.x,
+// + gridDim.x, ...), so each block's energy row covers a fixed set of
+// centres. Force-only passes take no tickets here.
+template <class R, bool E, bool F, bool LS>
+__global__ void __launch_bounds__(kChainThreads + 32) k_pass_chain(const __grid_constant__ PassArgs a) {
+    if (F && a.t.skip && *a.t.skip) return;
+    extern __shared__ __align__(128) unsigned char chain_smem[];
+    const int K = a.chain_stages;  // stages of the ring (1 when each block takes one segment)
+    ChainStage<LS>* stages = reinterpret_cast<ChainStage<LS>*>(chain_smem);
+    unsigned long long* full = reinterpret_cast<unsigned long long*>(chain_smem + K * sizeof(ChainStage<LS>));
+    unsigned long long* empty = full + K;
+    double* __restrict__ f = F ? target_force(a.t) : nullptr;
+    const double* d = LS ? a.t.d : nullptr;
+    const double lam = LS ? *a.t.lam : 0.0;
+    const int n = a.ch.n_pos;
+    const int nseg = (n + kChainSeg - 1) / kChainSeg;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const bool bulk = aligned16(a.x) && (!LS || aligned16(d)) && aligned16(a.ch.link_p) && aligned16(a.ch.bend_p) &&
+                      aligned16(a.ch.flags);
+    double acc[kMainVals] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < K; ++k) {
+            mbar_init(full + k, 1);
+            mbar_init(empty + k, kChainWarps);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (warp == kChainWarps) {
+        // producer: segment m of this block goes to stage m % K once its
+        // previous occupant (segment m - K) has been consumed
+        int m = 0;
+        bool ok = true;
+        for (int seg = blockIdx.x; seg < nseg; seg += gridDim.x, ++m) {
+            const int k = m % K;
+            if (m >= K) {
+                bool ready = lane == 0 ? mbar_wait(empty + k, ((m / K) - 1) & 1) : true;
+                ready = __shfl_sync(kFull, ready, 0);
+                if (!ready) {
+                    ok = false;
+                    break;
+                }
+            }
+            chain_produce<LS>(a, d, bulk, seg, stages[k], full + k);
+        }
+        if (!ok && lane == 0) {
+            // the consumers stopped: report it and wait (bounded) for the
+            // copies still in flight before the block's shared memory goes
+            if (F) atomicOr(a.f_status, 8);
+            if (E) atomicOr(a.e_bad, 4);
+            for (int q = m - K; q < m; ++q)
+                if (q >= 0) mbar_wait(full + q % K, (q / K) & 1);
+        }
+    } else {
+        int it = 0;
+        for (int seg = blockIdx.x; seg < nseg; seg += gridDim.x, ++it) {
+            const int k = it % K;
+            const ChainStage<LS>& st = stages[k];
+            bool ready = lane == 0 ? mbar_wait(full + k, (it / K) & 1) : true;
+            ready = __shfl_sync(kFull, ready, 0);
+            if (!ready) {
+                if (lane == 0) {
+                    if (F) atomicOr(a.f_status, 8);
+                    if (E) atomicOr(a.e_bad, 4);
+                }
+                break;
+            }
+            const int s0 = seg * kChainSeg;
+            const int j = warp * kWarpOut + lane;  // centre s0 - 1 + j
+            const int q = s0 - 1 + j;
+            const unsigned fl = st.fl[(s0 - 1) - flag_first(s0) + j];
+            const V3 cp = stage_pos<LS>(st, j, lam), c = stage_pos<LS>(st, j + 1, lam),
+                     cn = stage_pos<LS>(st, j + 2, lam);
+            const double2 lp = st.lp[j], bp = st.bp[j];
+            const bool own = lane >= 1 && lane <= kWarpOut && q < n;
+            if constexpr (F) {
+                T3<R> Fl{0, 0, 0}, A{0, 0, 0}, B{0, 0, 0};
+                if (fl & kLink) Fl = stretch_force<R>(c, cn, lp.x, lp.y);
+                if (fl & kBend) bend_force<R>(diff<R>(cp, c), diff<R>(c, cn), bp.x, bp.y, A, B);
+                const T3<R> Fp = shfl_up3(Fl), Bp = shfl_up3(B), An = shfl_down3(A);
+                if (own) {
+                    // link (q-1, q) acts on q; link (q, q+1) reacts on q; bends
+                    // centred at q-1 (third bead), q (middle), q+1 (first bead)
+                    const double fx =
+                        double(Fp.x) - double(Fl.x) + double(Bp.x) + (double(A.x) - double(B.x)) - double(An.x);
+                    const double fy =
+                        double(Fp.y) - double(Fl.y) + double(Bp.y) + (double(A.y) - double(B.y)) - double(An.y);
+                    const double fz =
+                        double(Fp.z) - double(Fl.z) + double(Bp.z) + (double(A.z) - double(B.z)) - double(An.z);
+                    target_add(a.t, f, 3 * q, fx, fy, fz);
+                }
+            }
+            if constexpr (E) {
+                if (own) {
+                    if (fl & kLink) acc[0] += stretch_energy<double>(c, cn, lp.x, lp.y);
+                    if (fl & kBend) acc[1] += bend_energy<double>(diff<double>(cp, c), diff<double>(c, cn), bp.x, bp.y);
+                }
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(empty + k);
+        }
+    }
+    if constexpr (E) block_done<0, E, F>(a, acc, a.row_chain + blockIdx.x, false);
 }
 
 // ------------------------------------------------------------ branch points
@@ -609,7 +863,7 @@ __global__ void __launch_bounds__(kZeroThreads) k_pass_zero(const ForceTarget t,
 
 template <class R, bool E, bool F>
 void launch_kernels(const PassArgs& a, const PassGeometry& g, int prec, cudaStream_t s_main, cudaStream_t s_branch,
-                    cudaStream_t s_excl) {
+                    cudaStream_t s_excl, cudaStream_t s_chain) {
     // the excluded-volume pairs first: their FP64 chains are the longest, and
     // their blocks should be resident before the main kernel's fill the SMs
     if (g.excl_blocks > 0) {
@@ -617,6 +871,14 @@ void launch_kernels(const PassArgs& a, const PassGeometry& g, int prec, cudaStre
             k_pass_excl<E, F, true><<<g.excl_blocks, g.excl_threads, 0, s_excl>>>(a);
         else
             k_pass_excl<E, F, false><<<g.excl_blocks, g.excl_threads, 0, s_excl>>>(a);
+    }
+    if (g.chain_blocks > 0) {
+        if (a.t.d)
+            k_pass_chain<R, E, F, true>
+                <<<g.chain_blocks, kChainThreads + 32, chain_smem_bytes<true>(g.chain_stages), s_chain>>>(a);
+        else
+            k_pass_chain<R, E, F, false>
+                <<<g.chain_blocks, kChainThreads + 32, chain_smem_bytes<false>(g.chain_stages), s_chain>>>(a);
     }
     if (g.branch_blocks > 0) k_pass_branch<R, E, F><<<g.branch_blocks, g.threads, 0, s_branch>>>(a);
     const int mb = E ? g.main_blocks : g.main_blocks_forces;
@@ -626,13 +888,25 @@ void launch_kernels(const PassArgs& a, const PassGeometry& g, int prec, cudaStre
         k_pass_main<R, E, F, false><<<mb, g.threads, 0, s_main>>>(a);
 }
 
+// Opts every chain kernel in to its dynamic shared memory (above the 48 KB
+// default).
+template <class R, bool E, bool F>
+cudaError_t chain_attrs() {
+    cudaError_t e = cudaFuncSetAttribute(k_pass_chain<R, E, F, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)chain_smem_bytes<false>());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_pass_chain<R, E, F, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)chain_smem_bytes<true>());
+    return e;
+}
+
 }  // namespace
 
 namespace {
 int g_num_sms = 148;  // SMs of the device (set at init; B200: 148)
 }  // namespace
 
-PassGeometry pass_geometry(const ChainDev& ch, const DeviceFF& ff) {
+PassGeometry pass_geometry(const ChainDev& ch, const DeviceFF& ff, bool stream) {
     PassGeometry g{};
     g.threads = kPassThreads;
     g.excl_threads = excl_block_of(ff) > 128 ? 128 : excl_block_of(ff);
@@ -658,7 +932,24 @@ PassGeometry pass_geometry(const ChainDev& ch, const DeviceFF& ff) {
     g.nch_forces = (tiles + warps * kTilesPerWarp - 1) / (warps * kTilesPerWarp);
     const int funits = g.nch_forces + g.nb_main;
     g.main_blocks_forces = funits < 1 ? 1 : funits;
-    g.rows = g.main_blocks + g.branch_blocks + g.excl_blocks;
+    g.stream = stream;
+    g.nseg = (ch.n_pos + kChainSeg - 1) / kChainSeg;
+    g.chain_blocks = 0;
+    g.chain_stages = kChainStages;
+    if (stream) {
+        // the chain kernel takes the chain; the main kernel keeps the
+        // records. One unit (chain segment, record chunk) per block and one
+        // energy row per unit: the hardware balances the blocks over the SMs
+        // (resident grids walking fixed unit sets left some SMs busy twice
+        // as long as the average), and the sums still add each unit's row
+        // in a fixed order
+        g.nch = g.nch_forces = 0;
+        g.main_blocks = g.nb_main < 1 ? 1 : g.nb_main;
+        g.main_blocks_forces = g.nb_main < 1 ? 1 : g.nb_main;
+        g.chain_blocks = g.nseg;
+        g.chain_stages = 1;
+    }
+    g.rows = g.main_blocks + g.branch_blocks + g.excl_blocks + g.chain_blocks;
     g.groups = (g.rows + kGroup - 1) / kGroup;
     return g;
 }
@@ -685,6 +976,8 @@ PassArgs pass_args(const ChainDev& ch, const DeviceFF& ff, const PassGeometry& g
     a.row_main = 0;
     a.row_branch = g.main_blocks;
     a.row_excl = energy ? g.main_blocks + g.branch_blocks : 0;
+    a.row_chain = g.main_blocks + g.branch_blocks + g.excl_blocks;  // energy passes only
+    a.chain_stages = g.chain_stages;
     a.nch = energy ? g.nch : g.nch_forces;
     a.nb_main = g.nb_main;
     for (int k = 0; k < 6; ++k) a.seg[k] = g.seg[k];
@@ -703,26 +996,30 @@ PassArgs pass_args(const ChainDev& ch, const DeviceFF& ff, const PassGeometry& g
 
 void launch_pass_fused(const ChainDev& ch, const DeviceFF& ff, int prec, const double* x, const ForceTarget* t,
                        bool energy, const LambdaSet* lam_set, const EnergyScratch& es, const ForceScratch& fs,
-                       const PassScratch& ps, const PassScratch& ps_forces, cudaStream_t s, const Fork* fk) {
-    const PassGeometry g = pass_geometry(ch, ff);
+                       const PassScratch& ps, const PassScratch& ps_forces, cudaStream_t s, const Fork* fk,
+                       bool stream) {
+    const PassGeometry g = pass_geometry(ch, ff, stream);
     const bool force = t != nullptr;
     const bool mixed = prec == MEDYAN_PREC_MIXED;
-    // streams: the force side on s, sides 0-1; the energy side on sides 2-4
-    // (everything on s without a fork)
-    cudaStream_t sf[3] = {s, s, s}, se[3] = {s, s, s};
+    // streams: the force side on s, sides 0-1 (and 5 for a streamed chain);
+    // the energy side on sides 2-4 (and 6) (everything on s without a fork)
+    constexpr int kSides = 7;
+    cudaStream_t sf[4] = {s, s, s, s}, se[4] = {s, s, s, s};
     if (fk) {
         cudaEventRecord(fk->fork, s);
-        for (int k = 0; k < 5; ++k) cudaStreamWaitEvent(fk->side[k], fk->fork, 0);
+        for (int k = 0; k < kSides; ++k) cudaStreamWaitEvent(fk->side[k], fk->fork, 0);
         sf[1] = fk->side[0];
         sf[2] = fk->side[1];
+        sf[3] = fk->side[5];
         se[0] = fk->side[2];
         se[1] = fk->side[3];
         se[2] = fk->side[4];
+        se[3] = fk->side[6];
     }
     if (energy) {
         // energy-only kernels (FP64 in both modes), their own tickets
         const PassArgs a = pass_args(ch, ff, g, x, t, true, lam_set, es, fs, ps);
-        launch_kernels<double, true, false>(a, g, prec, se[0], se[1], se[2]);
+        launch_kernels<double, true, false>(a, g, prec, se[0], se[1], se[2], se[3]);
     }
     if (force) {
         // the zero fill, then the force-only kernels side by side
@@ -735,12 +1032,13 @@ void launch_pass_fused(const ChainDev& ch, const DeviceFF& ff, int prec, const d
             cudaEventRecord(fk->mid, s);
             cudaStreamWaitEvent(sf[1], fk->mid, 0);
             cudaStreamWaitEvent(sf[2], fk->mid, 0);
+            cudaStreamWaitEvent(sf[3], fk->mid, 0);
         }
-        if (mixed) launch_kernels<float, false, true>(a, g, prec, sf[0], sf[1], sf[2]);
-        else launch_kernels<double, false, true>(a, g, prec, sf[0], sf[1], sf[2]);
+        if (mixed) launch_kernels<float, false, true>(a, g, prec, sf[0], sf[1], sf[2], sf[3]);
+        else launch_kernels<double, false, true>(a, g, prec, sf[0], sf[1], sf[2], sf[3]);
     }
     if (fk) {
-        for (int k = 0; k < 5; ++k) {
+        for (int k = 0; k < kSides; ++k) {
             cudaEventRecord(fk->join[k], fk->side[k]);
             cudaStreamWaitEvent(s, fk->join[k], 0);
         }
@@ -761,6 +1059,10 @@ cudaError_t init_pass_kernels() {
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return e;
     if (sms > 0) g_num_sms = sms;
+    e = chain_attrs<double, true, false>();
+    if (e == cudaSuccess) e = chain_attrs<double, false, true>();
+    if (e == cudaSuccess) e = chain_attrs<float, false, true>();
+    if (e != cudaSuccess) return e;
     cudaStream_t s = nullptr;
     e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
     if (e != cudaSuccess) return e;

@@ -30,9 +30,23 @@ struct PassGeometry {
     int main_blocks, branch_blocks, excl_blocks;
     int nch_forces;     // chain units of a force-only pass (kTilesPerWarp tiles per warp)
     int main_blocks_forces;  // main kernel grid of a force-only pass: one unit per block
-    int rows;           // energy rows = blocks of all three kernels
+    int rows;           // energy rows = blocks of all the pass's kernels
     int groups;         // rows / kPassGroup, rounded up
+    // streamed chain (pass layout 2): the chain segments run in their own
+    // kernel (k_pass_chain) and the main kernel keeps the generic records
+    bool stream;
+    int nseg;           // chain segments of kChainSeg positions
+    int chain_blocks;   // grid of the chain kernel (0 without streaming)
+    int chain_stages;   // segments in flight per chain block
 };
+
+// Streamed chain segments: kChainSeg positions per segment (one 30-position
+// warp tile per consumer warp; even, so every segment's coordinate window
+// starts on a 16-byte boundary), kChainStages segments in flight per block;
+// blocks of kChainThreads consumer threads and one producer warp.
+constexpr int kChainThreads = 256;
+constexpr int kChainSeg = (kChainThreads / 32) * 30;
+constexpr int kChainStages = 4;
 
 struct PassArgs {
     ChainDev ch;
@@ -43,8 +57,9 @@ struct PassArgs {
     double* group_rows;
     unsigned* group_ticket;
     unsigned* ticket;
-    int n_rows, n_groups, row_main, row_branch, row_excl;
+    int n_rows, n_groups, row_main, row_branch, row_excl, row_chain;
     int nch, nb_main;         // chain units (of this pass's kind), bonded chunks
+    int chain_stages;         // PassGeometry::chain_stages
     int seg[6];               // PassGeometry::seg
     double* out;              // [kMaxLambda][MEDYAN_FF_COUNT + 1] energies
     const LambdaSet* lam_set; // result copied to slots [0, K) (null: slot 0)
@@ -56,17 +71,20 @@ struct PassArgs {
     int* f_status;
 };
 
-PassGeometry pass_geometry(const ChainDev& ch, const DeviceFF& ff);
+// stream: the chain segments in their own kernel (pass layout 2)
+PassGeometry pass_geometry(const ChainDev& ch, const DeviceFF& ff, bool stream);
 
 // Energy (energy = true) and/or forces (t set) of a single network's force
 // fields at t's positions (x when t is null or t->d is null). The energy lands
 // in es.out; the forces in target_force(*t), overwritten. Single networks
 // only (ff.act == null). Energies and forces are separate sets of kernels
 // with their own tickets (ps, ps_forces); with fk all of them run on parallel
-// branches.
+// branches. stream: the chain segments are staged through shared memory by
+// bulk copies in their own kernel (pass layout 2).
 void launch_pass_fused(const ChainDev& ch, const DeviceFF& ff, int prec, const double* x, const ForceTarget* t,
                        bool energy, const LambdaSet* lam_set, const EnergyScratch& es, const ForceScratch& fs,
-                       const PassScratch& ps, const PassScratch& ps_forces, cudaStream_t s, const Fork* fk);
+                       const PassScratch& ps, const PassScratch& ps_forces, cudaStream_t s, const Fork* fk,
+                       bool stream);
 
 // Fills pass.cu's quadrature grids, once per device (the current one); call
 // before any stream capture.

@@ -21,7 +21,7 @@ constexpr int kBonded[3] = {128, 256, 512};
 constexpr int kExcl[3] = {32, 64, 128};
 constexpr int kChain[3] = {128, 256, 512};
 constexpr int kEnergyBps[3] = {2, 4, 8};
-constexpr int kLayout[3] = {0, 1, kNone};
+constexpr int kLayout[3] = {0, 1, 2};
 
 medyan_launch_shapes current(const medyan_mech* h) {
     medyan_launch_shapes s{};

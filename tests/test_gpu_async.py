@@ -12,7 +12,7 @@ pytestmark = pytest.mark.gpu
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-@pytest.mark.parametrize("layout", [0, 1])
+@pytest.mark.parametrize("layout", [0, 1, 2])
 def test_async_stream_matches_sync(gpu_lib, oracle, precision, layout):
     net = make_workload(1)
     st, extra = oracle.complete(net)

@@ -73,16 +73,18 @@ def test_both_precisions_converge_on_the_gradient(gpu_lib, oracle, deterministic
     assert abs(em - e64) <= 2e-2 * abs(e64), (e64, em)
 
 
-def test_fused_force_pass_short_run(gpu_lib, oracle):
-    """The minimizer with the fused pass layout (its force pass: zero fill,
-    then the chain/bonded, branching and excluded-volume kernels side by side)
-    takes the oracle's iterations and calls."""
+@pytest.mark.parametrize("layout", [0, 2])
+def test_fused_force_pass_short_run(gpu_lib, oracle, layout):
+    """The minimizer with a fused pass layout (its force pass: zero fill,
+    then the chain/bonded, branching and excluded-volume kernels side by side;
+    layout 2 with the chain segments staged through shared memory) takes the
+    oracle's iterations and calls."""
     sv, x = small_net(oracle)
     p = cgp(grad_tol=1e-4, energy_rel_tol=1e-14, energy_call_limit=40)
     so, xo, fo, ro = oracle.minimize(sv, x, p)
     with ForceFieldManager("fp64") as ff:
         ff.vectorize_all_force_fields(sv)
-        ff.set_shapes(pass_layout=0)
+        ff.set_shapes(pass_layout=layout)
         sg, xg, fg, rg = ff.minimize(x, p)
     assert sg == so == 0
     assert (rg.num_energy_call, rg.num_force_call, rg.num_iter) == (ro.num_energy_call, ro.num_force_call, ro.num_iter)

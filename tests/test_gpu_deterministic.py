@@ -22,7 +22,7 @@ def net_of(oracle, cfg):
     return net.system_view(**extra), net.flat_coords()
 
 
-@pytest.mark.parametrize("layout", [0, 1])
+@pytest.mark.parametrize("layout", [0, 1, 2])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_forces_reproducible_and_match_oracle(gpu_lib, oracle, precision, layout):
     sv, x = net_of(oracle, 1)

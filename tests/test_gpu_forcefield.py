@@ -63,8 +63,9 @@ def network_system(nets, tag):
     return SystemView(int(nets[f"{tag}/n_beads"][0]), **arrays), nets[f"{tag}/coord"]
 
 
-# pass layouts: 0 fused kernels (the default), 1 one kernel per potential group
-LAYOUTS = [0, 1]
+# pass layouts: 0 fused kernels (the default), 1 one kernel per potential
+# group, 2 fused with the chain segments staged through shared memory
+LAYOUTS = [0, 1, 2]
 
 
 @pytest.mark.parametrize("layout", LAYOUTS)

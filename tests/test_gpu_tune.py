@@ -28,7 +28,8 @@ def close(e, f, eo, fo):
 
 SHAPES = [dict(bonded_threads=b, excl_threads=x, chain_threads=c, chain_energy_blocks_per_sm=g, pass_layout=p)
           for b, x, c, g, p in [(128, 32, 128, 2, 1), (512, 128, 512, 8, 0), (256, 64, 256, 4, 1),
-                                (128, 128, 512, 2, 0), (256, 32, 256, 4, 0)]]
+                                (128, 128, 512, 2, 0), (256, 32, 256, 4, 0), (256, 64, 256, 4, 2),
+                                (512, 128, 128, 2, 2)]]
 
 
 @pytest.mark.parametrize("shape", SHAPES)
@@ -60,7 +61,7 @@ def test_autotune(gpu_lib, oracle):
         assert chosen == ff.get_shapes()
         assert chosen["bonded_threads"] in (128, 256, 512) and chosen["excl_threads"] in (32, 64, 128)
         assert chosen["chain_threads"] in (128, 256, 512) and chosen["chain_energy_blocks_per_sm"] in (2, 4, 8)
-        assert chosen["pass_layout"] in (0, 1)
+        assert chosen["pass_layout"] in (0, 1, 2)
         e, per, f = ff.evaluate(x)
         close(e, f, eo, fo)
         with pytest.raises(MedyanError):
