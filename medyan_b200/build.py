@@ -18,6 +18,11 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libmedyan_b200.so")
+# profiling build: the same sources with the pass timeline compiled in
+# (-DMEDYAN_PASS_TRACE), a library of its own that only
+# medyan_b200/pass_timeline.py loads
+BUILD_TRACE = os.path.join(HERE, "_build_trace")
+LIB_TRACE = os.path.join(HERE, "libmedyan_b200_trace.so")
 
 SOURCES = ["capi.cu", "ff_kernels.cu", "chain.cu", "excl_kernels.cu", "nl.cu", "cg.cu", "batch.cu", "pbatch.cu", "diff.cu", "hessian.cu", "aux.cu", "tune.cu", "noalloc.cu", "pass.cu", "async.cu", "vectorize.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -40,20 +45,22 @@ def _stale(out: str, deps: list[str]) -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build(verbose: bool = False, force: bool = False, jobs: int | None = None) -> str:
+def build(verbose: bool = False, force: bool = False, jobs: int | None = None, trace: bool = False) -> str:
     """Compiles the stale translation units (in parallel, one nvcc per core)
-    and links the library."""
+    and links the library (trace: the pass-timeline profiling library)."""
     from concurrent.futures import ThreadPoolExecutor
-    os.makedirs(BUILD, exist_ok=True)
+    build_dir, lib = (BUILD_TRACE, LIB_TRACE) if trace else (BUILD, LIB)
+    extra = ["-DMEDYAN_PASS_TRACE"] if trace else []
+    os.makedirs(build_dir, exist_ok=True)
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
     headers.append(os.path.join(ROOT, "include", "medyan_b200.h"))
     objs, cmds = [], []
     for src in SOURCES:
         path = os.path.join(CSRC, src)
-        obj = os.path.join(BUILD, src.replace(".cu", ".o"))
+        obj = os.path.join(build_dir, src.replace(".cu", ".o"))
         objs.append(obj)
         if force or _stale(obj, [path, *headers, __file__]):
-            cmds.append([nvcc(), *ARCH, *COMMON, *PER_FILE.get(src, []), "-c", path, "-o", obj])
+            cmds.append([nvcc(), *ARCH, *COMMON, *extra, *PER_FILE.get(src, []), "-c", path, "-o", obj])
 
     def run(cmd: list[str]) -> None:
         if verbose:
@@ -66,13 +73,13 @@ def build(verbose: bool = False, force: bool = False, jobs: int | None = None) -
         with ThreadPoolExecutor(max_workers=jobs or min(len(cmds), os.cpu_count() or 1)) as pool:
             for fut in [pool.submit(run, c) for c in cmds]:
                 fut.result()
-    if force or _stale(LIB, objs):
-        cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
+    if force or _stale(lib, objs):
+        cmd = [nvcc(), *ARCH, "-shared", "-o", lib, *objs, "-lcudart"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
-    return LIB
+    return lib
 
 
 if __name__ == "__main__":
-    build(verbose=True, force="--force" in sys.argv)
+    build(verbose=True, force="--force" in sys.argv, trace="--trace" in sys.argv)

@@ -37,6 +37,57 @@
 
 #include <mutex>
 
+// Pass timeline (profiling build only: compiled with -DMEDYAN_PASS_TRACE into
+// libmedyan_b200_trace.so by `python -m medyan_b200.build --trace`). Thread 0
+// of every block of the pass kernels records the block's kernel kind, SM,
+// index and its start and end on the global timer; the blocks that complete
+// a group of energy rows and the block that finishes the pass record those
+// stages too. medyan_pass_trace_reset / medyan_pass_trace_dump read the
+// records back (medyan_b200/pass_timeline.py prints them per kernel).
+#ifdef MEDYAN_PASS_TRACE
+namespace mb {
+namespace trace {
+struct Rec {
+    unsigned kind, smid, block, pad;
+    unsigned long long t0, t1;
+};
+constexpr unsigned kCap = 1u << 16;
+__device__ Rec g_rec[kCap];
+__device__ unsigned g_n;
+__device__ __forceinline__ unsigned long long now() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ void record(unsigned kind, unsigned long long t0) {
+    if (threadIdx.x != 0) return;
+    unsigned sm;
+    asm volatile("mov.u32 %0, %%smid;" : "=r"(sm));
+    const unsigned i = atomicAdd(&g_n, 1u);
+    if (i < kCap) g_rec[i] = Rec{kind, sm, blockIdx.x, 0u, t0, now()};
+}
+}  // namespace trace
+}  // namespace mb
+extern "C" int medyan_pass_trace_reset() {
+    const unsigned z = 0;
+    return (int)cudaMemcpyToSymbol(mb::trace::g_n, &z, sizeof(z));
+}
+// Copies up to max records to host (32 bytes each); returns how many.
+extern "C" int medyan_pass_trace_dump(void* host, int max) {
+    unsigned n = 0;
+    if (cudaMemcpyFromSymbol(&n, mb::trace::g_n, sizeof(n)) != cudaSuccess) return -1;
+    if (n > mb::trace::kCap) n = mb::trace::kCap;
+    if ((int)n > max) n = (unsigned)max;
+    if (n && cudaMemcpyFromSymbol(host, mb::trace::g_rec, n * sizeof(mb::trace::Rec)) != cudaSuccess) return -1;
+    return (int)n;
+}
+#define PASS_TRACE_BEGIN const unsigned long long trace_t0 = mb::trace::now();
+#define PASS_TRACE_END(kind) mb::trace::record((kind), trace_t0);
+#else
+#define PASS_TRACE_BEGIN
+#define PASS_TRACE_END(kind)
+#endif
+
 namespace mb {
 
 namespace {
@@ -257,6 +308,7 @@ __device__ __forceinline__ void block_done(const PassArgs& a, double (&acc)[NV],
     }
     __syncthreads();
     if (state == 0) return;
+    PASS_TRACE_BEGIN
     if constexpr (E) {
         if (threadIdx.x < 32) {
             const int r = kGroup * g + threadIdx.x;
@@ -278,8 +330,16 @@ __device__ __forceinline__ void block_done(const PassArgs& a, double (&acc)[NV],
         state = ticket_add(a.ticket, 1u) == (unsigned)ng - 1 ? 2 : 1;
     }
     __syncthreads();
+    PASS_TRACE_END(100 + KIND)
     if (state != 2) return;
+#ifdef MEDYAN_PASS_TRACE
+    const unsigned long long trace_f0 = mb::trace::now();
+#endif
     pass_finish<E, F>(a);
+#ifdef MEDYAN_PASS_TRACE
+    __syncthreads();
+    mb::trace::record(200 + KIND, trace_f0);
+#endif
 }
 
 // ------------------------------------------------------------ main kernel
@@ -461,6 +521,7 @@ __device__ __forceinline__ void main_chunk(const PassArgs& a, const Pos& P, doub
 template <class R, bool E, bool F, bool LS>
 __global__ void __launch_bounds__(kPassThreads, main_blocks_per_sm<R, E, F, LS>())
     k_pass_main(const __grid_constant__ PassArgs a) {
+    PASS_TRACE_BEGIN
     if (F && a.t.skip && *a.t.skip) return;
     double* __restrict__ f = F ? target_force(a.t) : nullptr;
     const Pos P = pos_of(a);
@@ -502,6 +563,7 @@ __global__ void __launch_bounds__(kPassThreads, main_blocks_per_sm<R, E, F, LS>(
     }
     // a force-only pass has no rows here: the main kernel's blocks take no ticket
     if constexpr (E) block_done<0, E, F>(a, acc, a.row_main + blockIdx.x, false);
+    PASS_TRACE_END(0 + (E ? 10 : 0))
 }
 
 // ------------------------------------------------------------ streamed chain
@@ -645,6 +707,7 @@ __device__ __forceinline__ V3 stage_pos(const ChainStage<LS>& st, int p, double 
 // centres. Force-only passes take no tickets here.
 template <class R, bool E, bool F, bool LS>
 __global__ void __launch_bounds__(kChainThreads + 32) k_pass_chain(const __grid_constant__ PassArgs a) {
+    PASS_TRACE_BEGIN
     if (F && a.t.skip && *a.t.skip) return;
     extern __shared__ __align__(128) unsigned char chain_smem[];
     const int K = a.chain_stages;  // stages of the ring (1 when each block takes one segment)
@@ -743,11 +806,13 @@ __global__ void __launch_bounds__(kChainThreads + 32) k_pass_chain(const __grid_
         }
     }
     if constexpr (E) block_done<0, E, F>(a, acc, a.row_chain + blockIdx.x, false);
+    PASS_TRACE_END(4 + (E ? 10 : 0))
 }
 
 // ------------------------------------------------------------ branch points
 template <class R, bool E, bool F>
 __global__ void __launch_bounds__(kPassThreads) k_pass_branch(const __grid_constant__ PassArgs a) {
+    PASS_TRACE_BEGIN
     if (F && a.t.skip && *a.t.skip) return;
     double* __restrict__ f = F ? target_force(a.t) : nullptr;
     const Pos P = pos_of(a);
@@ -804,6 +869,7 @@ __global__ void __launch_bounds__(kPassThreads) k_pass_branch(const __grid_const
         }
     }
     if constexpr (E) block_done<1, E, F>(a, acc, a.row_branch + blockIdx.x, false);
+    PASS_TRACE_END(1 + (E ? 10 : 0))
 }
 
 // ------------------------------------------------------------ excluded volume
@@ -811,6 +877,7 @@ __global__ void __launch_bounds__(kPassThreads) k_pass_branch(const __grid_const
 // reference would reject goes to the fallback queue instead.
 template <bool E, bool F, bool EXACT>
 __global__ void __launch_bounds__(kExclThreadsMax) k_pass_excl(const __grid_constant__ PassArgs a) {
+    PASS_TRACE_BEGIN
     if (F && a.t.skip && *a.t.skip) return;
     double* __restrict__ f = F ? target_force(a.t) : nullptr;
     const Pos P = pos_of(a);
@@ -848,10 +915,12 @@ __global__ void __launch_bounds__(kExclThreadsMax) k_pass_excl(const __grid_cons
         }
     }
     block_done<2, E, F>(a, acc, a.row_excl + blockIdx.x, queued);
+    PASS_TRACE_END(2 + (E ? 10 : 0))
 }
 
 // ------------------------------------------------------------ zero fill
 __global__ void __launch_bounds__(kZeroThreads) k_pass_zero(const ForceTarget t, int n3) {
+    PASS_TRACE_BEGIN
     if (t.skip && *t.skip) return;
     double* __restrict__ f = target_force(t);
     // cudaMalloc'd buffers are 256-byte aligned: pairs of doubles, then the odd tail
@@ -859,6 +928,7 @@ __global__ void __launch_bounds__(kZeroThreads) k_pass_zero(const ForceTarget t,
     const int n2 = n3 >> 1;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n2; i += gridDim.x * blockDim.x) f2[i] = double2{0.0, 0.0};
     if ((n3 & 1) && blockIdx.x == 0 && threadIdx.x == 0) f[n3 - 1] = 0.0;
+    PASS_TRACE_END(3)
 }
 
 template <class R, bool E, bool F>
