@@ -193,11 +193,14 @@ def run_ours(args, rank: int, world: int) -> dict:
 
     K = args.steps
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
-    if world > 1:
-        torch.distributed.barrier()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
+    # the clock sampler's process starts before the timed region: its
+    # start-up (fork, exec, NVML init) must not stall the launch of a timed step
     with ClockSampler(dev) as clocks:
+        time.sleep(0.3)
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
         with torch.cuda.stream(stream):
             for i in range(K):
                 flush.zero_()
