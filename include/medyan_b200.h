@@ -222,8 +222,9 @@ medyan_status medyan_mech_synchronize(medyan_mech* h);
    at most about 1e-9 pN per bead, and a contribution of 2^24 pN (1.7e7 pN)
    or more is out of range: the call reports MEDYAN_ERR_NONFINITE. Energies
    are deterministic in both modes. Applies to the standalone passes, the
-   evaluate entry points and the minimizer (not to packed batches, the
-   Hessian or the Hessian-vector product). on = 0 restores the default. */
+   evaluate entry points and the minimizer (packed batches have
+   medyan_batch_set_deterministic; not to the Hessian or the
+   Hessian-vector product). on = 0 restores the default. */
 medyan_status medyan_mech_set_deterministic(medyan_mech* h, int32_t on);
 
 /* Asynchronous medyan_mech_evaluate, for a caller that evaluates many
@@ -542,6 +543,14 @@ medyan_mech* medyan_batch_replica(medyan_batch* b, int32_t r);
    MEDYAN_ERR_LINE_SEARCH, else MEDYAN_OK. */
 medyan_status medyan_batch_minimize(medyan_batch* b, const medyan_cg_params* p, double* const* coords_inout,
                                     double* const* forces_out, medyan_min_result* results, int32_t* statuses);
+/* Bitwise reproducible force sums for the whole batch (no counterpart in
+   the reference, whose CPU sums are sequential): the packed minimizer's
+   force passes and every replica's own passes sum force contributions as
+   64-bit fixed-point integers, as medyan_mech_set_deterministic does for one
+   network, so a batched minimization gives the same bits on every run. A
+   contribution of 2^24 pN or more makes medyan_batch_minimize return
+   MEDYAN_ERR_NONFINITE. on = 0 restores floating-point atomic sums. */
+medyan_status medyan_batch_set_deterministic(medyan_batch* b, int32_t on);
 /* Energy and forces of every replica (e_totals: double[n]). */
 medyan_status medyan_batch_evaluate(medyan_batch* b, const double* const* coords, double* e_totals,
                                     double* const* forces_out);

@@ -53,6 +53,21 @@ medyan_status medyan_batch_destroy(medyan_batch* b) {
 
 int32_t medyan_batch_size(const medyan_batch* b) { return b ? (int32_t)b->h.size() : 0; }
 
+medyan_status medyan_batch_set_deterministic(medyan_batch* b, int32_t on) {
+    if (!b || (on != 0 && on != 1)) return MEDYAN_ERR_INVALID_ARG;
+    if (b->pb.stream) {
+        cudaError_t e = cudaStreamSynchronize(b->pb.stream);  // no packed pass may still write the old way
+        if (e != cudaSuccess) return cuda_status(e);
+    }
+    // the replicas' own passes (medyan_batch_evaluate) follow the same setting
+    for (medyan_mech* h : b->h) {
+        const medyan_status st = medyan_mech_set_deterministic(h, on);
+        if (st != MEDYAN_OK) return st;
+    }
+    b->pb.deterministic = on != 0;
+    return MEDYAN_OK;
+}
+
 medyan_mech* medyan_batch_replica(medyan_batch* b, int32_t r) {
     return (b && r >= 0 && r < (int32_t)b->h.size()) ? b->h[r] : nullptr;
 }
@@ -84,10 +99,15 @@ medyan_status medyan_batch_minimize(medyan_batch* b, const medyan_cg_params* p, 
         e = coords_to_host(b->h[r], pb.x.raw() + o, coords_inout[r], s);
         if (e == cudaSuccess && forces_out && forces_out[r]) e = coords_to_host(b->h[r], pb.fcur.raw() + o, forces_out[r], s);
     }
+    int force_status = 0;
+    if (e == cudaSuccess && pb.deterministic)
+        e = cudaMemcpyAsync(&force_status, pb.fs.status, sizeof(int), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_status(e);
     const int kOut = MEDYAN_FF_COUNT + 1;
-    medyan_status worst = MEDYAN_OK;
+    // a force contribution out of the fixed-point range (bit 2) leaves the
+    // sums wrong for the whole batch
+    medyan_status worst = (force_status & 4) ? MEDYAN_ERR_NONFINITE : MEDYAN_OK;
     for (int r = 0; r < n; ++r) {
         const CGState& c = sf[r];
         statuses[r] = c.status;

@@ -1102,7 +1102,8 @@ void b_step(PackedBatch& pb, int prec, cudaStream_t s) {
     const int R = pb.R;
     k_b_scale<<<R, kVecThreads, 0, s>>>(pb.base_dev.raw(), pb.d.raw(), pb.dS.raw(), pb.st.raw(), pb.lam0.raw(), 1,
                                         pb.act.raw());
-    const ForceTarget t{pb.fnew.raw(), nullptr, nullptr, nullptr, pb.dS.raw(), pb.one.raw()};
+    const ForceTarget t{pb.fnew.raw(), nullptr, nullptr, nullptr, pb.dS.raw(), pb.one.raw(), pb.deterministic ? 1 : 0,
+                        pb.fs.status};
     launch_forces(pb.ch, pb.ff, prec, pb.x.raw(), t, pb.fs, s, &pb.fork);
     k_b_dots<<<R, kVecThreads, 0, s>>>(pb.base_dev.raw(), pb.x.raw(), pb.d.raw(), pb.fcur.raw(), pb.fnew.raw(),
                                        pb.st.raw());
@@ -1203,7 +1204,8 @@ medyan_status cg_batch_time_evaluate(PackedBatch& pb, int prec, int reps, float*
     z.K = 1;
     if (e == cudaSuccess) e = pb.Lzero.assign(&z, 1, s);
     if (e != cudaSuccess) return cuda_status(e);
-    const ForceTarget t{pb.fnew.raw(), nullptr, nullptr, nullptr, nullptr, nullptr};
+    const ForceTarget t{pb.fnew.raw(), nullptr, nullptr, nullptr, nullptr, nullptr, pb.deterministic ? 1 : 0,
+                        pb.fs.status};
     auto pass = [&] {
         b_energy_pass(pb, nullptr, pb.Lzero.raw(), s);
         // the CG's decide step clears the fallback queue; do it here
@@ -1290,6 +1292,7 @@ medyan_status cg_batch_run(PackedBatch& pb, int prec, const medyan_cg_params* p)
     if (e == cudaSuccess) e = cudaMemsetAsync(pb.d.raw(), 0, bytes ? bytes : 8, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(pb.fcur.raw(), 0, bytes ? bytes : 8, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(pb.fnew.raw(), 0, bytes ? bytes : 8, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(pb.fs.status, 0, sizeof(int), s);
     if (e != cudaSuccess) return cuda_status(e);
 
     // energiesBefore, then the first force, F.F, d = F
@@ -1299,7 +1302,7 @@ medyan_status cg_batch_run(PackedBatch& pb, int prec, const medyan_cg_params* p)
     k_b_record<<<(R + 127) / 128, 128, 0, s>>>(R, pb.st.raw(), pb.out.raw(), pb.eout.raw(), 1);
     b_step(pb, prec, s);
 
-    if (pb.graph && (pb.graph_gen != pb.gen || pb.graph_prec != prec)) {
+    if (pb.graph && (pb.graph_gen != pb.gen || pb.graph_prec != prec || pb.graph_det != pb.deterministic)) {
         cudaGraphExecDestroy(pb.graph);
         pb.graph = nullptr;
     }
@@ -1308,6 +1311,7 @@ medyan_status cg_batch_run(PackedBatch& pb, int prec, const medyan_cg_params* p)
         if (e != cudaSuccess) return cuda_status(e);
         pb.graph_gen = pb.gen;
         pb.graph_prec = prec;
+        pb.graph_det = pb.deterministic;
     }
     e = cudaGraphLaunch(pb.graph, s);
     if (e != cudaSuccess) return cuda_status(e);

@@ -145,76 +145,91 @@ __global__ void __launch_bounds__(kBlock) k_excl_force_fallback(const DeviceFF f
 constexpr int kFinishThreads = 1024;
 constexpr int kSplitFinishThreads = 256;
 
-// Slot sums of one block's share [r_lo, r_hi) of a lambda's partial rows:
-// each thread adds its rows' columns into the slot their range belongs to
-// (chain rows: slots 0 and 1; bonded segment s: slot s, or slots 4-7 for
-// branching, slot 9 for the boundary; excluded-volume rows: slot 8), then the
-// block reduces in a fixed tree. Valid in thread 0 of warp 0 (out[slot]).
-__device__ void finish_rows(const DeviceFF& ff, const double* __restrict__ base, int r_lo, int r_hi, int nch,
-                            int nbb, double* wsum /* [32][MEDYAN_FF_COUNT] */, double* out) {
+// Slot sums of one block's share [r_lo, r_hi) of the partial rows of the K
+// step sizes (the rows of step size k start at base + k * stride): each
+// thread adds its rows' columns into the slot their range belongs to (chain
+// rows: slots 0 and 1; bonded segment s: slot s, or slots 4-7 for branching,
+// slot 9 for the boundary; excluded-volume rows: slot 8), then the block
+// reduces in a fixed tree. The rows of all K step sizes are loaded in one
+// round (one round of loads and barriers per step size made a line-search
+// pass's finish several L2 round trips longer); per step size the additions
+// are those of a single one. Valid in thread 0 (out + k * out_stride).
+__device__ void finish_rows(const DeviceFF& ff, const double* __restrict__ base, size_t stride, int K, int r_lo,
+                            int r_hi, int nch, int nbb,
+                            double* wsum /* [32][kMaxLambda][MEDYAN_FF_COUNT] */, double* out, size_t out_stride) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
     int seg[7];
 #pragma unroll
     for (int i = 0; i < 7; ++i) seg[i] = ff.seg[i];
-    double acc[MEDYAN_FF_COUNT];
+    double acc[kMaxLambda][MEDYAN_FF_COUNT];
 #pragma unroll
-    for (int i = 0; i < MEDYAN_FF_COUNT; ++i) acc[i] = 0.0;
-    constexpr int kRows = 2;
-    for (int r0 = r_lo; r0 < r_hi; r0 += kRows * blockDim.x) {
-        double2 lo[kRows], hi[kRows];
+    for (int k = 0; k < kMaxLambda; ++k)
 #pragma unroll
-        for (int u = 0; u < kRows; ++u) {
-            const int r = r0 + u * blockDim.x + threadIdx.x;
-            if (r < r_hi) {
-                const double2* row = reinterpret_cast<const double2*>(base + (size_t)r * 4);
-                lo[u] = __ldcg(row);
-                hi[u] = __ldcg(row + 1);
+        for (int i = 0; i < MEDYAN_FF_COUNT; ++i) acc[k][i] = 0.0;
+    for (int r = r_lo + threadIdx.x; r < r_hi; r += blockDim.x) {
+        double2 lo[kMaxLambda], hi[kMaxLambda];
+#pragma unroll
+        for (int k = 0; k < kMaxLambda; ++k) {
+            if (k < K) {
+                const double2* row = reinterpret_cast<const double2*>(base + k * stride + (size_t)r * 4);
+                lo[k] = __ldcg(row);
+                hi[k] = __ldcg(row + 1);
             } else {
-                lo[u] = hi[u] = double2{0.0, 0.0};
+                lo[k] = hi[k] = double2{0.0, 0.0};
             }
         }
-#pragma unroll
-        for (int u = 0; u < kRows; ++u) {
-            const int r = r0 + u * blockDim.x + threadIdx.x;
-            if (r >= r_hi) continue;
-            if (r < nch) {
-                acc[0] += lo[u].x;
-                acc[1] += lo[u].y;
-                continue;
-            }
+        int cls;  // 0 chain, 1-4 bonded segment 0-3, 5 branching, 6 boundary, 7 excluded volume
+        if (r < nch) {
+            cls = 0;
+        } else {
             const int rb = r - nch;
-            if (rb >= nbb) {
-                acc[MEDYAN_FF_EXCLUDED_VOLUME] += lo[u].x;
-            } else if (rb < seg[4]) {
-                const int sg = rb < seg[1] ? 0 : rb < seg[2] ? 1 : rb < seg[3] ? 2 : 3;
+            if (rb >= nbb) cls = 7;
+            else if (rb < seg[4]) cls = 1 + (rb < seg[1] ? 0 : rb < seg[2] ? 1 : rb < seg[3] ? 2 : 3);
+            else if (rb < seg[5]) cls = 5;
+            else cls = 6;
+        }
+#pragma unroll
+        for (int k = 0; k < kMaxLambda; ++k) {
+            if (cls == 0) {
+                acc[k][0] += lo[k].x;
+                acc[k][1] += lo[k].y;
+            } else if (cls <= 4) {
 #pragma unroll
                 for (int i = 0; i < 4; ++i)
-                    if (i == sg) acc[i] += lo[u].x;
-            } else if (rb < seg[5]) {
-                acc[4] += lo[u].x;
-                acc[5] += lo[u].y;
-                acc[6] += hi[u].x;
-                acc[7] += hi[u].y;
+                    if (i == cls - 1) acc[k][i] += lo[k].x;
+            } else if (cls == 5) {
+                acc[k][4] += lo[k].x;
+                acc[k][5] += lo[k].y;
+                acc[k][6] += hi[k].x;
+                acc[k][7] += hi[k].y;
+            } else if (cls == 6) {
+                acc[k][9] += lo[k].x;
             } else {
-                acc[9] += lo[u].x;
+                acc[k][MEDYAN_FF_EXCLUDED_VOLUME] += lo[k].x;
             }
         }
     }
 #pragma unroll
-    for (int i = 0; i < MEDYAN_FF_COUNT; ++i) {
-        double v = acc[i];
+    for (int k = 0; k < kMaxLambda; ++k) {
+        if (k >= K) break;
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-        if (lane == 0) wsum[warp * MEDYAN_FF_COUNT + i] = v;
+        for (int i = 0; i < MEDYAN_FF_COUNT; ++i) {
+            double v = acc[k][i];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+            if (lane == 0) wsum[(warp * kMaxLambda + k) * MEDYAN_FF_COUNT + i] = v;
+        }
     }
     __syncthreads();
     if (warp == 0) {
+        for (int k = 0; k < K; ++k) {
 #pragma unroll
-        for (int i = 0; i < MEDYAN_FF_COUNT; ++i) {
-            double v = lane < nwarp ? wsum[lane * MEDYAN_FF_COUNT + i] : 0.0;
+            for (int i = 0; i < MEDYAN_FF_COUNT; ++i) {
+                double v = lane < nwarp ? wsum[(lane * kMaxLambda + k) * MEDYAN_FF_COUNT + i] : 0.0;
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-            if (lane == 0) out[i] = v;
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+                if (lane == 0) out[k * out_stride + i] = v;
+            }
         }
     }
     __syncthreads();
@@ -236,20 +251,22 @@ __global__ void __launch_bounds__(kSplitFinishThreads) k_energy_finish(
     int2* __restrict__ fb_list, int* __restrict__ bad, double* __restrict__ out, double* __restrict__ stage,
     unsigned int* __restrict__ ticket) {
     __shared__ double red[4 * 32];
-    __shared__ double wsum[(kSplitFinishThreads / 32) * MEDYAN_FF_COUNT];
+    __shared__ double wsum[(kSplitFinishThreads / 32) * kMaxLambda * MEDYAN_FF_COUNT];
     __shared__ double sums[kMaxLambda][MEDYAN_FF_COUNT];
     __shared__ double fbE[kMaxLambda];
-    __shared__ int nfb;
+    __shared__ int nfb, n_queued, bad0[kMaxLambda];
     __shared__ bool last;
     const int K = lset ? lset->K : 1;
     const int total_blocks = nch + nbb + nbe;
     const int G = gridDim.x;
     const int chunk = (total_blocks + G - 1) / G;
     const int r_lo = min(total_blocks, (int)blockIdx.x * chunk), r_hi = min(total_blocks, r_lo + chunk);
-    for (int k = 0; k < K; ++k) {
-        double* dst = G > 1 ? stage + ((size_t)k * G + blockIdx.x) * MEDYAN_FF_COUNT : sums[k];
-        finish_rows(ff, partial + (size_t)k * total_blocks * 4, r_lo, r_hi, nch, nbb, wsum, dst);
-    }
+    if (G > 1)
+        finish_rows(ff, partial, (size_t)total_blocks * 4, K, r_lo, r_hi, nch, nbb, wsum,
+                    stage + (size_t)blockIdx.x * MEDYAN_FF_COUNT, (size_t)G * MEDYAN_FF_COUNT);
+    else
+        finish_rows(ff, partial, (size_t)total_blocks * 4, K, r_lo, r_hi, nch, nbb, wsum, &sums[0][0],
+                    MEDYAN_FF_COUNT);
     if (G > 1) {
         // last-block-done: this block's shares (thread 0's stores) are
         // published by thread 0's acquire-release ticket
@@ -258,16 +275,27 @@ __global__ void __launch_bounds__(kSplitFinishThreads) k_energy_finish(
         __syncthreads();
         if (!last) return;
         if (threadIdx.x < K * MEDYAN_FF_COUNT) {
+            // the G shares loaded at once, added in block order
             const int k = threadIdx.x / MEDYAN_FF_COUNT, slot = threadIdx.x % MEDYAN_FF_COUNT;
+            double sh[kFinishBlocks];
+#pragma unroll
+            for (int b = 0; b < kFinishBlocks; ++b)
+                sh[b] = b < G ? __ldcg(stage + ((size_t)k * G + b) * MEDYAN_FF_COUNT + slot) : 0.0;
             double v = 0.0;
-            for (int b = 0; b < G; ++b) v += __ldcg(stage + ((size_t)k * G + b) * MEDYAN_FF_COUNT + slot);
+#pragma unroll
+            for (int b = 0; b < kFinishBlocks; ++b)
+                if (b < G) v += sh[b];
             sums[k][slot] = v;
         }
         if (threadIdx.x == 0) *ticket = 0u;
     }
+    // the queue length and the status flags, fetched before they are needed
+    if (threadIdx.x == 0) n_queued = *fb_count;
+    if (threadIdx.x < kMaxLambda) bad0[threadIdx.x] = bad[threadIdx.x];
+    __syncthreads();
     // queued fallback pairs: energyN in (slot, pair) order
     if (threadIdx.x == 0) {
-        int n = min(*fb_count, kFallbackCap);
+        int n = min(n_queued, kFallbackCap);
         for (int a = 1; a < n; ++a) {
             int2 v = fb_list[a];
             int b = a - 1;
@@ -307,7 +335,8 @@ __global__ void __launch_bounds__(kSplitFinishThreads) k_energy_finish(
                 double v = sums[k][slot];
                 if (slot == MEDYAN_FF_EXCLUDED_VOLUME) {
                     v += fbE[k];
-                    if (bad[k]) v = -1.0;
+                    // the fallbacks may have flagged a pair: read the flag again then
+                    if (nfb > 0 ? bad[k] : bad0[k]) v = -1.0;
                 }
                 o[slot] = v;
                 if (v <= -1) inf = true;

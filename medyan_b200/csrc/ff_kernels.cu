@@ -301,20 +301,23 @@ int bonded_blocks(const DeviceFF& ff) { return ff.seg[6]; }
 namespace {
 
 // Deterministic mode: the fixed-point sums back to double, in place.
-__global__ void __launch_bounds__(256) k_fixed_to_double(const ForceTarget t, int n3) {
+// rep/act (packed batches): the positions of replicas not in the pass were
+// not written by it and still hold doubles; they are left alone.
+__global__ void __launch_bounds__(256) k_fixed_to_double(const ForceTarget t, int n3, const int* __restrict__ rep,
+                                                         const int* __restrict__ act) {
     if (t.skip && *t.skip) return;
     double* __restrict__ f = target_force(t);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x)
-        f[i] = double(__double_as_longlong(f[i])) / kFixedScale;
+        if (!act || act[rep[i / 3]]) f[i] = double(__double_as_longlong(f[i])) / kFixedScale;
 }
 
 }  // namespace
 
-void launch_fixed_to_double(const ForceTarget& t, int n3, cudaStream_t s) {
+void launch_fixed_to_double(const ForceTarget& t, int n3, cudaStream_t s, const int* rep, const int* act) {
     if (!t.fixed || n3 <= 0) return;
     int g = (n3 + 255) / 256;
     g = g > 148 * 8 ? 148 * 8 : g;
-    k_fixed_to_double<<<g, 256, 0, s>>>(t, n3);
+    k_fixed_to_double<<<g, 256, 0, s>>>(t, n3, rep, act);
 }
 
 namespace {
@@ -402,7 +405,7 @@ void launch_forces(const ChainDev& ch, const DeviceFF& ff, int prec, const doubl
     bonded_forces_group<0, 2>(ff, prec, x, t, b[3]);
     launch_excl_forces(ff, prec, x, t, fs, s);
     if (fk) join_from(fk, s, 3);
-    launch_fixed_to_double(t, 3 * ch.n_pos, s);
+    launch_fixed_to_double(t, 3 * ch.n_pos, s, ch.rep, ch.act);
 }
 
 void launch_evaluate(const ChainDev& ch, const DeviceFF& ff, int prec, const double* x, const double* d,
@@ -442,7 +445,7 @@ void launch_evaluate(const ChainDev& ch, const DeviceFF& ff, int prec, const dou
         cudaEventRecord(fk->join[k], fk->side[k]);
         cudaStreamWaitEvent(s, fk->join[k], 0);
     }
-    launch_fixed_to_double(t, 3 * ch.n_pos, s);
+    launch_fixed_to_double(t, 3 * ch.n_pos, s, ch.rep, ch.act);
 }
 
 }  // namespace mb

@@ -197,7 +197,8 @@ void launch_evaluate(const ChainDev& ch, const DeviceFF& ff, int prec, const dou
 void launch_chain_forces(const ChainDev& ch, int prec, const double* x, const ForceTarget& t, cudaStream_t s);
 // Deterministic mode: the target's fixed-point sums back to double, in place
 // (nothing when t.fixed is 0).
-void launch_fixed_to_double(const ForceTarget& t, int n3, cudaStream_t s);
+void launch_fixed_to_double(const ForceTarget& t, int n3, cudaStream_t s, const int* rep = nullptr,
+                            const int* act = nullptr);
 // table (optional): block b evaluates positions [table[b].y, table[b].z) of one
 // replica (batched layouts), table_blocks blocks; else a grid-stride pass.
 void launch_chain_energy(const ChainDev& ch, int prec, const double* x, const double* d, const LambdaSet* lam,

@@ -67,6 +67,10 @@ struct PackedBatch {
     cudaGraphExec_t graph = nullptr;
     int graph_prec = -1;
     long long graph_gen = -1;
+    // fixed-point force sums (medyan_batch_set_deterministic); the graph
+    // is rebuilt when it changes
+    bool deterministic = false;
+    bool graph_det = false;
 
     cudaStream_t stream = nullptr;
     Fork fork{};

@@ -325,6 +325,12 @@ class BatchMinimizer:
         L.check(self.lib.medyan_batch_autotune(self.handle, reps, C.byref(sh)), "medyan_batch_autotune")
         return sh.as_dict()
 
+    def set_deterministic(self, on: bool = True) -> None:
+        """Fixed-point force sums for the packed minimizer and every replica
+        (medyan_batch_set_deterministic): bitwise reproducible batches."""
+        L.check(self.lib.medyan_batch_set_deterministic(self.handle, 1 if on else 0),
+                "medyan_batch_set_deterministic")
+
     def replica(self, r: int) -> C.c_void_p:
         """The handle of replica r (for set_cylinders / rebuild_neighbors)."""
         return C.c_void_p(self.lib.medyan_batch_replica(self.handle, r))

@@ -39,6 +39,7 @@ PROTOTYPES = {
     "medyan_mech_synchronize": (C.c_int32, [_vp]),
     "medyan_mech_evaluate_async": (C.c_int32, [_vp, _pd, _pd, _pd]),
     "medyan_mech_set_deterministic": (C.c_int32, [_vp, C.c_int32]),
+    "medyan_batch_set_deterministic": (C.c_int32, [_vp, C.c_int32]),
     "medyan_mech_set_host_packing": (C.c_int32, [_vp, C.c_int32]),
     "medyan_mech_wait": (C.c_int32, [_vp]),
     "medyan_mech_stream": (_vp, [_vp]),

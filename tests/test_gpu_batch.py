@@ -144,3 +144,32 @@ def test_full_ensemble_start_state_matches_oracle(gpu_lib, oracle, precision):
         # energies are FP64 in both precisions
         assert abs(rs[r].energy_before_total - eo) <= 1e-12 * abs(eo), (r, rs[r].energy_before_total, eo)
         assert np.abs(fo[r] - fref).max() <= tol * np.abs(fref).max(), r
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batch_deterministic_reproducible(gpu_lib, oracle, precision):
+    """medyan_batch_set_deterministic: fixed-point force sums make a batched
+    minimization bitwise reproducible, and each replica still takes the
+    calls and steps it takes alone (single network, deterministic sums)."""
+    reps = replicas(oracle, n=6, seed=11)
+    p = cgp(grad_tol=1e-4, energy_rel_tol=1e-14, energy_call_limit=40)
+    runs = []
+    with BatchMinimizer([sv for sv, _ in reps], precision) as b:
+        b.set_deterministic(True)
+        for _ in range(2):
+            runs.append(b.minimize([x for _, x in reps], p))
+    (st1, xs1, fs1, rs1), (st2, xs2, fs2, rs2) = runs
+    for r, (sv, x) in enumerate(reps):
+        assert st1[r] == st2[r] == 0
+        assert np.array_equal(xs1[r], xs2[r]) and np.array_equal(fs1[r], fs2[r])
+        assert rs1[r].energy_after_total == rs2[r].energy_after_total
+        assert (rs1[r].num_energy_call, rs1[r].num_iter) == (rs2[r].num_energy_call, rs2[r].num_iter)
+        with ForceFieldManager(precision) as ff:
+            ff.vectorize_all_force_fields(sv)
+            ff.set_deterministic(True)
+            s1, x1, f1, r1 = ff.minimize(x, p)
+        assert s1 == 0
+        assert (rs1[r].num_energy_call, rs1[r].num_force_call, rs1[r].num_iter) == \
+            (r1.num_energy_call, r1.num_force_call, r1.num_iter)
+        assert np.abs(xs1[r] - x1).max() <= 1e-7
+        assert np.abs(fs1[r] - f1).max() <= 1e-7 * np.abs(f1).max()
