@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-minimize", action="store_true", help="skip the minimization extras")
     ap.add_argument("--cpu-sample-s", type=float, default=15.0)
+    ap.add_argument("--cpu-ensemble", action="store_true",
+                    help="only the host baseline of the batched ensemble (one JSON line; used by the bench itself)")
     return ap.parse_args()
 
 
@@ -461,6 +463,66 @@ def minimize_extras(net, make) -> dict:
     return out
 
 
+_CPU_WORKER = {}
+
+
+def _cpu_replica_init() -> None:
+    from oracle.oracle import Oracle, Reference
+    _CPU_WORKER["orc"] = Oracle()
+    _CPU_WORKER["ref"] = Reference() if Reference.available() else None
+
+
+def _cpu_replica_minimize(net):
+    """One replica minimized by the reference's CGMethod (oracle/_ref), in a
+    worker process: (start, end, force calls)."""
+    from medyan_b200.forcefield import conjugate_gradient_params
+    orc, ref = _CPU_WORKER["orc"], _CPU_WORKER["ref"]
+    st, extra = orc.complete(net)
+    sv = net.system_view(**extra)
+    p = conjugate_gradient_params(grad_tol=1.0, max_dist=1.0, lambda_max=0.01, energy_rel_tol=1e-9)
+    t0 = time.perf_counter()
+    s, xm, fm, r = (ref or orc).minimize(sv, net.flat_coords(), p)
+    return t0, time.perf_counter(), int(r.num_force_call)
+
+
+def cpu_ensemble(n_replicas: int = 256, budget_s: float = 60.0) -> dict:
+    """The batched ensemble on the host: every replica minimized by the
+    reference's CGMethod, one replica per host core at a time (a spawn pool
+    of one process per core), the same networks and criteria as the device
+    batch. Bounded: replicas not finished within budget_s are not counted."""
+    import multiprocessing as mp
+
+    from oracle.oracle import Reference
+    nets = ensemble(n_replicas)
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    ctx = mp.get_context("spawn")
+    done = []
+    t_wall = time.perf_counter()
+    with ctx.Pool(cores, initializer=_cpu_replica_init) as pool:
+        # largest replicas first, so the pool's tail is short
+        order = sorted(range(len(nets)), key=lambda r: -nets[r].n_beads)
+        it = pool.imap_unordered(_cpu_replica_minimize, [nets[r] for r in order])
+        for _ in order:
+            left = budget_s - (time.perf_counter() - t_wall)
+            if left <= 0:
+                break
+            try:
+                done.append(it.next(timeout=left))
+            except mp.TimeoutError:
+                break
+        pool.terminate()
+    if not done:
+        return {"unavailable": f"no replica finished within {budget_s:.0f} s"}
+    t0 = min(d[0] for d in done)
+    t1 = max(d[1] for d in done)
+    # process start-up is excluded: the span runs from the first replica's
+    # start to the last one's end
+    return {"kind": "reference" if Reference.available() else "port", "cores": cores,
+            "minimizations_per_s": len(done) / (t1 - t0), "replicas_done": len(done), "replicas": len(nets),
+            "sample": f"{len(done)} of {len(nets)} replicas minimized in {t1 - t0:.1f} s on {cores} processes",
+            "force_calls_mean": float(sum(d[2] for d in done) / len(done))}
+
+
 def cpu_extras(net, gpu_min: dict | None) -> dict:
     """CPU baselines beside the device numbers, each a bounded sample on one
     host thread: the reference's own CGMethod (oracle/_ref) on the benchmark
@@ -507,7 +569,28 @@ def cpu_extras(net, gpu_min: dict | None) -> dict:
     dt = time.perf_counter() - t0
     out["nl_rebuild"] = {"kind": "port", "cores": 1, "rebuilds_per_s": n / dt,
                          "sample": f"{n} rebuilds of the 400k-cylinder list in {dt:.1f} s"}
+    out["batched_ensemble"] = cpu_ensemble_in_child()
     return out
+
+
+def cpu_ensemble_in_child(budget_s: float = 60.0) -> dict:
+    """cpu_ensemble in a child process (bench.py --cpu-ensemble), so its
+    process pool never shares a process with the device work, and a hard
+    timeout ends the child's whole process group."""
+    import signal
+    cmd = [sys.executable, os.path.abspath(__file__), "--cpu-ensemble", "--cpu-sample-s", str(budget_s)]
+    proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, start_new_session=True,
+                            text=True)
+    try:
+        out, _ = proc.communicate(timeout=budget_s + 120)
+    except subprocess.TimeoutExpired:
+        os.killpg(proc.pid, signal.SIGKILL)
+        proc.communicate()
+        return {"unavailable": "the host ensemble run did not end in time"}
+    try:
+        return json.loads(out.strip().splitlines()[-1])
+    except (ValueError, IndexError):
+        return {"unavailable": f"the host ensemble run exited with {proc.returncode}"}
 
 
 def medium_network_extras(make_for) -> dict:
@@ -535,6 +618,18 @@ def medium_network_extras(make_for) -> dict:
     return out
 
 
+_ENSEMBLE = {}
+
+
+def ensemble(n_replicas: int = 256) -> list:
+    """The batched-ensemble networks (config-1 composition, 200-4,000
+    cylinders each, seed 2), built once per process."""
+    if n_replicas not in _ENSEMBLE:
+        from medyan_b200.network import make_batch
+        _ENSEMBLE[n_replicas] = make_batch(n_replicas, 2)
+    return _ENSEMBLE[n_replicas]
+
+
 def batch_extras(n_replicas: int = 256) -> dict:
     """The batched ensemble (256 networks of the medium network's composition,
     200-4,000 cylinders each): one batched minimization per precision, gradTol
@@ -544,8 +639,7 @@ def batch_extras(n_replicas: int = 256) -> dict:
     import torch
 
     from medyan_b200.forcefield import BatchMinimizer, ForceFieldManager, conjugate_gradient_params
-    from medyan_b200.network import make_batch
-    nets = make_batch(n_replicas, 2)
+    nets = ensemble(n_replicas)
     p = conjugate_gradient_params(grad_tol=1.0, max_dist=1.0, lambda_max=0.01, energy_rel_tol=1e-9)
     warm = conjugate_gradient_params(grad_tol=1.0, energy_call_limit=3)
     xs = [net.flat_coords() for net in nets]
@@ -650,6 +744,9 @@ def cpu_reference_rate(net, sample_s: float):
 
 def main():
     args = parse()
+    if args.cpu_ensemble:
+        print(json.dumps(cpu_ensemble(budget_s=args.cpu_sample_s)), flush=True)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if world > 1:
