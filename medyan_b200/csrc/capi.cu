@@ -290,6 +290,21 @@ medyan_status refresh_device_ff(medyan_mech* h) {
             e = cudaMemsetAsync(h->pass_fgroup_ticket.raw(), 0, sizeof(unsigned int) * h->pass_fgroup_ticket.cap,
                                 h->stream);
     }
+    {
+        // fallback queues with room for every pair (energies: every pair at
+        // every step size of a pass), so a pair the analytic formulas reject
+        // always gets its quadrature, as in the reference, however many
+        // there are
+        const size_t n_ex = ff.n_excl > 0 ? (size_t)ff.n_excl : 0;
+        const size_t ecap = n_ex * kMaxLambda > (size_t)kFallbackCap ? n_ex * kMaxLambda : (size_t)kFallbackCap;
+        const size_t fcap = n_ex > (size_t)kFallbackCap ? n_ex : (size_t)kFallbackCap;
+        if (e == cudaSuccess) e = h->e_fb_list.reserve(ecap);
+        if (e == cudaSuccess) e = h->f_fb_list.reserve(fcap);
+        h->es.fb_list = h->e_fb_list.raw();
+        h->fs.fb_list = h->f_fb_list.raw();
+        h->es.fb_cap = (int)h->e_fb_list.cap;
+        h->fs.fb_cap = (int)h->f_fb_list.cap;
+    }
     if (e != cudaSuccess) return cuda_status(e);
     h->es.partial = h->partial.ptr();
     h->ff_gen++;

@@ -824,7 +824,7 @@ CGLaunch make_launch(medyan_mech* h) {
                         h->deterministic, h->fs.status};
     c.spec = ForceTarget{c.f0,           c.f1, &c.st->parity, &c.st->spec_skip, c.d, &c.st->spec_lam,
                          h->deterministic, &c.st->spec_status};
-    c.spec_fs = ForceScratch{h->fs.fb_count, h->fs.fb_list, &c.st->spec_status};
+    c.spec_fs = ForceScratch{h->fs.fb_count, h->fs.fb_list, &c.st->spec_status, h->fs.fb_cap};
     return c;
 }
 

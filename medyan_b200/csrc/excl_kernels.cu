@@ -30,7 +30,8 @@ __global__ void __launch_bounds__(kMaxExclThreads) k_excl_energy(const DeviceFF 
                                                             const LambdaSet* __restrict__ lset,
                                                             double* __restrict__ partial, int nblk_total,
                                                             int blk_off, int* __restrict__ fb_count,
-                                                            int2* __restrict__ fb_list, int* __restrict__ bad, int n_logical) {
+                                                            int2* __restrict__ fb_list, int fb_cap, int* __restrict__ bad,
+                                                            int n_logical) {
     __shared__ double smem[4 * 32];
     for (int lb = blockIdx.x; lb < n_logical; lb += gridDim.x) {  // capped grid in batches
         if (ff.act && !ff.act[ff.rep_excl[lb]]) continue;  // batched: replica not in this pass
@@ -57,7 +58,7 @@ __global__ void __launch_bounds__(kMaxExclThreads) k_excl_energy(const DeviceFF 
                                           at(X[2], D[2], lam, move), at(X[3], D[3], lam, move), krs);
                 if (excl_energy_bad(U)) {
                     int slot = atomicAdd(fb_count, 1);
-                    if (slot < kFallbackCap) fb_list[slot] = make_int2(i, k);
+                    if (slot < fb_cap) fb_list[slot] = make_int2(i, k);
                     else atomicOr(bad + k, 2);
                     U = 0.0;
                 }
@@ -84,7 +85,8 @@ __device__ __forceinline__ V3 pos_at(const double* __restrict__ x, const ForceTa
 template <bool EXACT>
 __global__ void __launch_bounds__(kMaxExclThreads) k_excl_forces(const DeviceFF ff, const double* __restrict__ x,
                                                             const ForceTarget tgt, int* __restrict__ fb_count,
-                                                            int* __restrict__ fb_list, int* __restrict__ status, int n_logical) {
+                                                            int* __restrict__ fb_list, int fb_cap, int* __restrict__ status,
+                                                            int n_logical) {
     if (tgt.skip && *tgt.skip) return;
     for (int lb = blockIdx.x; lb < n_logical; lb += gridDim.x) {  // capped grid in batches
         if (ff.act && !ff.act[ff.rep_excl[lb]]) continue;  // batched: replica not in this pass
@@ -103,7 +105,7 @@ __global__ void __launch_bounds__(kMaxExclThreads) k_excl_forces(const DeviceFF 
             target_add(tgt, f, q.w, fo[3].x, fo[3].y, fo[3].z);
         } else {
             int slot = atomicAdd(fb_count, 1);
-            if (slot < kFallbackCap) fb_list[slot] = i;
+            if (slot < fb_cap) fb_list[slot] = i;
             else atomicOr(status, 2);
         }
     }
@@ -111,10 +113,10 @@ __global__ void __launch_bounds__(kMaxExclThreads) k_excl_forces(const DeviceFF 
 
 __global__ void __launch_bounds__(kBlock) k_excl_force_fallback(const DeviceFF ff, const double* __restrict__ x,
                                                                 const ForceTarget tgt, int* __restrict__ fb_count,
-                                                                const int* __restrict__ fb_list,
+                                                                const int* __restrict__ fb_list, int fb_cap,
                                                                 int* __restrict__ status) {
     __shared__ double red[6 * 32];
-    const int n = min(*fb_count, kFallbackCap);
+    const int n = min(*fb_count, fb_cap);
     if (n == 0) return;
     double* __restrict__ f = target_force(tgt);
     const double lam = tgt.lam ? *tgt.lam : 0.0;
@@ -248,8 +250,8 @@ __device__ void finish_rows(const DeviceFF& ff, const double* __restrict__ base,
 __global__ void __launch_bounds__(kSplitFinishThreads) k_energy_finish(
     const DeviceFF ff, const double* __restrict__ x, const double* __restrict__ d, const LambdaSet* __restrict__ lset,
     const double* __restrict__ partial, int nch, int nbb, int nbe, int* __restrict__ fb_count,
-    int2* __restrict__ fb_list, int* __restrict__ bad, double* __restrict__ out, double* __restrict__ stage,
-    unsigned int* __restrict__ ticket) {
+    int2* __restrict__ fb_list, int fb_cap, int* __restrict__ bad, double* __restrict__ out,
+    double* __restrict__ stage, unsigned int* __restrict__ ticket) {
     __shared__ double red[4 * 32];
     __shared__ double wsum[(kSplitFinishThreads / 32) * kMaxLambda * MEDYAN_FF_COUNT];
     __shared__ double sums[kMaxLambda][MEDYAN_FF_COUNT];
@@ -295,7 +297,7 @@ __global__ void __launch_bounds__(kSplitFinishThreads) k_energy_finish(
     __syncthreads();
     // queued fallback pairs: energyN in (slot, pair) order
     if (threadIdx.x == 0) {
-        int n = min(n_queued, kFallbackCap);
+        int n = min(n_queued, fb_cap);
         for (int a = 1; a < n; ++a) {
             int2 v = fb_list[a];
             int b = a - 1;
@@ -487,11 +489,12 @@ void launch_excl_energy(const DeviceFF& ff, int prec, const double* x, const dou
     (void)prec;
     const int g = logical_grid(ff, nbe), off = es.n_blocks_chain + es.n_blocks_bonded;
     if (d)
-        k_excl_energy<double, true><<<g, excl_block_of(ff), 0, s>>>(ff, x, d, lam, es.partial, total, off,
-                                                                   es.fb_count, es.fb_list, es.bad, nbe);
+        k_excl_energy<double, true><<<g, excl_block_of(ff), 0, s>>>(ff, x, d, lam, es.partial, total, off, es.fb_count,
+                                                                   es.fb_list, fb_capacity(es.fb_cap), es.bad, nbe);
     else
         k_excl_energy<double, false><<<g, excl_block_of(ff), 0, s>>>(ff, x, d, lam, es.partial, total, off,
-                                                                    es.fb_count, es.fb_list, es.bad, nbe);
+                                                                    es.fb_count, es.fb_list, fb_capacity(es.fb_cap),
+                                                                    es.bad, nbe);
 }
 
 void launch_excl_energy_fallback_and_finish(const DeviceFF& ff, const double* x, const double* d,
@@ -499,7 +502,7 @@ void launch_excl_energy_fallback_and_finish(const DeviceFF& ff, const double* x,
     const int g = es.stage && es.ticket ? kFinishBlocks : 1;
     k_energy_finish<<<g, kSplitFinishThreads, 0, s>>>(ff, x, d, lam, es.partial, es.n_blocks_chain,
                                                       es.n_blocks_bonded, es.n_blocks_excl, es.fb_count, es.fb_list,
-                                                      es.bad, es.out, es.stage, es.ticket);
+                                                      fb_capacity(es.fb_cap), es.bad, es.out, es.stage, es.ticket);
 }
 
 void launch_excl_forces(const DeviceFF& ff, int prec, const double* x, const ForceTarget& t, const ForceScratch& fs,
@@ -510,11 +513,11 @@ void launch_excl_forces(const DeviceFF& ff, int prec, const double* x, const For
     // the reference's expression order
     if (prec == MEDYAN_PREC_FP64)
         k_excl_forces<true><<<logical_grid(ff, nbe), excl_block_of(ff), 0, s>>>(ff, x, t, fs.fb_count, fs.fb_list,
-                                                                             fs.status, nbe);
+                                                                             fb_capacity(fs.fb_cap), fs.status, nbe);
     else
         k_excl_forces<false><<<logical_grid(ff, nbe), excl_block_of(ff), 0, s>>>(ff, x, t, fs.fb_count, fs.fb_list,
-                                                                              fs.status, nbe);
-    k_excl_force_fallback<<<1, kBlock, 0, s>>>(ff, x, t, fs.fb_count, fs.fb_list, fs.status);
+                                                                              fb_capacity(fs.fb_cap), fs.status, nbe);
+    k_excl_force_fallback<<<1, kBlock, 0, s>>>(ff, x, t, fs.fb_count, fs.fb_list, fb_capacity(fs.fb_cap), fs.status);
 }
 
 void launch_energy_finish_batched(const DeviceFF& ff, const double* x, const double* d, const LambdaSet* lam,

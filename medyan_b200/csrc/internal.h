@@ -81,6 +81,7 @@ struct EnergyScratch {
     double* partial;      // [kMaxLambda][n_blocks_total][4]: chain rows, bonded rows, excluded-volume rows
     int* fb_count;        // excluded-volume pairs needing energyN
     int2* fb_list;        // (pair, lambda slot)
+    int fb_cap;           // entries of fb_list (0: kFallbackCap)
     int* bad;             // per lambda slot: fallback failed / queue overflow
     double* out;          // [kMaxLambda][MEDYAN_FF_COUNT + 1]: per FF, then total
     // split finish (null: one block does it all): per-block slot sums
@@ -167,7 +168,11 @@ struct ForceScratch {
     int* fb_count;        // excluded-volume pairs needing forceN
     int* fb_list;
     int* status;          // bit 0: fallback failed, bit 1: queue overflow
+    int fb_cap;           // entries of fb_list (0: kFallbackCap)
 };
+
+// The capacity of a fallback queue (fb_cap, or kFallbackCap when unset).
+__host__ __device__ __forceinline__ int fb_capacity(int fb_cap) { return fb_cap > 0 ? fb_cap : kFallbackCap; }
 
 // Two side streams and their events. A pass launched with a Fork runs its
 // independent kernels on separate streams joined back into the caller's

@@ -121,6 +121,7 @@ extern "C" medyan_status medyan_excl_energy_noalloc(const double* d_coords, int3
     es.partial = scratch + kPartialOff;
     es.fb_count = fb_count;
     es.fb_list = reinterpret_cast<int2*>(scratch + kFbListOff);
+    es.fb_cap = kFallbackCap;  // the static array's queue holds kFallbackCap entries
     es.bad = bad;
     es.out = scratch + kOutOff;
     es.stage = nullptr;  // one-block finish: no arrival ticket to keep

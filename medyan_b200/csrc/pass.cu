@@ -196,7 +196,7 @@ __device__ __noinline__ void pass_finish(const PassArgs& a) {
         __syncthreads();
         if (threadIdx.x == 0) {
             // queued pairs in pair order (the queue fills in arrival order)
-            const int n = min(n_queued, kFallbackCap);
+            const int n = min(n_queued, a.e_fb_cap);
             for (int i = 1; i < n; ++i) {
                 const int2 q = __ldcg(a.e_fb_list + i);
                 int j = i - 1;
@@ -249,7 +249,7 @@ __device__ __noinline__ void pass_finish(const PassArgs& a) {
     }
     if constexpr (F) {
         double* __restrict__ f = target_force(a.t);
-        const int n = min(__ldcg(a.f_fb_count), kFallbackCap);
+        const int n = min(__ldcg(a.f_fb_count), a.f_fb_cap);
         for (int q = 0; q < n; ++q) {
             const int i = __ldcg(a.f_fb_list + q);
             const int4 bs = a.ff.excl_bs[i];
@@ -892,7 +892,7 @@ __global__ void __launch_bounds__(kExclThreadsMax) k_pass_excl(const __grid_cons
             const double U = excl_energy<double>(c1, c2, c3, c4, krs);
             if (excl_energy_bad(U)) {
                 const int slot = atomicAdd(a.e_fb_count, 1);
-                if (slot < kFallbackCap) a.e_fb_list[slot] = make_int2(i, 0);
+                if (slot < a.e_fb_cap) a.e_fb_list[slot] = make_int2(i, 0);
                 else atomicOr(a.e_bad, 2);
                 queued = true;
             } else {
@@ -908,7 +908,7 @@ __global__ void __launch_bounds__(kExclThreadsMax) k_pass_excl(const __grid_cons
                 target_add(a.t, f, q.w, fo[3].x, fo[3].y, fo[3].z);
             } else {
                 const int slot = atomicAdd(a.f_fb_count, 1);
-                if (slot < kFallbackCap) a.f_fb_list[slot] = i;
+                if (slot < a.f_fb_cap) a.f_fb_list[slot] = i;
                 else atomicOr(a.f_status, 2);
                 queued = true;
             }
@@ -1055,6 +1055,8 @@ PassArgs pass_args(const ChainDev& ch, const DeviceFF& ff, const PassGeometry& g
     a.lam_set = lam_set;
     a.e_fb_count = es.fb_count;
     a.e_fb_list = es.fb_list;
+    a.e_fb_cap = fb_capacity(es.fb_cap);
+    a.f_fb_cap = fb_capacity(fs.fb_cap);
     a.e_bad = es.bad;
     a.f_fb_count = fs.fb_count;
     a.f_fb_list = fs.fb_list;

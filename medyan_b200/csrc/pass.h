@@ -65,6 +65,7 @@ struct PassArgs {
     const LambdaSet* lam_set; // result copied to slots [0, K) (null: slot 0)
     int* e_fb_count;
     int2* e_fb_list;
+    int e_fb_cap, f_fb_cap;   // entries of the fallback queues
     int* e_bad;
     int* f_fb_count;
     int* f_fb_list;

@@ -210,3 +210,25 @@ def test_pass_kernel_count(gpu_lib, nets):
         # building the graphs for the count does not disturb evaluation
         e, per, f = ff.evaluate(x)
         assert np.isfinite(e)
+
+
+@pytest.mark.parametrize("layout", [0, 1])
+def test_many_quadrature_pairs(gpu_lib, oracle, layout):
+    """More rejected pairs than the fallback queue's minimum capacity (256):
+    the queues hold every pair of the network, so each rejected pair still
+    gets the reference's numerical integral (energyN) and the energy stays
+    finite and equal to the oracle's. 300 collinear cylinder pairs, energies
+    only (their force quadrature is 10^8 points per pair)."""
+    n_groups = 300
+    base = np.array([0, 0, 0, 10, 0, 0, 20, 0, 0, 30, 0, 0], float).reshape(4, 3)
+    x = np.concatenate([base + np.array([0.0, 100.0 * g, 0.0]) for g in range(n_groups)]).ravel()
+    excl_beads = np.concatenate([3 * (4 * g + np.arange(4)) for g in range(n_groups)])
+    sv = SystemView(4 * n_groups, excl_beads=excl_beads, excl_k=np.full(n_groups, 1e5),
+                    excl_eqlen=np.full(2 * n_groups, 10.0))
+    eo, pero = oracle.energy(sv, x)
+    assert np.isfinite(eo)
+    with ForceFieldManager("fp64") as ff:
+        ff.vectorize_all_force_fields(sv)
+        ff.set_shapes(pass_layout=layout)
+        e = ff.compute_energy(x)
+    assert np.isfinite(e) and abs(e - eo) <= 1e-9 * abs(eo), (e, eo)
