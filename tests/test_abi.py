@@ -72,3 +72,12 @@ def test_errors_without_device_are_reported_not_faked():
     # the CUDA error behind the status is named, in the message too
     name = lib.load().medyan_last_cuda_error().decode()
     assert name.startswith("cudaError") and name in str(e.value)
+
+
+def test_deterministic_switches_check_their_arguments():
+    # argument checks come before any CUDA call, so they hold without a GPU
+    L = lib.load()
+    invalid = 1  # MEDYAN_ERR_INVALID_ARG
+    assert L.medyan_mech_set_deterministic(None, 1) == invalid
+    assert L.medyan_batch_set_deterministic(None, 1) == invalid
+    assert L.medyan_batch_set_deterministic(None, 2) == invalid
