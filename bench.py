@@ -255,6 +255,15 @@ def run_ours(args, rank: int, world: int) -> dict:
         w1.record(stream)
     L.medyan_mech_synchronize(h)
     t_warm = w0.elapsed_time(w1) / 1e3 / K
+    # force passes back to back without the flush: the L2-warm side of the
+    # roofline (coordinates and records stay in the 126 MB L2)
+    with torch.cuda.stream(stream):
+        w0.record(stream)
+        for i in range(K):
+            L.medyan_mech_enqueue_forces(h)
+        w1.record(stream)
+    L.medyan_mech_synchronize(h)
+    t_force_warm = w0.elapsed_time(w1) / 1e3 / K
     t_step = max_over_ranks(sum(t_steps), world, "cuda")
 
     # e2e through the C ABI from page-locked host buffers: each step's own
@@ -340,13 +349,17 @@ def run_ours(args, rank: int, world: int) -> dict:
         "accuracy_vs_fp64": {"rel_force_err": rel_force_err, "rel_energy_err": rel_energy_err},
         "fp64": fp64_arm,
         "breakdown_ms": {"force_pass_alone": 1e3 * sum(t_force) / K, "energy_pass_alone": 1e3 * sum(t_energy) / K,
-                         "step_l2_warm": 1e3 * t_warm,
+                         "step_l2_warm": 1e3 * t_warm, "force_pass_l2_warm": 1e3 * t_force_warm,
                          "step_spread": {"min": 1e3 * min(t_steps), "median": 1e3 * statistics.median(t_steps),
                                          "max": 1e3 * max(t_steps)}},
     }
     fb = abytes["forces"]
     t_f = sum(t_force) / K
     result["roofline"] = roofline(fb / t_f / 1e9, fb)
+    # the same bytes over the L2-warm pass time: what the pass would reach if
+    # DRAM were free, so the gap to the peak is not DRAM time
+    result["roofline"]["l2_warm"] = {"achieved": fb / t_force_warm / 1e9,
+                                     "frac": fb / t_force_warm / 1e9 / result["roofline"]["peak"]}
     result["algorithmic_bytes"] = abytes
 
     # neighbor-list rebuild on the device (host call, coordinates resident)
