@@ -21,7 +21,6 @@ from __future__ import annotations
 
 import argparse
 import ctypes as C
-import os
 import sys
 
 import numpy as np
@@ -62,8 +61,7 @@ def main(argv=None) -> int:
     from .forcefield import ForceFieldManager
     from .network import make_workload
 
-    if not os.path.exists(_build.LIB_TRACE):
-        _build.build(trace=True)
+    _build.build(trace=True)  # recompiles only what is stale
     _lib.LIB_PATH = _build.LIB_TRACE
     raw = C.CDLL(_build.LIB_TRACE)
     raw.medyan_pass_trace_dump.restype = C.c_int
